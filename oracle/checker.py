@@ -1,0 +1,180 @@
+"""ORACLE / TEST INFRASTRUCTURE ONLY -- ctypes access to the two CPU checkers.
+
+* ``ReferenceEngine``   -- the reference Cyclops engine compiled from source
+  (``oracle/_ref/libccd_ref.so``, built by ``make -C oracle ref`` where the
+  reference sources are present).
+* ``RestatementEngine`` -- the plain-C FP64 restatement (``oracle/_build/
+  libccd_oracle.so``, ``make -C oracle port``; builds anywhere gcc exists).
+
+Both expose the same calls (``fit``, ``grad_hess``, ``update_beta``,
+``loglik``, ``xbeta`` ...) on a ``CyclopsData`` problem.  Only tests/,
+``__graft_entry__.smoke`` and the CPU-baseline leg of ``bench.py`` import this
+module; the product path never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_LIB = os.path.join(HERE, "_ref", "libccd_ref.so")
+PORT_LIB = os.path.join(HERE, "_build", "libccd_oracle.so")
+
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def build(target: str = "all") -> None:
+    subprocess.run(["make", "-s", "-C", HERE, target], check=True)
+
+
+def reference_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+class _Engine:
+    prefix = ""
+    libpath = ""
+    _lib_cache: dict = {}
+
+    @classmethod
+    def lib(cls):
+        if cls.libpath not in _Engine._lib_cache:
+            if not os.path.exists(cls.libpath):
+                if cls is RestatementEngine:
+                    build("port")
+                else:
+                    raise FileNotFoundError(cls.libpath)
+            lib = C.CDLL(cls.libpath)
+            p = cls.prefix
+            getattr(lib, p + "create").restype = _P
+            getattr(lib, p + "create").argtypes = [C.c_int, C.c_int, C.c_int64, C.c_int] + [_P] * 8 + [
+                C.c_int, _P, _P, C.c_char_p, C.c_int]
+            getattr(lib, p + "destroy").argtypes = [_P]
+            getattr(lib, p + "fit").argtypes = [_P, C.c_int, C.c_double, C.c_int, C.c_double, C.c_int,
+                                                _P, _P, _P, _P, C.c_char_p, C.c_int]
+            getattr(lib, p + "grad_hess").argtypes = [_P, C.c_int, _P, _P]
+            getattr(lib, p + "update_beta").argtypes = [_P, C.c_int, C.c_double]
+            for name in ("set_weights", "set_beta", "loglik", "log_prior", "get_beta", "get_xbeta"):
+                getattr(lib, p + name).argtypes = [_P, _P]
+            getattr(lib, p + "predictive_loglik").argtypes = [_P, _P, _P]
+            getattr(lib, p + "num_patients").argtypes = [_P]
+            _Engine._lib_cache[cls.libpath] = lib
+        return _Engine._lib_cache[cls.libpath]
+
+    def __init__(self, d, fp32: bool = False):
+        self.d = d
+        self._keep = []
+
+        def arr(a, dt):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype=dt)
+            self._keep.append(a)
+            return a
+
+        lib = self.lib()
+        err = C.create_string_buffer(512)
+        self.h = getattr(lib, self.prefix + "create")(
+            d.model_type, int(fp32), d.K, d.J, _ptr(arr(d.y, np.float64)),
+            _ptr(arr(d.time, np.float64)), _ptr(arr(d.stratum, np.int64)),
+            _ptr(arr(d.col_start, np.int64)), _ptr(arr(d.rows, np.int32)),
+            _ptr(arr(d.val_start, np.int64)), _ptr(arr(d.vals, np.float64)),
+            _ptr(arr(d.fmt, np.uint8)), int(d.offset_col0), _ptr(arr(d.prior_type, np.int32)),
+            _ptr(arr(d.prior_var, np.float64)), err, 512)
+        if not self.h:
+            raise RuntimeError(err.value.decode())
+
+    def _f(self, name):
+        return getattr(self.lib(), self.prefix + name)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._f("destroy")(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_weights(self, w: Optional[np.ndarray]):
+        if w is not None:
+            w = np.ascontiguousarray(w, np.float64)
+            self._w = w
+        self._f("set_weights")(self.h, _ptr(w))
+
+    def set_beta(self, beta: np.ndarray):
+        beta = np.ascontiguousarray(beta, np.float64)
+        self._f("set_beta")(self.h, _ptr(beta))
+
+    def fit(self, conv_type: int = 0, tol: float = 1e-6, max_iter: int = 1000,
+            initial_bound: float = 2.0, max_bound_count: int = 5):
+        beta = np.zeros(self.d.J)
+        ll = C.c_double()
+        it = C.c_int()
+        fl = C.c_int()
+        err = C.create_string_buffer(512)
+        rc = self._f("fit")(self.h, conv_type, tol, max_iter, initial_bound, max_bound_count,
+                            _ptr(beta), C.byref(ll), C.byref(it), C.byref(fl), err, 512)
+        if rc != 0:
+            raise RuntimeError(err.value.decode())
+        return {"beta": beta, "loglik": ll.value, "iterations": it.value, "flag": fl.value}
+
+    def grad_hess(self, j: int):
+        g, h = C.c_double(), C.c_double()
+        self._f("grad_hess")(self.h, j, C.byref(g), C.byref(h))
+        return g.value, h.value
+
+    def update_beta(self, j: int, delta: float):
+        self._f("update_beta")(self.h, j, delta)
+
+    def loglik(self) -> float:
+        v = C.c_double()
+        self._f("loglik")(self.h, C.byref(v))
+        return v.value
+
+    def log_prior(self) -> float:
+        v = C.c_double()
+        self._f("log_prior")(self.h, C.byref(v))
+        return v.value
+
+    def beta(self) -> np.ndarray:
+        b = np.zeros(self.d.J)
+        self._f("get_beta")(self.h, _ptr(b))
+        return b
+
+    def xbeta(self) -> np.ndarray:
+        x = np.zeros(self.d.K)
+        self._f("get_xbeta")(self.h, _ptr(x))
+        return x
+
+    def predictive_loglik(self, w: np.ndarray) -> float:
+        w = np.ascontiguousarray(w, np.float64)
+        v = C.c_double()
+        self._f("predictive_loglik")(self.h, _ptr(w), C.byref(v))
+        return v.value
+
+
+class ReferenceEngine(_Engine):
+    prefix = "ref_"
+    libpath = REF_LIB
+
+
+class RestatementEngine(_Engine):
+    prefix = "orc_"
+    libpath = PORT_LIB
+
+
+def best_engine():
+    """The compiled reference when present, else the restatement."""
+    return ReferenceEngine if reference_available() else RestatementEngine

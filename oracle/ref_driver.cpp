@@ -1,0 +1,288 @@
+// ref_driver.cpp -- ORACLE / TEST INFRASTRUCTURE ONLY.
+//
+// A flat extern "C" driver around the reference Cyclops engine (namespace
+// bsccs), compiled from the reference's own sources by oracle/Makefile into
+// oracle/_ref/libccd_ref.so.  It is the checker the CUDA path is compared
+// against and the timed CPU baseline; nothing in the product links it.
+//
+// Data enters exactly the way the reference's R binding feeds it:
+//   ModelData::loadY   (src/cyclops/ModelData.cpp:69-140)
+//   ModelData::loadX   (src/cyclops/ModelData.cpp:246-370), intercept first
+//   ModelData::setOffsetCovariate (src/cyclops/ModelData.cpp:640-651)
+//   AbstractModelSpecifics::factory (src/cyclops/engine/AbstractModelSpecifics.cpp:128-154)
+//   CyclicCoordinateDescent::update (src/cyclops/CyclicCoordinateDescent.cpp:586-615)
+// so the resulting column order is [offset?, intercept?, covariates...].
+
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#include <map>
+
+#include "ModelData.h"
+#include "CyclicCoordinateDescent.h"
+#include "priors/JointPrior.h"
+#include "priors/CovariatePrior.h"
+
+using namespace bsccs;
+
+namespace {
+
+struct QuietLogger : loggers::ProgressLogger {
+    void writeLine(const std::ostringstream&) override {}
+    void yield() override {}
+};
+struct ThrowingErrors : loggers::ErrorHandler {
+    void throwError(const std::ostringstream& s) override { throw std::runtime_error(s.str()); }
+};
+
+// Column format codes: the reference's FormatType (CompressedDataMatrix.h:36-38).
+enum { F_DENSE = 0, F_SPARSE = 1, F_INDICATOR = 2, F_INTERCEPT = 3 };
+
+struct RefHandle {
+    std::shared_ptr<QuietLogger> log;
+    std::shared_ptr<ThrowingErrors> err;
+    std::unique_ptr<AbstractModelData> data;
+    std::unique_ptr<AbstractModelSpecifics> ms;
+    priors::JointPriorPtr prior;
+    std::unique_ptr<CyclicCoordinateDescent> ccd;
+    int J = 0;
+    int64_t K = 0;
+    bool weighted = false;
+};
+
+void set_err(char* err, int errlen, const char* msg) {
+    if (err && errlen > 0) {
+        std::strncpy(err, msg, errlen - 1);
+        err[errlen - 1] = 0;
+    }
+}
+
+template <typename Real>
+AbstractModelData* build_data(ModelType mt, int64_t K, int J, const double* y, const double* time,
+                              const int64_t* stratum, const int64_t* col_start, const int32_t* rows,
+                              const int64_t* val_start, const double* vals, const uint8_t* fmt,
+                              int offset_col0, loggers::ProgressLoggerPtr lg,
+                              loggers::ErrorHandlerPtr er) {
+    auto* md = new ModelData<Real>(mt, lg, er);
+    std::vector<IdType> rid(K);
+    for (int64_t i = 0; i < K; ++i) rid[i] = i;
+    std::vector<IdType> sid;
+    if (stratum) sid.assign(stratum, stratum + K);
+    std::vector<double> yv(y, y + K);
+    std::vector<double> tv;
+    if (time) tv.assign(time, time + K);
+    md->loadY(sid, rid, yv, tv);
+
+    // The reference moves an INTERCEPT to the front on load and the offset to
+    // the front on setOffsetCovariate; loading the intercept first and the
+    // offset last reproduces the caller's [offset?, intercept?, rest] order.
+    const int first = offset_col0 ? 1 : 0;
+    std::vector<int> order;
+    for (int j = first; j < J; ++j)
+        if (fmt[j] == F_INTERCEPT) order.push_back(j);
+    for (int j = first; j < J; ++j)
+        if (fmt[j] != F_INTERCEPT) order.push_back(j);
+    if (offset_col0) order.push_back(0);
+
+    for (int j : order) {
+        std::vector<IdType> r;
+        std::vector<double> v;
+        bool forceSparse = false;
+        switch (fmt[j]) {
+        case F_INTERCEPT:
+            break;
+        case F_DENSE:
+            v.assign(vals + val_start[j], vals + val_start[j + 1]);
+            break;
+        case F_INDICATOR:
+            r.assign(rows + col_start[j], rows + col_start[j + 1]);
+            break;
+        case F_SPARSE:
+            r.assign(rows + col_start[j], rows + col_start[j + 1]);
+            v.assign(vals + val_start[j], vals + val_start[j + 1]);
+            forceSparse = true;
+            break;
+        default:
+            throw std::runtime_error("unknown column format");
+        }
+        const IdType label = (offset_col0 && j == 0) ? IdType(1000000000) : IdType(j + 1);
+        if (fmt[j] == F_INDICATOR && r.empty()) {
+            // an empty indicator column: loadX needs no values to keep it INDICATOR
+            md->loadX(label, r, v, false, false, false);
+        } else {
+            md->loadX(label, r, v, false, false, forceSparse);
+        }
+    }
+    if (offset_col0) md->setOffsetCovariate(IdType(1000000000));
+    return md;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Build ModelData + ModelSpecifics + MixtureJointPrior + CyclicCoordinateDescent.
+// model_type uses the reference's ModelType numbering (Types.h:134-147).
+// prior_type per column: 0 none, 1 Laplace, 2 Normal (priors::PriorType, Types.h:100-105).
+void* ref_create(int model_type, int fp32, int64_t K, int J, const double* y, const double* time,
+                 const int64_t* stratum, const int64_t* col_start, const int32_t* rows,
+                 const int64_t* val_start, const double* vals, const uint8_t* fmt, int offset_col0,
+                 const int32_t* prior_type, const double* prior_var, char* err, int errlen) {
+    try {
+        auto h = new RefHandle();
+        h->log = std::make_shared<QuietLogger>();
+        h->err = std::make_shared<ThrowingErrors>();
+        h->J = J;
+        h->K = K;
+        const ModelType mt = static_cast<ModelType>(model_type);
+        if (fp32) {
+            h->data.reset(build_data<float>(mt, K, J, y, time, stratum, col_start, rows, val_start,
+                                            vals, fmt, offset_col0, h->log, h->err));
+        } else {
+            h->data.reset(build_data<double>(mt, K, J, y, time, stratum, col_start, rows, val_start,
+                                             vals, fmt, offset_col0, h->log, h->err));
+        }
+        h->ms.reset(AbstractModelSpecifics::factory(mt, *h->data, DeviceType::CPU, "native"));
+        if (!h->ms) throw std::runtime_error("factory returned nullptr (unsupported model)");
+
+        std::map<std::pair<int, double>, priors::PriorPtr> unique;
+        auto getPrior = [&](int type, double var) -> priors::PriorPtr {
+            auto key = std::make_pair(type, type == 0 ? 0.0 : var);
+            auto it = unique.find(key);
+            if (it != unique.end()) return it->second;
+            priors::PriorPtr p;
+            if (type == 1) p = std::make_shared<priors::LaplacePrior>(var);
+            else if (type == 2) p = std::make_shared<priors::NormalPrior>(var);
+            else p = std::make_shared<priors::NoPrior>();
+            unique[key] = p;
+            return p;
+        };
+        auto mix = std::make_shared<priors::MixtureJointPrior>(getPrior(prior_type[0], prior_var[0]), J);
+        for (int j = 1; j < J; ++j) mix->changePrior(getPrior(prior_type[j], prior_var[j]), j);
+        h->prior = mix;
+        h->ccd.reset(new CyclicCoordinateDescent(*h->data, *h->ms, h->prior, h->log, h->err));
+        h->ccd->setNoiseLevel(SILENT);
+        return h;
+    } catch (const std::exception& e) {
+        set_err(err, errlen, e.what());
+        return nullptr;
+    }
+}
+
+void ref_destroy(void* hp) {
+    auto h = static_cast<RefHandle*>(hp);
+    if (!h) return;
+    h->ccd.reset();
+    h->ms.reset();
+    h->data.reset();
+    delete h;
+}
+
+// Row weights (CV fold weights); NULL clears them (CyclicCoordinateDescent.cpp:496-519).
+int ref_set_weights(void* hp, const double* w) {
+    auto h = static_cast<RefHandle*>(hp);
+    if (w) {
+        std::vector<double> buf(w, w + h->K);
+        h->ccd->setWeights(buf.data());
+        h->weighted = true;
+    } else {
+        h->ccd->setWeights(nullptr);
+        h->weighted = false;
+    }
+    return 0;
+}
+
+int ref_set_beta(void* hp, const double* beta) {
+    auto h = static_cast<RefHandle*>(hp);
+    std::vector<double> b(beta, beta + h->J);
+    h->ccd->setBeta(b);
+    return 0;
+}
+
+// Full mode finding through CyclicCoordinateDescent::update.
+int ref_fit(void* hp, int conv_type, double tol, int max_iter, double initial_bound,
+            int max_bound_count, double* beta_out, double* ll_out, int* iters_out, int* flag_out,
+            char* err, int errlen) {
+    auto h = static_cast<RefHandle*>(hp);
+    try {
+        ModeFindingArguments a;
+        a.tolerance = tol;
+        a.maxIterations = max_iter;
+        a.convergenceType = conv_type;
+        a.initialBound = initial_bound;
+        a.maxBoundCount = max_bound_count;
+        h->ccd->update(a);
+        for (int j = 0; j < h->J; ++j) beta_out[j] = h->ccd->getBeta(j);
+        *ll_out = h->ccd->getLogLikelihood();
+        *iters_out = h->ccd->getIterationCount();
+        *flag_out = static_cast<int>(h->ccd->getUpdateReturnFlag());
+        return 0;
+    } catch (const std::exception& e) {
+        set_err(err, errlen, e.what());
+        return -1;
+    }
+}
+
+// Per-coordinate gradient/Hessian exactly as ccdUpdateBeta obtains them
+// (CyclicCoordinateDescent.cpp:1394-1405), before the h<0 clamp.
+int ref_grad_hess(void* hp, int j, double* g, double* hs) {
+    auto h = static_cast<RefHandle*>(hp);
+    h->ccd->getLogLikelihood();  // brings the lazy state up to date (checkAllLazyFlags)
+    h->ms->computeNumeratorForGradient(j, h->weighted);
+    h->ms->computeGradientAndHessian(j, g, hs, h->weighted);
+    return 0;
+}
+
+// beta[j] += delta followed by ModelSpecifics::updateXBeta (setBeta(int,double),
+// CyclicCoordinateDescent.cpp:719-733).
+int ref_update_beta(void* hp, int j, double delta) {
+    auto h = static_cast<RefHandle*>(hp);
+    h->ccd->getLogLikelihood();
+    h->ccd->setBeta(j, h->ccd->getBeta(j) + delta);
+    return 0;
+}
+
+int ref_loglik(void* hp, double* ll) {
+    auto h = static_cast<RefHandle*>(hp);
+    *ll = h->ccd->getLogLikelihood();
+    return 0;
+}
+
+int ref_log_prior(void* hp, double* lp) {
+    auto h = static_cast<RefHandle*>(hp);
+    *lp = h->ccd->getLogPrior();
+    return 0;
+}
+
+int ref_get_beta(void* hp, double* out) {
+    auto h = static_cast<RefHandle*>(hp);
+    for (int j = 0; j < h->J; ++j) out[j] = h->ccd->getBeta(j);
+    return 0;
+}
+
+int ref_get_xbeta(void* hp, double* out) {
+    auto h = static_cast<RefHandle*>(hp);
+    h->ccd->getLogLikelihood();
+    auto xb = h->ms->getXBeta();
+    std::memcpy(out, xb.data(), sizeof(double) * xb.size());
+    return static_cast<int>(xb.size());
+}
+
+// Predictive log-likelihood on held-out weights (CyclicCoordinateDescent.cpp:319-355).
+int ref_predictive_loglik(void* hp, const double* w, double* out) {
+    auto h = static_cast<RefHandle*>(hp);
+    std::vector<double> buf(w, w + h->K);
+    *out = h->ccd->getNewPredictiveLogLikelihood(buf.data());
+    return 0;
+}
+
+int ref_num_patients(void* hp) {
+    auto h = static_cast<RefHandle*>(hp);
+    return static_cast<int>(h->data->getNumberOfPatients());
+}
+
+}  // extern "C"
