@@ -1,0 +1,770 @@
+// api.cu -- the C ABI of libccdb.so (include/ccdb.h) and the host runtime
+// behind it: device memory under a per-context HBM budget, matrix upload,
+// per-fit lazy state (the flags of CyclicCoordinateDescent::checkAllLazyFlags,
+// CyclicCoordinateDescent.cpp:388-406), schedule caching, and the mode-finding
+// driver (CyclicCoordinateDescent::update, .cpp:586-615).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/ccdb.h"
+#include "engine.h"
+
+namespace ccdb {
+
+thread_local std::string g_last_error;
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void check_cuda(cudaError_t e, const char* what) {
+    if (e != cudaSuccess)
+        throw Error(CCDB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void* Context::alloc(size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    bytes = (bytes + 255) / 256 * 256;
+    {
+        std::lock_guard<std::mutex> g(mu);
+        if (budget && in_use + bytes > budget)
+            throw Error(CCDB_ERR_BUDGET, "device allocation of " + std::to_string(bytes) +
+                                             " bytes exceeds the HBM budget");
+        in_use += bytes;
+    }
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        std::lock_guard<std::mutex> g(mu);
+        in_use -= bytes;
+        check_cuda(e, "cudaMalloc");
+    }
+    std::lock_guard<std::mutex> g(mu);
+    sizes[p] = bytes;
+    return p;
+}
+
+void Context::release(void* p) {
+    if (!p) return;
+    cudaFree(p);
+    std::lock_guard<std::mutex> g(mu);
+    auto it = sizes.find(p);
+    if (it != sizes.end()) {
+        in_use -= it->second;
+        sizes.erase(it);
+    }
+}
+
+template <typename T>
+T* upload(Context* c, const T* h, size_t n, cudaStream_t s) {
+    T* d = static_cast<T*>(c->alloc(sizeof(T) * (n ? n : 1)));
+    if (n && h) check_cuda(cudaMemcpyAsync(d, h, sizeof(T) * n, cudaMemcpyHostToDevice, s), "upload");
+    return d;
+}
+
+int64_t Matrix::entries(int j) const {
+    if (fmt[j] == F_DENSE || fmt[j] == F_INTERCEPT) return K;
+    return col_start[j + 1] - col_start[j];
+}
+
+Matrix::~Matrix() {
+    for (void* p : {(void*)d_col_ptr, (void*)d_rows, (void*)d_val_ptr, (void*)d_vals, (void*)d_fmt,
+                    (void*)d_row_ptr, (void*)d_csr_col, (void*)d_csr_val})
+        ctx->release(p);
+}
+
+// Row-major copy for computeXBeta: per row, entries in increasing column order
+// (dense-like columns included), built once by a stable counting sort.
+void Matrix::ensure_csr(cudaStream_t s) {
+    if (d_row_ptr) return;
+    std::vector<int64_t> cnt(K + 1, 0);
+    for (int j = 0; j < J; ++j) {
+        if (fmt[j] == F_DENSE || fmt[j] == F_INTERCEPT) {
+            for (int64_t k = 0; k < K; ++k) cnt[k + 1]++;
+        } else {
+            for (int64_t p = col_start[j]; p < col_start[j + 1]; ++p) cnt[rows_h[p] + 1]++;
+        }
+    }
+    for (int64_t k = 0; k < K; ++k) cnt[k + 1] += cnt[k];
+    const int64_t n = cnt[K];
+    std::vector<int32_t> col(n);
+    std::vector<double> val(n);
+    std::vector<int64_t> pos(cnt.begin(), cnt.end() - 1);
+    for (int j = 0; j < J; ++j) {
+        const uint8_t f = fmt[j];
+        if (f == F_DENSE || f == F_INTERCEPT) {
+            for (int64_t k = 0; k < K; ++k) {
+                const int64_t q = pos[k]++;
+                col[q] = j;
+                val[q] = (f == F_DENSE) ? vals_h[val_start[j] + k] : 1.0;
+            }
+        } else {
+            for (int64_t p = col_start[j]; p < col_start[j + 1]; ++p) {
+                const int64_t q = pos[rows_h[p]]++;
+                col[q] = j;
+                val[q] = (f == F_SPARSE) ? vals_h[val_start[j] + (p - col_start[j])] : 1.0;
+            }
+        }
+    }
+    d_row_ptr = upload(ctx, cnt.data(), cnt.size(), s);
+    d_csr_col = upload(ctx, col.data(), col.size(), s);
+    d_csr_val = upload(ctx, val.data(), val.size(), s);
+    check_cuda(cudaStreamSynchronize(s), "csr upload");
+}
+
+// ------------------------------------------------------------------ Fit
+
+Fit::~Fit() {
+    for (void* p : {(void*)row, (void*)y, (void*)beta, (void*)hdelta, (void*)xjy, (void*)ptype,
+                    (void*)pvar, (void*)st, (void*)grid_bar, (void*)red, (void*)xb_tmp, (void*)w,
+                    (void*)gh_parts, (void*)gh_out})
+        ctx->release(p);
+    release_schedule();
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+}
+
+void Fit::release_schedule() {
+    if (!sched) return;
+    for (void* p : {(void*)sched->segs, (void*)sched->cta_seg, (void*)sched->tasks,
+                    (void*)sched->level_need, (void*)sched->level_done, (void*)sched->col_arrive,
+                    (void*)sched->partials})
+        ctx->release(p);
+    sched.reset();
+}
+
+IndepParams Fit::params() const {
+    IndepParams P{};
+    P.col_ptr = m->d_col_ptr;
+    P.rows = m->d_rows;
+    P.val_ptr = m->d_val_ptr;
+    P.vals = m->d_vals;
+    P.fmt = m->d_fmt;
+    P.K = K;
+    P.J = J;
+    P.model = model;
+    P.row = row;
+    P.y = y;
+    P.beta = beta;
+    P.hdelta = hdelta;
+    P.xjy = xjy;
+    P.ptype = ptype;
+    P.pvar = pvar;
+    P.red = red;
+    P.grid_bar = grid_bar;
+    P.st = st;
+    P.ll_fixed = ll_fixed;
+    P.wait_limit_ns = wait_limit_ns;
+    if (sched) {
+        P.segs = sched->segs;
+        P.cta_seg = sched->cta_seg;
+        P.tasks = sched->tasks;
+        P.n_levels = sched->host.n_levels;
+        P.level_done = sched->level_done;
+        P.level_need = sched->level_need;
+        P.col_arrive = sched->col_arrive;
+        P.partials = sched->partials;
+    }
+    return P;
+}
+
+// ModelSpecifics::setWeights + computeFixedTermsInLogLikelihood + computeXjY
+// (ModelSpecifics.hpp:427-484, 570-587, 486-524).  Independent rows: the
+// N-weights equal the row weights (observationCount = 1).
+void Fit::apply_weights() {
+    std::vector<double> wh(K, 1.0);
+    if (weighted) wh = w_h;
+    check_cuda(cudaMemcpyAsync(w, wh.data(), sizeof(double) * K, cudaMemcpyHostToDevice, stream),
+               "weights");
+    check_cuda(launch_xjy(m->d_col_ptr, m->d_rows, m->d_val_ptr, m->d_vals, m->d_fmt, y,
+                          weighted ? w : nullptr, K, J, xjy, stream),
+               "xjy");
+    ll_fixed = 0.0;
+    if (model == M_POISSON) {  // PoissonRegression::logLikeFixedTermsContrib, ModelSpecifics.h:1596-1601
+        for (int64_t i = 0; i < K; ++i) {
+            double t = 0.0;
+            for (int c = 2; c <= (int)y_h[i]; c++) t += -std::log((double)c);
+            ll_fixed += weighted ? t * wh[i] : t;
+        }
+    }
+    check_cuda(cudaStreamSynchronize(stream), "weights sync");
+    valid_weights = true;
+    suff_known = false;
+}
+
+// CyclicCoordinateDescent::computeXBeta (.cpp:1452-1470).
+void Fit::compute_xbeta() {
+    int nonzero = 0, only = -1;
+    for (int j = 0; j < J; ++j)
+        if (beta_h[j] != 0.0) {
+            ++nonzero;
+            only = j;
+        }
+    if (nonzero == 0) {
+        check_cuda(cudaMemsetAsync(xb_tmp, 0, sizeof(double) * K, stream), "xb zero");
+    } else {
+        const_cast<Matrix*>(m)->ensure_csr(stream);
+        check_cuda(launch_xbeta_csr(m->d_row_ptr, m->d_csr_col, m->d_csr_val, beta, K, xb_tmp, stream),
+                   "xbeta");
+    }
+    (void)only;
+    xb_pending = true;
+    xb_known = true;
+    suff_known = false;
+}
+
+// computeRemainingStatistics (ModelSpecifics.hpp:1588-1633).
+void Fit::remaining_statistics() {
+    const double null_denom = (model == M_LOGISTIC) ? 1.0 : 0.0;
+    check_cuda(launch_remaining_stats(row, xb_pending ? xb_tmp : nullptr, w, K, null_denom, stream),
+               "remaining statistics");
+    xb_pending = false;
+    suff_known = true;
+}
+
+void Fit::check_lazy() {
+    if (!xb_known) compute_xbeta();
+    if (!valid_weights) apply_weights();
+    if (!suff_known) remaining_statistics();
+}
+
+void Fit::upload_beta() {
+    check_cuda(cudaMemcpyAsync(beta, beta_h.data(), sizeof(double) * J, cudaMemcpyHostToDevice, stream),
+               "beta upload");
+}
+
+void Fit::download_beta() {
+    check_cuda(cudaMemcpyAsync(beta_h.data(), beta, sizeof(double) * J, cudaMemcpyDeviceToHost, stream),
+               "beta download");
+    check_cuda(cudaStreamSynchronize(stream), "beta sync");
+}
+
+void Fit::ensure_schedule() {
+    if (sched && sched->fixed == fixed) return;
+    release_schedule();
+    int bps = 0;
+    check_cuda(indep_sweep_occupancy(model, &bps), "occupancy");
+    if (bps < 1) throw Error(CCDB_ERR_CUDA, "sweep kernel does not fit on an SM");
+    ScheduleParams sp;
+    sp.n_cta = ctx->n_sm * std::min(bps, 1);
+    sp.warps_per_cta = indep_threads() / 32;
+    std::vector<int64_t> entries(J);
+    for (int j = 0; j < J; ++j) entries[j] = m->entries(j);
+    auto s = std::make_unique<DevSchedule>();
+    s->fixed = fixed;
+    s->host = build_schedule(K, J, m->col_start.data(), m->rows_h.data(), m->fmt.data(),
+                             fixed.data(), nullptr, K, entries.data(), sp);
+    if (s->host.max_split_per_seg > indep_max_split())
+        throw Error(CCDB_ERR_UNSUPPORTED, "too many split columns on one level");
+    s->segs = upload(ctx, s->host.segs.data(), s->host.segs.size(), stream);
+    s->cta_seg = upload(ctx, s->host.cta_seg.data(), s->host.cta_seg.size(), stream);
+    s->tasks = upload(ctx, s->host.tasks.data(), s->host.tasks.size(), stream);
+    s->level_need = upload(ctx, s->host.level_need.data(), s->host.level_need.size(), stream);
+    s->level_done = static_cast<unsigned*>(ctx->alloc(sizeof(unsigned) * std::max(1, s->host.n_levels)));
+    s->col_arrive = static_cast<unsigned*>(ctx->alloc(sizeof(unsigned) * std::max(1, J)));
+    s->partials = static_cast<double2*>(ctx->alloc(sizeof(double2) * std::max(1, s->host.n_partials)));
+    check_cuda(cudaStreamSynchronize(stream), "schedule upload");
+    sched = std::move(s);
+}
+
+// Objective terms {LL num, LL den, gradient objective, log prior} of the
+// current state, reduced in a fixed order.
+void Fit::objective_terms(double* out4) {
+    check_lazy();
+    const int nb = ctx->n_sm;
+    IndepParams P = params();
+    check_cuda(launch_indep_objective(P, nb, stream), "objective");
+    std::vector<double2> parts(2 * nb);
+    check_cuda(cudaMemcpyAsync(parts.data(), red, sizeof(double2) * 2 * nb, cudaMemcpyDeviceToHost, stream),
+               "objective copy");
+    check_cuda(cudaStreamSynchronize(stream), "objective sync");
+    double t[4] = {0, 0, 0, 0};
+    for (int c = 0; c < nb; ++c) {
+        t[0] += parts[2 * c].x;
+        t[1] += parts[2 * c].y;
+        t[2] += parts[2 * c + 1].x;
+        t[3] += parts[2 * c + 1].y;
+    }
+    for (int i = 0; i < 4; ++i) out4[i] = t[i];
+}
+
+double Fit::log_likelihood() {
+    double t[4];
+    objective_terms(t);
+    return (t[0] - t[1]) + ll_fixed;
+}
+
+double Fit::objective(int conv) {
+    double t[4];
+    objective_terms(t);
+    const double ll = (t[0] - t[1]) + ll_fixed;
+    if (conv == C_GRADIENT) return t[2];
+    if (conv == C_MITTAL) return ll;
+    return ll + t[3];
+}
+
+void Fit::gradient_hessian(int j, double* g, double* h) {
+    check_lazy();
+    IndepParams P = params();
+    check_cuda(launch_indep_gh(P, j, m->entries(j), gh_parts, kGhParts, gh_out, stream), "gh");
+    double2 r;
+    check_cuda(cudaMemcpyAsync(&r, gh_out, sizeof(double2), cudaMemcpyDeviceToHost, stream), "gh copy");
+    check_cuda(cudaStreamSynchronize(stream), "gh sync");
+    *g = r.x;
+    *h = r.y;
+}
+
+void Fit::update_xbeta(int j, double delta) {
+    check_lazy();
+    beta_h[j] += delta;
+    check_cuda(cudaMemcpyAsync(beta + j, &beta_h[j], sizeof(double), cudaMemcpyHostToDevice, stream),
+               "beta j");
+    IndepParams P = params();
+    check_cuda(launch_indep_update(P, j, m->fmt[j], m->entries(j), delta, stream), "update");
+    check_cuda(cudaStreamSynchronize(stream), "update sync");
+}
+
+// findMode (CyclicCoordinateDescent.cpp:909-1216), CCD algorithm.
+void Fit::find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* iters,
+                         double* obj, float* ms) {
+    if (!valid_weights || touched_y) {
+        apply_weights();
+        touched_y = false;
+    }
+    if (!xb_known) compute_xbeta();
+    if (!suff_known) remaining_statistics();
+    std::vector<double> hd(J, bound);  // resetBounds
+    check_cuda(cudaMemcpyAsync(hdelta, hd.data(), sizeof(double) * J, cudaMemcpyHostToDevice, stream),
+               "bounds");
+    if (a.per_coordinate) {
+        // the reference's call pattern: one host round trip per coordinate
+        double last = objective(a.convergence_type);
+        int iteration = 0;
+        bool done = false;
+        auto t0 = std::chrono::steady_clock::now();
+        while (!done) {
+            for (int j = 0; j < J; ++j) {
+                if (fixed[j]) continue;
+                double g, h;
+                gradient_hessian(j, &g, &h);
+                double delta = newton_prior_delta(g, h, beta_h[j], ptype_h[j], pvar_h[j]);
+                delta = apply_bounds(delta, hd[j]);
+                if (delta != 0.0) update_xbeta(j, delta);
+            }
+            ++iteration;
+            const double cur = objective(a.convergence_type);
+            double conv;
+            bool ill = false;
+            if (cur != cur) {
+                conv = 0.0;
+                ill = true;
+            } else {
+                conv = std::fabs(cur - last) / (std::fabs(cur) + 1.0);
+            }
+            last = cur;
+            if (a.tolerance > 0 && conv < a.tolerance) {
+                *flag = ill ? R_ILLCONDITIONED : R_SUCCESS;
+                done = true;
+            } else if (iteration == a.max_iterations) {
+                *flag = R_MAX_ITERATIONS;
+                done = true;
+            }
+        }
+        *iters = iteration;
+        *obj = last;
+        *ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        check_cuda(cudaMemcpyAsync(hdelta, hd.data(), sizeof(double) * J, cudaMemcpyHostToDevice, stream),
+                   "bounds");
+        return;
+    }
+    ensure_schedule();
+    if (sched->host.n_levels == 0) {
+        // every coordinate is fixed: each cycle changes nothing, so the first
+        // convergence check sees conv = 0 (findMode with an empty cycle)
+        *obj = objective(a.convergence_type);
+        *flag = (*obj != *obj) ? R_ILLCONDITIONED
+                : (a.tolerance > 0 ? R_SUCCESS : (a.max_iterations == 1 ? R_MAX_ITERATIONS : R_SUCCESS));
+        *iters = 1;
+        *ms = 0.f;
+        return;
+    }
+    DevStatus zero{};
+    zero.flag = R_FAIL;
+    check_cuda(cudaMemcpyAsync(st, &zero, sizeof(zero), cudaMemcpyHostToDevice, stream), "status");
+    check_cuda(cudaMemsetAsync(sched->level_done, 0, sizeof(unsigned) * std::max(1, sched->host.n_levels), stream), "reset");
+    check_cuda(cudaMemsetAsync(sched->col_arrive, 0, sizeof(unsigned) * std::max(1, J), stream), "reset");
+    check_cuda(cudaMemsetAsync(grid_bar, 0, sizeof(unsigned), stream), "reset");
+    IndepParams P = params();
+    P.conv = a.convergence_type;
+    P.tol = a.tolerance;
+    P.max_iter = a.max_iterations;
+    check_cuda(cudaEventRecord(ev0, stream), "event");
+    check_cuda(launch_indep_sweep(P, sched->host.n_cta, stream), "sweep launch");
+    check_cuda(cudaEventRecord(ev1, stream), "event");
+    DevStatus out{};
+    check_cuda(cudaMemcpyAsync(&out, st, sizeof(out), cudaMemcpyDeviceToHost, stream), "status");
+    check_cuda(cudaStreamSynchronize(stream), "sweep");
+    check_cuda(cudaEventElapsedTime(ms, ev0, ev1), "elapsed");
+    if (out.error != E_NONE)
+        throw Error(CCDB_ERR_TIMEOUT, "device wait timed out (code " + std::to_string(out.error) +
+                                          " at " + std::to_string(out.error_where) + ")");
+    *flag = out.flag;
+    *iters = out.iterations;
+    *obj = out.objective;
+    beta_dirty_host = true;
+}
+
+void Fit::find_mode(const ccdb_mode_args& a, double* beta_inout, ccdb_fit_result* res) {
+    if (!a.prior_type || !a.prior_var) throw Error(CCDB_ERR_INVALID, "prior arrays are required");
+    ptype_h.assign(a.prior_type, a.prior_type + J);
+    pvar_h.assign(a.prior_var, a.prior_var + J);
+    for (int j = 0; j < J; ++j)
+        if (ptype_h[j] < 0 || ptype_h[j] > 2) throw Error(CCDB_ERR_UNSUPPORTED, "prior type");
+    check_cuda(cudaMemcpyAsync(ptype, ptype_h.data(), sizeof(int32_t) * J, cudaMemcpyHostToDevice, stream), "prior");
+    check_cuda(cudaMemcpyAsync(pvar, pvar_h.data(), sizeof(double) * J, cudaMemcpyHostToDevice, stream), "prior");
+    if (a.convergence_type < C_GRADIENT || a.convergence_type > C_MITTAL)
+        throw Error(CCDB_ERR_UNSUPPORTED, "convergence type");
+    if (beta_inout) {
+        for (int j = 0; j < J; ++j) beta_h[j] = beta_inout[j];
+        upload_beta();
+        xb_known = false;
+        suff_known = false;
+    }
+    int active = 0;
+    for (int j = 0; j < J; ++j) active += fixed[j] ? 0 : 1;
+    double bound = a.initial_bound;
+    int count = 0, flag = R_FAIL, iters = 0;
+    double obj = 0.0, secs = 0.0;
+    int64_t updates = 0;
+    for (;;) {
+        float ms = 0.f;
+        find_mode_once(a, bound, &flag, &iters, &obj, &ms);
+        secs += ms * 1e-3;
+        updates += (int64_t)iters * active;
+        ++count;
+        if (beta_dirty_host) {
+            download_beta();
+            beta_dirty_host = false;
+        }
+        if (flag == R_ILLCONDITIONED && count < a.max_bound_count) {
+            bound /= 10.0;  // resetBeta (.cpp:256-264)
+            for (int j = offset_col0 ? 1 : 0; j < J; ++j) beta_h[j] = 0.0;
+            upload_beta();
+            compute_xbeta();
+            suff_known = false;
+        } else {
+            break;
+        }
+    }
+    if (beta_inout)
+        for (int j = 0; j < J; ++j) beta_inout[j] = beta_h[j];
+    if (res) {
+        res->return_flag = flag;
+        res->iterations = iters;
+        res->objective = obj;
+        res->log_likelihood = log_likelihood();
+        res->coordinate_updates = updates;
+        res->device_seconds = secs;
+    }
+}
+
+}  // namespace ccdb
+
+// ====================================================================== C ABI
+using namespace ccdb;
+
+struct ccdb_context : Context {};
+struct ccdb_matrix : Matrix {};
+struct ccdb_fit : Fit {};
+
+namespace {
+
+template <typename F>
+int guard(F&& f) {
+    try {
+        f();
+        return CCDB_OK;
+    } catch (const Error& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return CCDB_ERR_INVALID;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return CCDB_ERR_INVALID;
+    }
+}
+
+void require(bool ok, const char* msg) {
+    if (!ok) throw Error(CCDB_ERR_INVALID, msg);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ccdb_last_error(void) { return g_last_error.c_str(); }
+
+int ccdb_context_create(int device, size_t hbm_budget_bytes, ccdb_context** out) {
+    return guard([&] {
+        require(out != nullptr, "out is NULL");
+        int n = 0;
+        check_cuda(cudaGetDeviceCount(&n), "cudaGetDeviceCount");
+        require(device >= 0 && device < n, "no such CUDA device");
+        check_cuda(cudaSetDevice(device), "cudaSetDevice");
+        auto* c = new ccdb_context();
+        c->device = device;
+        c->budget = hbm_budget_bytes;
+        check_cuda(cudaDeviceGetAttribute(&c->n_sm, cudaDevAttrMultiProcessorCount, device), "attr");
+        int coop = 0;
+        check_cuda(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device), "attr");
+        if (!coop) {
+            delete c;
+            throw Error(CCDB_ERR_UNSUPPORTED, "device lacks cooperative launch");
+        }
+        check_cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream");
+        *out = c;
+    });
+}
+
+int ccdb_context_destroy(ccdb_context* ctx) {
+    return guard([&] {
+        if (!ctx) return;
+        cudaSetDevice(ctx->device);
+        cudaStreamSynchronize(ctx->stream);
+        cudaStreamDestroy(ctx->stream);
+        delete ctx;
+    });
+}
+
+int ccdb_context_memory(const ccdb_context* ctx, size_t* bytes) {
+    return guard([&] {
+        require(ctx && bytes, "NULL argument");
+        *bytes = ctx->in_use;
+    });
+}
+
+int ccdb_matrix_create(ccdb_context* ctx, int64_t K, int32_t J, const int64_t* col_start,
+                       const int32_t* rows, const int64_t* val_start, const double* vals,
+                       const uint8_t* fmt, ccdb_matrix** out) {
+    return guard([&] {
+        require(ctx && out && col_start && val_start && fmt, "NULL argument");
+        require(K > 0 && K < (int64_t(1) << 31) && J > 0, "bad dimensions");
+        check_cuda(cudaSetDevice(ctx->device), "cudaSetDevice");
+        std::unique_ptr<ccdb_matrix> m(new ccdb_matrix());
+        m->ctx = ctx;
+        m->K = K;
+        m->J = J;
+        m->col_start.assign(col_start, col_start + J + 1);
+        m->val_start.assign(val_start, val_start + J + 1);
+        m->fmt.assign(fmt, fmt + J);
+        const int64_t nnz = col_start[J], nv = val_start[J];
+        require(col_start[0] == 0 && val_start[0] == 0 && nnz >= 0 && nv >= 0, "bad offsets");
+        require(nnz == 0 || rows, "rows is NULL");
+        require(nv == 0 || vals, "vals is NULL");
+        for (int j = 0; j < J; ++j) {
+            const int64_t nr = col_start[j + 1] - col_start[j], nvj = val_start[j + 1] - val_start[j];
+            require(nr >= 0 && nvj >= 0, "offsets must be non-decreasing");
+            switch (fmt[j]) {
+            case F_DENSE: require(nr == 0 && nvj == K, "DENSE column needs K values, no rows"); break;
+            case F_INTERCEPT: require(nr == 0 && nvj == 0, "INTERCEPT column takes no data"); break;
+            case F_INDICATOR: require(nvj == 0, "INDICATOR column takes no values"); break;
+            case F_SPARSE: require(nvj == nr, "SPARSE column needs one value per row"); break;
+            default: require(false, "unknown column format");
+            }
+            int32_t last = -1;
+            for (int64_t p = col_start[j]; p < col_start[j + 1]; ++p) {
+                require(rows[p] > last && rows[p] < K, "row ids must be ascending and < K");
+                last = rows[p];
+            }
+        }
+        m->rows_h.assign(rows, rows + nnz);
+        m->vals_h.assign(vals, vals + nv);
+        cudaStream_t s = ctx->stream;
+        m->d_col_ptr = upload(ctx, col_start, J + 1, s);
+        m->d_val_ptr = upload(ctx, val_start, J + 1, s);
+        m->d_fmt = upload(ctx, fmt, J, s);
+        m->d_rows = upload(ctx, rows, nnz, s);
+        m->d_vals = upload(ctx, vals, nv, s);
+        check_cuda(cudaStreamSynchronize(s), "matrix upload");
+        *out = m.release();
+    });
+}
+
+int ccdb_matrix_destroy(ccdb_matrix* m) {
+    return guard([&] { delete m; });
+}
+
+int ccdb_fit_create(ccdb_context* ctx, const ccdb_matrix* m, const ccdb_fit_desc* d, ccdb_fit** out) {
+    return guard([&] {
+        require(ctx && m && d && out && d->y, "NULL argument");
+        require(m->ctx == ctx, "matrix belongs to another context");
+        if (d->model_type != M_LOGISTIC && d->model_type != M_POISSON)
+            throw Error(CCDB_ERR_UNSUPPORTED, "model type not supported by this engine");
+        if (d->precision != CCDB_PRECISION_FP64)
+            throw Error(CCDB_ERR_UNSUPPORTED, "precision not supported for this model");
+        check_cuda(cudaSetDevice(ctx->device), "cudaSetDevice");
+        std::unique_ptr<ccdb_fit> f(new ccdb_fit());
+        f->ctx = ctx;
+        f->m = m;
+        f->model = d->model_type;
+        f->precision = d->precision;
+        f->K = m->K;
+        f->J = m->J;
+        f->offset_col0 = d->offset_col0 != 0;
+        f->stream = ctx->stream;
+        f->y_h.assign(d->y, d->y + m->K);
+        const int64_t K = m->K;
+        const int J = m->J;
+        f->row = static_cast<double2*>(ctx->alloc(sizeof(double2) * 2 * K));
+        f->y = upload(ctx, d->y, K, f->stream);
+        f->beta = static_cast<double*>(ctx->alloc(sizeof(double) * J));
+        f->hdelta = static_cast<double*>(ctx->alloc(sizeof(double) * J));
+        f->xjy = static_cast<double*>(ctx->alloc(sizeof(double) * J));
+        f->ptype = static_cast<int32_t*>(ctx->alloc(sizeof(int32_t) * J));
+        f->pvar = static_cast<double*>(ctx->alloc(sizeof(double) * J));
+        f->st = static_cast<DevStatus*>(ctx->alloc(sizeof(DevStatus)));
+        f->grid_bar = static_cast<unsigned*>(ctx->alloc(sizeof(unsigned)));
+        f->red = static_cast<double2*>(ctx->alloc(sizeof(double2) * 4 * ctx->n_sm * 2));
+        f->xb_tmp = static_cast<double*>(ctx->alloc(sizeof(double) * K));
+        f->w = static_cast<double*>(ctx->alloc(sizeof(double) * K));
+        f->gh_parts = static_cast<double2*>(ctx->alloc(sizeof(double2) * Fit::kGhParts));
+        f->gh_out = static_cast<double2*>(ctx->alloc(sizeof(double2)));
+        check_cuda(cudaEventCreate(&f->ev0), "event");
+        check_cuda(cudaEventCreate(&f->ev1), "event");
+        // CyclicCoordinateDescent::init (.cpp:200-239)
+        f->beta_h.assign(J, 0.0);
+        f->fixed.assign(J, 0);
+        f->ptype_h.assign(J, 0);
+        f->pvar_h.assign(J, 1.0);
+        if (f->offset_col0) {
+            f->beta_h[0] = 1.0;
+            f->fixed[0] = 1;
+            f->xb_known = false;
+        } else {
+            f->xb_known = false;  // xBeta = 0: computed (zero-filled) on first use
+        }
+        f->upload_beta();
+        check_cuda(cudaStreamSynchronize(f->stream), "fit upload");
+        *out = f.release();
+    });
+}
+
+int ccdb_fit_destroy(ccdb_fit* f) {
+    return guard([&] { delete f; });
+}
+
+int ccdb_set_weights(ccdb_fit* f, const double* w) {
+    return guard([&] {
+        require(f != nullptr, "NULL fit");
+        if (w) {
+            f->w_h.assign(w, w + f->K);
+            f->weighted = true;
+        } else {
+            f->w_h.clear();
+            f->weighted = false;
+        }
+        f->valid_weights = false;
+        f->suff_known = false;
+    });
+}
+
+int ccdb_set_beta(ccdb_fit* f, const double* beta) {
+    return guard([&] {
+        require(f && beta, "NULL argument");
+        f->beta_h.assign(beta, beta + f->J);
+        f->upload_beta();
+        f->xb_known = false;
+        f->suff_known = false;
+    });
+}
+
+int ccdb_compute_gradient_hessian(ccdb_fit* f, int32_t j, double* g, double* h) {
+    return guard([&] {
+        require(f && g && h, "NULL argument");
+        require(j >= 0 && j < f->J, "column out of range");
+        f->gradient_hessian(j, g, h);
+    });
+}
+
+int ccdb_update_xbeta(ccdb_fit* f, int32_t j, double delta) {
+    return guard([&] {
+        require(f != nullptr, "NULL fit");
+        require(j >= 0 && j < f->J, "column out of range");
+        f->update_xbeta(j, delta);
+    });
+}
+
+int ccdb_compute_remaining_statistics(ccdb_fit* f) {
+    return guard([&] {
+        require(f != nullptr, "NULL fit");
+        f->check_lazy();
+        f->remaining_statistics();
+        check_cuda(cudaStreamSynchronize(f->stream), "sync");
+    });
+}
+
+int ccdb_get_log_likelihood(ccdb_fit* f, double* ll) {
+    return guard([&] {
+        require(f && ll, "NULL argument");
+        *ll = f->log_likelihood();
+    });
+}
+
+int ccdb_get_xbeta(ccdb_fit* f, double* out) {
+    return guard([&] {
+        require(f && out, "NULL argument");
+        f->check_lazy();
+        std::vector<double2> r(2 * f->K);
+        check_cuda(cudaMemcpyAsync(r.data(), f->row, sizeof(double2) * 2 * f->K, cudaMemcpyDeviceToHost,
+                                   f->stream), "xbeta copy");
+        check_cuda(cudaStreamSynchronize(f->stream), "sync");
+        for (int64_t k = 0; k < f->K; ++k) out[k] = r[2 * k].x;
+    });
+}
+
+int ccdb_get_beta(ccdb_fit* f, double* out) {
+    return guard([&] {
+        require(f && out, "NULL argument");
+        std::copy(f->beta_h.begin(), f->beta_h.end(), out);
+    });
+}
+
+int ccdb_find_mode(ccdb_fit* f, const ccdb_mode_args* args, double* beta_inout, ccdb_fit_result* res) {
+    return guard([&] {
+        require(f && args, "NULL argument");
+        check_cuda(cudaSetDevice(f->ctx->device), "cudaSetDevice");
+        f->find_mode(*args, beta_inout, res);
+    });
+}
+
+int ccdb_fit_model(ccdb_context* ctx, int64_t K, int32_t J, const int64_t* col_start, const int32_t* rows,
+                   const int64_t* val_start, const double* vals, const uint8_t* fmt,
+                   const ccdb_fit_desc* desc, const double* weights, const ccdb_mode_args* args,
+                   double* beta_out, ccdb_fit_result* result) {
+    ccdb_matrix* m = nullptr;
+    ccdb_fit* f = nullptr;
+    int rc = ccdb_matrix_create(ctx, K, J, col_start, rows, val_start, vals, fmt, &m);
+    if (rc == CCDB_OK) rc = ccdb_fit_create(ctx, m, desc, &f);
+    if (rc == CCDB_OK && weights) rc = ccdb_set_weights(f, weights);
+    if (rc == CCDB_OK) rc = ccdb_find_mode(f, args, nullptr, result);
+    if (rc == CCDB_OK && beta_out) rc = ccdb_get_beta(f, beta_out);
+    std::string err = g_last_error;
+    if (f) ccdb_fit_destroy(f);
+    if (m) ccdb_matrix_destroy(m);
+    g_last_error = err;
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,129 @@
+// engine.h -- host-side objects behind the C ABI: a device context with an
+// HBM budget, an immutable device CompressedDataMatrix, and per-fit state
+// mirroring ModelSpecifics + CyclicCoordinateDescent.
+#pragma once
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/ccdb.h"
+#include "indep.h"
+#include "schedule.h"
+#include "step.h"
+
+namespace ccdb {
+
+void check_cuda(cudaError_t e, const char* what);
+
+struct Context {
+    int device = 0;
+    int n_sm = 0;
+    size_t budget = 0;
+    size_t in_use = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    std::map<void*, size_t> sizes;
+
+    void* alloc(size_t bytes);
+    void release(void* p);
+};
+
+struct Matrix {
+    Context* ctx = nullptr;
+    int64_t K = 0;
+    int32_t J = 0;
+    std::vector<int64_t> col_start, val_start;
+    std::vector<uint8_t> fmt;
+    std::vector<int32_t> rows_h;
+    std::vector<double> vals_h;
+    int64_t* d_col_ptr = nullptr;
+    int32_t* d_rows = nullptr;
+    int64_t* d_val_ptr = nullptr;
+    double* d_vals = nullptr;
+    uint8_t* d_fmt = nullptr;
+    // row-major copy, built on first need (computeXBeta with nonzero beta)
+    int64_t* d_row_ptr = nullptr;
+    int32_t* d_csr_col = nullptr;
+    double* d_csr_val = nullptr;
+
+    int64_t entries(int j) const;
+    void ensure_csr(cudaStream_t s);
+    ~Matrix();
+};
+
+struct DevSchedule {
+    std::vector<uint8_t> fixed;
+    Schedule host;
+    Seg* segs = nullptr;
+    int64_t* cta_seg = nullptr;
+    Task* tasks = nullptr;
+    int32_t* level_need = nullptr;
+    unsigned* level_done = nullptr;
+    unsigned* col_arrive = nullptr;
+    double2* partials = nullptr;
+};
+
+struct Fit {
+    static constexpr int kGhParts = 1024;
+    Context* ctx = nullptr;
+    const Matrix* m = nullptr;
+    int model = 0, precision = 0;
+    int64_t K = 0;
+    int32_t J = 0;
+    bool offset_col0 = false;
+    cudaStream_t stream = nullptr;
+    long long wait_limit_ns = 20LL * 1000 * 1000 * 1000;
+
+    // device state
+    double2* row = nullptr;
+    double* y = nullptr;
+    double* beta = nullptr;
+    double* hdelta = nullptr;
+    double* xjy = nullptr;
+    int32_t* ptype = nullptr;
+    double* pvar = nullptr;
+    DevStatus* st = nullptr;
+    unsigned* grid_bar = nullptr;
+    double2* red = nullptr;
+    double* xb_tmp = nullptr;
+    double* w = nullptr;
+    double2* gh_parts = nullptr;
+    double2* gh_out = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::unique_ptr<DevSchedule> sched;
+
+    // host mirror and lazy flags (CyclicCoordinateDescent.h:152-166)
+    std::vector<double> y_h, w_h, beta_h, pvar_h;
+    std::vector<int32_t> ptype_h;
+    std::vector<uint8_t> fixed;
+    bool weighted = false;
+    bool valid_weights = false, xb_known = false, suff_known = false, touched_y = true;
+    bool xb_pending = false, beta_dirty_host = false;
+    double ll_fixed = 0.0;
+
+    ~Fit();
+    IndepParams params() const;
+    void release_schedule();
+    void ensure_schedule();
+    void apply_weights();
+    void compute_xbeta();
+    void remaining_statistics();
+    void check_lazy();
+    void upload_beta();
+    void download_beta();
+    void objective_terms(double* out4);
+    double log_likelihood();
+    double objective(int conv);
+    void gradient_hessian(int j, double* g, double* h);
+    void update_xbeta(int j, double delta);
+    void find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* iters, double* obj,
+                        float* ms);
+    void find_mode(const ccdb_mode_args& a, double* beta_inout, ccdb_fit_result* res);
+};
+
+}  // namespace ccdb

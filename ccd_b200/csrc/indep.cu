@@ -1,0 +1,527 @@
+// indep.cu -- coordinate descent for models with independent rows
+// (LogisticRegression, PoissonRegression: IndependentData in
+// src/cyclops/engine/ModelSpecifics.h:383-395).
+//
+// Row state lives in HBM as two 16-byte words per row, {xBeta, offsExpXBeta}
+// and {denominator, weight}, so a gathered row is one 32-byte sector fetched
+// with two 128-bit loads.  The fused sweep kernel is persistent and
+// cooperative: each CTA walks its own list of (dependency level, tasks); a task
+// reduces the gradient/Hessian of one column (warp, CTA, or a chunk of a long
+// column), applies the Newton/prior/bound step on the device and scatters the
+// update into xBeta, exp(xBeta) and the denominators.  Levels are ordered by
+// per-level arrival counters; the convergence objective is reduced on the
+// device after each sweep, so a whole findMode is one launch.
+//
+// Arithmetic follows the reference's per-entry expressions operation by
+// operation (the file is compiled with -fmad=false so no product is fused
+// into a sum); only the order of the column reductions differs (a fixed,
+// deterministic tree instead of a serial loop).
+#include <cstdint>
+
+#include "common.cuh"
+#include "indep.h"
+
+namespace ccdb {
+
+namespace {
+
+constexpr int kThreads = 512;
+constexpr int kWarps = kThreads / 32;
+constexpr int kMaxSplit = 64;
+
+template <int FMT>
+__device__ __forceinline__ int64_t entry_row(const int32_t* rows, int64_t cb, int64_t p) {
+    if (FMT == F_SPARSE || FMT == F_INDICATOR) return (int64_t)__ldg(rows + cb + p);
+    return p;
+}
+template <int FMT>
+__device__ __forceinline__ double entry_val(const double* vals, int64_t vb, int64_t p) {
+    if (FMT == F_SPARSE || FMT == F_DENSE) return __ldg(vals + vb + p);
+    return 1.0;
+}
+
+// Gradient/Hessian contributions of entries [p0,p1) of column j, strided by
+// nthr: ModelSpecifics.hpp:1022-1038 with Logistic::incrementGradientAndHessian
+// (ModelSpecifics.h:541-568) or PoissonRegression's (ModelSpecifics.h:1509-1543).
+// Unweighted fits carry weight 1.0, which leaves every product bit-identical.
+template <int MODEL, int FMT>
+__device__ __forceinline__ void gh_range(const IndepParams& P, int j, int64_t p0, int64_t p1, int tid,
+                                         int nthr, double& g, double& h) {
+    const int64_t cb = P.col_ptr[j], vb = P.val_ptr[j];
+    constexpr bool ind = (FMT == F_INDICATOR || FMT == F_INTERCEPT);
+#pragma unroll 4
+    for (int64_t p = p0 + tid; p < p1; p += nthr) {
+        const int64_t k = entry_row<FMT>(P.rows, cb, p);
+        const double x = entry_val<FMT>(P.vals, vb, p);
+        const double2 a = __ldcg(P.row + 2 * k);      // {xBeta, offsExpXBeta}
+        const double2 b = __ldcg(P.row + 2 * k + 1);  // {denominator, weight}
+        const double n1 = a.y * x;
+        if (MODEL == M_LOGISTIC) {
+            const double gg = n1 / b.x;
+            g += b.y * gg;
+            if (ind) h += b.y * gg * (1.0 - gg);
+            else h += b.y * ((n1 * x) / b.x - gg * gg);
+        } else {
+            if (ind) {
+                const double v = b.y * n1;
+                g += v;
+                h += v;
+            } else {
+                g += b.y * n1;
+                h += b.y * (n1 * x);
+            }
+        }
+    }
+}
+
+// updateXBetaImpl for independent rows (ModelSpecifics.hpp:1561-1571):
+// xBeta += delta*x; offsExpXBeta = exp(xBeta); denom += new - old.
+template <int FMT>
+__device__ __forceinline__ void update_range(const IndepParams& P, int j, int64_t p0, int64_t p1,
+                                             int tid, int nthr, double delta) {
+    const int64_t cb = P.col_ptr[j], vb = P.val_ptr[j];
+#pragma unroll 4
+    for (int64_t p = p0 + tid; p < p1; p += nthr) {
+        const int64_t k = entry_row<FMT>(P.rows, cb, p);
+        const double x = entry_val<FMT>(P.vals, vb, p);
+        const double2 a = __ldcg(P.row + 2 * k);
+        const double2 b = __ldcg(P.row + 2 * k + 1);
+        const double xb = a.x + delta * x;
+        const double en = exp(xb);
+        const double dn = b.x + (en - a.y);
+        __stcg(P.row + 2 * k, make_double2(xb, en));
+        __stcg(P.row + 2 * k + 1, make_double2(dn, b.y));
+    }
+}
+
+template <int MODEL>
+__device__ __forceinline__ void gh_dispatch(const IndepParams& P, int j, uint8_t f, int64_t p0,
+                                            int64_t p1, int tid, int nthr, double& g, double& h) {
+    switch (f) {
+    case F_INDICATOR: gh_range<MODEL, F_INDICATOR>(P, j, p0, p1, tid, nthr, g, h); break;
+    case F_SPARSE: gh_range<MODEL, F_SPARSE>(P, j, p0, p1, tid, nthr, g, h); break;
+    case F_DENSE: gh_range<MODEL, F_DENSE>(P, j, p0, p1, tid, nthr, g, h); break;
+    default: gh_range<MODEL, F_INTERCEPT>(P, j, p0, p1, tid, nthr, g, h); break;
+    }
+}
+
+__device__ __forceinline__ void update_dispatch(const IndepParams& P, int j, uint8_t f, int64_t p0,
+                                                int64_t p1, int tid, int nthr, double delta) {
+    switch (f) {
+    case F_INDICATOR: update_range<F_INDICATOR>(P, j, p0, p1, tid, nthr, delta); break;
+    case F_SPARSE: update_range<F_SPARSE>(P, j, p0, p1, tid, nthr, delta); break;
+    case F_DENSE: update_range<F_DENSE>(P, j, p0, p1, tid, nthr, delta); break;
+    default: update_range<F_INTERCEPT>(P, j, p0, p1, tid, nthr, delta); break;
+    }
+}
+
+// (g, h) of a whole column -> delta; writes beta[j] and hDelta[j].
+// Empty columns give (0, 0) (ModelSpecifics.hpp:720-723).
+__device__ __forceinline__ double column_step(const IndepParams& P, int j, int64_t entries,
+                                              double gsum, double hsum, double beta, double hd,
+                                              bool write) {
+    double g = 0.0, h = 0.0;
+    if (entries > 0) {
+        g = gsum - P.xjy[j];
+        h = hsum;
+    }
+    double delta = newton_prior_delta(g, h, beta, P.ptype[j], P.pvar[j]);
+    delta = apply_bounds(delta, hd);
+    if (write) {
+        P.hdelta[j] = hd;
+        if (delta != 0.0) P.beta[j] = beta + delta;
+    }
+    return delta;
+}
+
+// Objective terms of the current state: {LL numerator, LL denominator,
+// gradient objective, log prior} (ModelSpecifics.hpp:103-120, 605-650;
+// JointPrior.h:121-128), reduced over the grid into red[buf*G + cta].
+template <int MODEL>
+__device__ void objective_partials(const IndepParams& P, int buf, double4* s_red4) {
+    double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
+    const int64_t G = gridDim.x, b = blockIdx.x;
+    const int64_t k0 = P.K * b / G, k1 = P.K * (b + 1) / G;
+    for (int64_t k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+        const double2 a = __ldcg(P.row + 2 * k);
+        const double2 dw = __ldcg(P.row + 2 * k + 1);
+        const double yk = P.y[k];
+        acc.x += (double)((int)yk) * a.x * dw.y;
+        if (MODEL == M_LOGISTIC) acc.y += dw.y * log(dw.x);
+        else acc.y += dw.y * dw.x;
+        acc.z += a.x * yk * dw.y;
+    }
+    const int64_t j0 = (int64_t)P.J * b / G, j1 = (int64_t)P.J * (b + 1) / G;
+    for (int64_t j = j0 + threadIdx.x; j < j1; j += blockDim.x)
+        acc.w += log_prior_one(__ldcg(P.beta + j), P.ptype[j], P.pvar[j]);
+    acc = block_sum4<kWarps>(acc, s_red4);
+    if (threadIdx.x == 0) {
+        __stcg(P.red + 2 * (buf * G + b), make_double2(acc.x, acc.y));
+        __stcg(P.red + 2 * (buf * G + b) + 1, make_double2(acc.z, acc.w));
+    }
+}
+
+__device__ __forceinline__ double4 objective_total(const IndepParams& P, int buf) {
+    double4 t = make_double4(0.0, 0.0, 0.0, 0.0);
+    for (int c = 0; c < (int)gridDim.x; ++c) {
+        const double2 u = __ldcg(P.red + 2 * (buf * gridDim.x + c));
+        const double2 v = __ldcg(P.red + 2 * (buf * gridDim.x + c) + 1);
+        t.x += u.x;
+        t.y += u.y;
+        t.z += v.x;
+        t.w += v.y;
+    }
+    return t;
+}
+
+__device__ __forceinline__ double objective_of(const IndepParams& P, double4 t, double& ll) {
+    ll = (t.x - t.y) + P.ll_fixed;
+    if (P.conv == C_GRADIENT) return t.z;
+    if (P.conv == C_MITTAL) return ll;
+    return ll + t.w;
+}
+
+template <int MODEL>
+__global__ void __launch_bounds__(kThreads, 1) indep_sweep_kernel(IndepParams P) {
+    __shared__ double4 s_red4[kWarps];
+    __shared__ double2 s_red2[kWarps];
+    __shared__ double2 s_stash[kMaxSplit];  // {beta, hDelta} of split columns, read before arrival
+    __shared__ double s_delta;
+    __shared__ int32_t s_fail;
+    __shared__ int32_t s_done;
+
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    unsigned epoch = 0;
+    const int64_t seg0 = P.cta_seg[blockIdx.x], seg1 = P.cta_seg[blockIdx.x + 1];
+
+    // initial objective (findMode: lastObjFunc before the first cycle)
+    objective_partials<MODEL>(P, 0, s_red4);
+    if (!grid_barrier(P.grid_bar, epoch, P.wait_limit_ns, P.st, &s_fail)) return;
+    double last = 0.0;
+    if (tid == 0) {
+        double ll;
+        last = objective_of(P, objective_total(P, 0), ll);
+    }
+
+    int iteration = 0;
+    for (int it = 0; it < P.max_iter; ++it) {
+        for (int64_t si = seg0; si < seg1; ++si) {
+            const Seg sg = P.segs[si];
+            if (sg.level > 0) {
+                if (tid == 0) {
+                    const unsigned target = (unsigned)(it + 1) * (unsigned)P.level_need[sg.level - 1];
+                    s_fail = wait_geq(P.level_done + sg.level - 1, target, P.wait_limit_ns, P.st,
+                                      E_WAIT_LEVEL, sg.level) ? 0 : 1;
+                }
+                __syncthreads();
+                if (s_fail) return;
+            }
+            const Task* T = P.tasks + sg.t0;
+            // phase 1: partial sums of split columns, published without waiting
+            for (int q = 0; q < sg.n_chunk; ++q) {
+                const Task t = T[q];
+                const uint8_t f = P.fmt[t.col];
+                double g = 0.0, h = 0.0;
+                gh_dispatch<MODEL>(P, t.col, f, t.p0, t.p1, tid, blockDim.x, g, h);
+                const double2 s = block_sum2<kWarps>(make_double2(g, h), s_red2);
+                if (tid == 0) {
+                    s_stash[q] = make_double2(__ldcg(P.beta + t.col), __ldcg(P.hdelta + t.col));
+                    __stcg(P.partials + t.part_base + t.chunk, s);
+                    __threadfence();
+                    atomicAdd(P.col_arrive + t.col, 1u);
+                }
+            }
+            // phase 2a: whole-CTA columns
+            for (int q = sg.n_chunk; q < sg.n_chunk + sg.n_cta; ++q) {
+                const Task t = T[q];
+                const uint8_t f = P.fmt[t.col];
+                double g = 0.0, h = 0.0;
+                gh_dispatch<MODEL>(P, t.col, f, t.p0, t.p1, tid, blockDim.x, g, h);
+                const double2 s = block_sum2<kWarps>(make_double2(g, h), s_red2);
+                if (tid == 0)
+                    s_delta = column_step(P, t.col, t.p1, s.x, s.y, __ldcg(P.beta + t.col),
+                                          __ldcg(P.hdelta + t.col), true);
+                __syncthreads();
+                const double d = s_delta;
+                if (d != 0.0) update_dispatch(P, t.col, f, t.p0, t.p1, tid, blockDim.x, d);
+                __syncthreads();
+            }
+            // phase 2b: one warp per short column
+            const int qw0 = sg.n_chunk + sg.n_cta, qw1 = qw0 + sg.n_warp;
+            for (int q = qw0; q < qw1; ++q) {
+                const Task t = T[q];
+                if (t.warp != wid) continue;
+                const uint8_t f = P.fmt[t.col];
+                double g = 0.0, h = 0.0;
+                gh_dispatch<MODEL>(P, t.col, f, t.p0, t.p1, lane, 32, g, h);
+                const double2 s = warp_sum2(make_double2(g, h));
+                double d = 0.0;
+                if (lane == 0)
+                    d = column_step(P, t.col, t.p1, s.x, s.y, __ldcg(P.beta + t.col),
+                                    __ldcg(P.hdelta + t.col), true);
+                d = __shfl_sync(0xffffffffu, d, 0);
+                if (d != 0.0) update_dispatch(P, t.col, f, t.p0, t.p1, lane, 32, d);
+            }
+            // phase 3: split columns -- combine partials, step, scatter own chunk
+            for (int q = 0; q < sg.n_chunk; ++q) {
+                const Task t = T[q];
+                if (tid == 0) {
+                    const unsigned target = (unsigned)(it + 1) * (unsigned)t.nchunks;
+                    if (!wait_geq(P.col_arrive + t.col, target, P.wait_limit_ns, P.st, E_WAIT_COLUMN,
+                                  t.col)) {
+                        s_fail = 1;
+                    } else {
+                        s_fail = 0;
+                        double2 s = make_double2(0.0, 0.0);
+                        for (int c = 0; c < t.nchunks; ++c) {
+                            const double2 v = __ldcg(P.partials + t.part_base + c);
+                            s.x += v.x;
+                            s.y += v.y;
+                        }
+                        // split columns are never empty
+                        s_delta = column_step(P, t.col, 1, s.x, s.y, s_stash[q].x,
+                                              s_stash[q].y, t.chunk == 0);
+                    }
+                }
+                __syncthreads();
+                if (s_fail) return;
+                const double d = s_delta;
+                if (d != 0.0) update_dispatch(P, t.col, P.fmt[t.col], t.p0, t.p1, tid, blockDim.x, d);
+                __syncthreads();
+            }
+            __syncthreads();
+            if (tid == 0) {
+                __threadfence();
+                atomicAdd(P.level_done + sg.level, 1u);
+            }
+        }
+        // the objective reads every row: wait until the last level is complete
+        if (tid == 0) {
+            const unsigned target = (unsigned)(it + 1) * (unsigned)P.level_need[P.n_levels - 1];
+            s_fail = wait_geq(P.level_done + P.n_levels - 1, target, P.wait_limit_ns, P.st,
+                              E_WAIT_LEVEL, P.n_levels - 1) ? 0 : 1;
+        }
+        __syncthreads();
+        if (s_fail) return;
+        const int buf = (it + 1) & 1;
+        objective_partials<MODEL>(P, buf, s_red4);
+        if (!grid_barrier(P.grid_bar, epoch, P.wait_limit_ns, P.st, &s_fail)) return;
+        iteration = it + 1;
+        if (tid == 0) {
+            double ll;
+            const double4 tot = objective_total(P, buf);
+            const double cur = objective_of(P, tot, ll);
+            double conv;
+            bool ill = false;
+            if (cur != cur) {
+                conv = 0.0;
+                ill = true;
+            } else {
+                conv = fabs(cur - last) / (fabs(cur) + 1.0);
+            }
+            last = cur;
+            int done = 0, flag = R_SUCCESS;
+            if (P.tol > 0 && conv < P.tol) {
+                flag = ill ? R_ILLCONDITIONED : R_SUCCESS;
+                done = 1;
+            } else if (iteration == P.max_iter) {
+                flag = R_MAX_ITERATIONS;
+                done = 1;
+            }
+            s_done = done;
+            if (blockIdx.x == 0) {
+                P.st->iterations = iteration;
+                P.st->objective = cur;
+                P.st->loglik = ll;
+                P.st->log_prior = tot.w;
+                if (done) P.st->flag = flag;
+            }
+        }
+        __syncthreads();
+        if (s_done) break;
+    }
+}
+
+// ---------------------------------------------------------------- per-coordinate kernels
+
+template <int MODEL>
+__global__ void __launch_bounds__(256) gh_column_kernel(IndepParams P, int j, int64_t entries,
+                                                        int64_t per_block, double2* out) {
+    __shared__ double2 s_red2[8];
+    const int64_t p0 = per_block * blockIdx.x;
+    const int64_t p1 = min(entries, p0 + per_block);
+    double g = 0.0, h = 0.0;
+    if (p0 < p1) gh_dispatch<MODEL>(P, j, P.fmt[j], p0, p1, threadIdx.x, blockDim.x, g, h);
+    const double2 s = block_sum2<8>(make_double2(g, h), s_red2);
+    if (threadIdx.x == 0) out[blockIdx.x] = s;
+}
+
+__global__ void gh_finish_kernel(const double2* parts, int n, const double* xjy, int j,
+                                 int64_t entries, double2* out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double2 s = make_double2(0.0, 0.0);
+        for (int c = 0; c < n; ++c) {
+            s.x += parts[c].x;
+            s.y += parts[c].y;
+        }
+        if (entries == 0) s = make_double2(0.0, 0.0);
+        else s.x -= xjy[j];
+        *out = s;
+    }
+}
+
+// Each thread handles entries p = tid, tid + nthr, ... of column j.
+template <int FMT>
+__global__ void update_column_grid(IndepParams P, int j, int64_t entries, double delta) {
+    const int64_t cb = P.col_ptr[j], vb = P.val_ptr[j];
+    const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < entries; p += nthr) {
+        const int64_t k = entry_row<FMT>(P.rows, cb, p);
+        const double x = entry_val<FMT>(P.vals, vb, p);
+        const double2 a = P.row[2 * k];
+        const double2 b = P.row[2 * k + 1];
+        const double xb = a.x + delta * x;
+        const double en = exp(xb);
+        const double dn = b.x + (en - a.y);
+        P.row[2 * k] = make_double2(xb, en);
+        P.row[2 * k + 1] = make_double2(dn, b.y);
+    }
+}
+
+// computeRemainingStatistics for independent rows (ModelSpecifics.hpp:1604-1613):
+// e = exp(xBeta); denom = null value (LR 1, Poisson 0) + e.  w = row weight.
+__global__ void remaining_stats_kernel(double2* row, const double* xb, const double* w, int64_t K,
+                                       double null_denom) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const double x = xb ? xb[k] : row[2 * k].x;
+        const double e = exp(x);
+        const double wk = w ? w[k] : row[2 * k + 1].y;
+        row[2 * k] = make_double2(x, e);
+        row[2 * k + 1] = make_double2(null_denom + e, wk);
+    }
+}
+
+template <int MODEL>
+__global__ void __launch_bounds__(512) objective_kernel(IndepParams P) {
+    __shared__ double4 s_red4[kWarps];
+    objective_partials<MODEL>(P, 0, s_red4);
+}
+
+__global__ void xjy_kernel(const int64_t* col_ptr, const int32_t* rows, const int64_t* val_ptr,
+                           const double* vals, const uint8_t* fmt, const double* y, const double* w,
+                           int64_t K, int32_t J, double* xjy) {
+    __shared__ double2 s_red2[8];
+    for (int j = blockIdx.x; j < J; j += gridDim.x) {
+        const uint8_t f = fmt[j];
+        const int64_t cb = col_ptr[j], vb = val_ptr[j];
+        const int64_t n = (f == F_DENSE || f == F_INTERCEPT) ? K : col_ptr[j + 1] - cb;
+        double s = 0.0;
+        for (int64_t p = threadIdx.x; p < n; p += blockDim.x) {
+            const int64_t k = (f == F_SPARSE || f == F_INDICATOR) ? rows[cb + p] : p;
+            const double x = (f == F_SPARSE || f == F_DENSE) ? vals[vb + p] : 1.0;
+            s += w ? x * y[k] * w[k] : x * y[k];
+        }
+        const double2 t = block_sum2<8>(make_double2(s, 0.0), s_red2);
+        if (threadIdx.x == 0) xjy[j] = t.x;
+    }
+}
+
+// xBeta = X beta, per row in increasing column order over the row-major copy
+// (the same sequence of additions as the column axpy loop of
+// CyclicCoordinateDescent::computeXBeta, .cpp:1452-1470).
+__global__ void xbeta_csr_kernel(const int64_t* row_ptr, const int32_t* col_idx, const double* val,
+                                 const double* beta, int64_t K, double* xb) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int64_t p = row_ptr[k]; p < row_ptr[k + 1]; ++p) {
+            const double b = beta[col_idx[p]];
+            if (b != 0.0) s += b * val[p];
+        }
+        xb[k] = s;
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- launchers
+
+int indep_threads() { return kThreads; }
+int indep_max_split() { return kMaxSplit; }
+
+cudaError_t indep_sweep_occupancy(int model, int* blocks_per_sm) {
+    if (model == M_LOGISTIC)
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm,
+                                                             indep_sweep_kernel<M_LOGISTIC>,
+                                                             kThreads, 0);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm,
+                                                         indep_sweep_kernel<M_POISSON>, kThreads, 0);
+}
+
+cudaError_t launch_indep_sweep(const IndepParams& P, int n_cta, cudaStream_t stream) {
+    void* args[] = {(void*)&P};
+    const void* fn = (P.model == M_LOGISTIC) ? (const void*)indep_sweep_kernel<M_LOGISTIC>
+                                             : (const void*)indep_sweep_kernel<M_POISSON>;
+    return cudaLaunchCooperativeKernel(fn, dim3(n_cta), dim3(kThreads), args, 0, stream);
+}
+
+cudaError_t launch_indep_gh(const IndepParams& P, int j, int64_t entries, double2* parts,
+                            int max_parts, double2* out, cudaStream_t stream) {
+    int64_t per_block = 8192;
+    int nb = (int)((entries + per_block - 1) / per_block);
+    if (nb < 1) nb = 1;
+    if (nb > max_parts) {
+        nb = max_parts;
+        per_block = (entries + nb - 1) / nb;
+    }
+    if (P.model == M_LOGISTIC)
+        gh_column_kernel<M_LOGISTIC><<<nb, 256, 0, stream>>>(P, j, entries, per_block, parts);
+    else
+        gh_column_kernel<M_POISSON><<<nb, 256, 0, stream>>>(P, j, entries, per_block, parts);
+    gh_finish_kernel<<<1, 32, 0, stream>>>(parts, nb, P.xjy, j, entries, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_indep_update(const IndepParams& P, int j, uint8_t fmt, int64_t entries,
+                                double delta, cudaStream_t stream) {
+    if (entries <= 0) return cudaSuccess;
+    int nb = (int)((entries + 255) / 256);
+    if (nb > 4096) nb = 4096;
+    switch (fmt) {
+    case F_INDICATOR: update_column_grid<F_INDICATOR><<<nb, 256, 0, stream>>>(P, j, entries, delta); break;
+    case F_SPARSE: update_column_grid<F_SPARSE><<<nb, 256, 0, stream>>>(P, j, entries, delta); break;
+    case F_DENSE: update_column_grid<F_DENSE><<<nb, 256, 0, stream>>>(P, j, entries, delta); break;
+    default: update_column_grid<F_INTERCEPT><<<nb, 256, 0, stream>>>(P, j, entries, delta); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_remaining_stats(double2* row, const double* xb, const double* w, int64_t K,
+                                   double null_denom, cudaStream_t stream) {
+    remaining_stats_kernel<<<1184, 256, 0, stream>>>(row, xb, w, K, null_denom);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_indep_objective(const IndepParams& P, int n_blocks, cudaStream_t stream) {
+    if (P.model == M_LOGISTIC) objective_kernel<M_LOGISTIC><<<n_blocks, kThreads, 0, stream>>>(P);
+    else objective_kernel<M_POISSON><<<n_blocks, kThreads, 0, stream>>>(P);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_xjy(const int64_t* col_ptr, const int32_t* rows, const int64_t* val_ptr,
+                       const double* vals, const uint8_t* fmt, const double* y, const double* w,
+                       int64_t K, int32_t J, double* xjy, cudaStream_t stream) {
+    int nb = J < 65535 ? J : 65535;
+    if (nb < 1) nb = 1;
+    xjy_kernel<<<nb, 256, 0, stream>>>(col_ptr, rows, val_ptr, vals, fmt, y, w, K, J, xjy);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_xbeta_csr(const int64_t* row_ptr, const int32_t* col_idx, const double* val,
+                             const double* beta, int64_t K, double* xb, cudaStream_t stream) {
+    xbeta_csr_kernel<<<1184, 256, 0, stream>>>(row_ptr, col_idx, val, beta, K, xb);
+    return cudaGetLastError();
+}
+
+}  // namespace ccdb

@@ -1,0 +1,69 @@
+// indep.h -- parameters and launchers of the independent-row engine (indep.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "types.h"
+
+namespace ccdb {
+
+struct IndepParams {
+    // CompressedDataMatrix on the device
+    const int64_t* col_ptr;
+    const int32_t* rows;
+    const int64_t* val_ptr;
+    const double* vals;
+    const uint8_t* fmt;
+    int64_t K;
+    int32_t J;
+    int32_t model;  // M_LOGISTIC or M_POISSON
+    // row state: row[2k] = {xBeta, offsExpXBeta}, row[2k+1] = {denominator, weight}
+    double2* row;
+    const double* y;
+    // per-column state
+    double* beta;
+    double* hdelta;
+    const double* xjy;
+    const int32_t* ptype;
+    const double* pvar;
+    // schedule
+    const Seg* segs;
+    const int64_t* cta_seg;
+    const Task* tasks;
+    int32_t n_levels;
+    int32_t max_iter;
+    unsigned* level_done;
+    const int32_t* level_need;
+    unsigned* col_arrive;
+    double2* partials;
+    unsigned* grid_bar;
+    double2* red;  // 2 buffers x n_cta x 2 double2: {LL num, LL den}, {grad obj, log prior}
+    // convergence
+    int32_t conv;
+    int32_t pad0;
+    double tol;
+    double ll_fixed;
+    DevStatus* st;
+    long long wait_limit_ns;  // bound on any single device-side wait
+};
+
+int indep_threads();
+int indep_max_split();
+cudaError_t indep_sweep_occupancy(int model, int* blocks_per_sm);
+cudaError_t launch_indep_sweep(const IndepParams& P, int n_cta, cudaStream_t stream);
+cudaError_t launch_indep_gh(const IndepParams& P, int j, int64_t entries, double2* parts,
+                            int max_parts, double2* out, cudaStream_t stream);
+cudaError_t launch_indep_update(const IndepParams& P, int j, uint8_t fmt, int64_t entries,
+                                double delta, cudaStream_t stream);
+cudaError_t launch_remaining_stats(double2* row, const double* xb, const double* w, int64_t K,
+                                   double null_denom, cudaStream_t stream);
+// one pass of the objective reduction into P.red[0 .. n_blocks) (buffer 0)
+cudaError_t launch_indep_objective(const IndepParams& P, int n_blocks, cudaStream_t stream);
+cudaError_t launch_xjy(const int64_t* col_ptr, const int32_t* rows, const int64_t* val_ptr,
+                       const double* vals, const uint8_t* fmt, const double* y, const double* w,
+                       int64_t K, int32_t J, double* xjy, cudaStream_t stream);
+cudaError_t launch_xbeta_csr(const int64_t* row_ptr, const int32_t* col_idx, const double* val,
+                             const double* beta, int64_t K, double* xb, cudaStream_t stream);
+
+}  // namespace ccdb

@@ -1,0 +1,276 @@
+"""ctypes binding of libccdb.so (the C ABI in include/ccdb.h).
+
+The objects mirror the reference's operator API: ``Fit`` exposes the
+``AbstractModelSpecifics`` calls (``compute_gradient_and_hessian``,
+``update_xbeta``, ``get_log_likelihood`` ...) and ``find_mode`` is
+``CyclicCoordinateDescent::update``.  There is no CPU fallback: if the CUDA
+library is missing or no GPU is present, constructing a ``Context`` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from .data import CyclopsData, GRADIENT
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libccdb.so")
+
+OK = 0
+ERR_INVALID, ERR_CUDA, ERR_UNSUPPORTED, ERR_BUDGET, ERR_TIMEOUT = -1, -2, -3, -4, -5
+PRECISION_FP64, PRECISION_MIXED = 0, 1
+
+
+class CcdbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"ccdb error {code}: {msg}")
+        self.code = code
+
+
+class _FitDesc(C.Structure):
+    _fields_ = [("model_type", C.c_int32), ("precision", C.c_int32), ("y", C.c_void_p),
+                ("time", C.c_void_p), ("stratum", C.c_void_p), ("offset_col0", C.c_int32)]
+
+
+class _ModeArgs(C.Structure):
+    _fields_ = [("prior_type", C.c_void_p), ("prior_var", C.c_void_p),
+                ("convergence_type", C.c_int32), ("tolerance", C.c_double),
+                ("max_iterations", C.c_int32), ("initial_bound", C.c_double),
+                ("max_bound_count", C.c_int32), ("per_coordinate", C.c_int32)]
+
+
+class _FitResult(C.Structure):
+    _fields_ = [("return_flag", C.c_int32), ("iterations", C.c_int32),
+                ("log_likelihood", C.c_double), ("objective", C.c_double),
+                ("coordinate_updates", C.c_int64), ("device_seconds", C.c_double)]
+
+
+@dataclass
+class ModeFindingArguments:
+    """CcdInterface.h:70-94 defaults."""
+    convergence_type: int = GRADIENT
+    tolerance: float = 1e-6
+    max_iterations: int = 1000
+    initial_bound: float = 2.0
+    max_bound_count: int = 5
+    per_coordinate: bool = False
+
+
+@dataclass
+class FitResult:
+    beta: np.ndarray
+    return_flag: int
+    iterations: int
+    log_likelihood: float
+    objective: float
+    coordinate_updates: int
+    device_seconds: float
+
+
+_lib = None
+
+_P = C.c_void_p
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m ccd_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        L.ccdb_last_error.restype = C.c_char_p
+        L.ccdb_context_create.argtypes = [C.c_int, C.c_size_t, C.POINTER(_P)]
+        L.ccdb_context_destroy.argtypes = [_P]
+        L.ccdb_context_memory.argtypes = [_P, C.POINTER(C.c_size_t)]
+        L.ccdb_matrix_create.argtypes = [_P, C.c_int64, C.c_int32, _P, _P, _P, _P, _P, C.POINTER(_P)]
+        L.ccdb_matrix_destroy.argtypes = [_P]
+        L.ccdb_fit_create.argtypes = [_P, _P, C.POINTER(_FitDesc), C.POINTER(_P)]
+        L.ccdb_fit_destroy.argtypes = [_P]
+        L.ccdb_set_weights.argtypes = [_P, _P]
+        L.ccdb_set_beta.argtypes = [_P, _P]
+        L.ccdb_compute_gradient_hessian.argtypes = [_P, C.c_int32, _P, _P]
+        L.ccdb_update_xbeta.argtypes = [_P, C.c_int32, C.c_double]
+        L.ccdb_compute_remaining_statistics.argtypes = [_P]
+        L.ccdb_get_log_likelihood.argtypes = [_P, _P]
+        L.ccdb_get_xbeta.argtypes = [_P, _P]
+        L.ccdb_get_beta.argtypes = [_P, _P]
+        L.ccdb_find_mode.argtypes = [_P, C.POINTER(_ModeArgs), _P, C.POINTER(_FitResult)]
+        L.ccdb_fit_model.argtypes = [_P, C.c_int64, C.c_int32, _P, _P, _P, _P, _P, C.POINTER(_FitDesc),
+                                     _P, C.POINTER(_ModeArgs), _P, C.POINTER(_FitResult)]
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != OK:
+        raise CcdbError(rc, lib().ccdb_last_error().decode(errors="replace"))
+
+
+def _p(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _c(a, dt):
+    return None if a is None else np.ascontiguousarray(a, dtype=dt)
+
+
+class Context:
+    """One GPU; ``hbm_budget`` bytes bound every allocation made through it."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        h = _P()
+        _check(lib().ccdb_context_create(device, hbm_budget, C.byref(h)))
+        self.h = h
+        self.device = device
+
+    def memory_in_use(self) -> int:
+        v = C.c_size_t()
+        _check(lib().ccdb_context_memory(self.h, C.byref(v)))
+        return v.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().ccdb_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Matrix:
+    """Device-resident CompressedDataMatrix, shared by fits."""
+
+    def __init__(self, ctx: Context, d: CyclopsData):
+        self.ctx = ctx
+        self.K, self.J = d.K, d.J
+        arrs = [_c(d.col_start, np.int64), _c(d.rows, np.int32), _c(d.val_start, np.int64),
+                _c(d.vals, np.float64), _c(d.fmt, np.uint8)]
+        h = _P()
+        _check(lib().ccdb_matrix_create(ctx.h, d.K, d.J, *[_p(a) for a in arrs], C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().ccdb_matrix_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _desc(d: CyclopsData, precision: int, keep: list) -> _FitDesc:
+    y = _c(d.y, np.float64)
+    t = _c(d.time, np.float64)
+    s = _c(d.stratum, np.int64)
+    keep += [y, t, s]
+    return _FitDesc(d.model_type, precision, _p(y), _p(t), _p(s), int(d.offset_col0))
+
+
+def _mode_args(d: CyclopsData, a: ModeFindingArguments, keep: list) -> _ModeArgs:
+    pt = _c(d.prior_type, np.int32)
+    pv = _c(d.prior_var, np.float64)
+    keep += [pt, pv]
+    return _ModeArgs(_p(pt), _p(pv), a.convergence_type, a.tolerance, a.max_iterations,
+                     a.initial_bound, a.max_bound_count, int(a.per_coordinate))
+
+
+class Fit:
+    """Per-fit device state: the B200 counterpart of ModelSpecifics<Model,Real>
+    driven by CyclicCoordinateDescent."""
+
+    def __init__(self, ctx: Context, matrix: Matrix, d: CyclopsData,
+                 precision: int = PRECISION_FP64):
+        self.ctx, self.matrix, self.d = ctx, matrix, d
+        keep = []
+        desc = _desc(d, precision, keep)
+        h = _P()
+        _check(lib().ccdb_fit_create(ctx.h, matrix.h, C.byref(desc), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().ccdb_fit_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- AbstractModelSpecifics-level calls
+    def set_weights(self, w: Optional[np.ndarray]) -> None:
+        w = _c(w, np.float64)
+        _check(lib().ccdb_set_weights(self.h, _p(w)))
+
+    def set_beta(self, beta: np.ndarray) -> None:
+        b = _c(beta, np.float64)
+        _check(lib().ccdb_set_beta(self.h, _p(b)))
+
+    def compute_gradient_and_hessian(self, j: int):
+        g, h = C.c_double(), C.c_double()
+        _check(lib().ccdb_compute_gradient_hessian(self.h, j, C.byref(g), C.byref(h)))
+        return g.value, h.value
+
+    def update_xbeta(self, j: int, delta: float) -> None:
+        _check(lib().ccdb_update_xbeta(self.h, j, delta))
+
+    def compute_remaining_statistics(self) -> None:
+        _check(lib().ccdb_compute_remaining_statistics(self.h))
+
+    def get_log_likelihood(self) -> float:
+        v = C.c_double()
+        _check(lib().ccdb_get_log_likelihood(self.h, C.byref(v)))
+        return v.value
+
+    def get_xbeta(self) -> np.ndarray:
+        out = np.zeros(self.d.K)
+        _check(lib().ccdb_get_xbeta(self.h, _p(out)))
+        return out
+
+    def get_beta(self) -> np.ndarray:
+        out = np.zeros(self.d.J)
+        _check(lib().ccdb_get_beta(self.h, _p(out)))
+        return out
+
+    # --- CyclicCoordinateDescent::update
+    def find_mode(self, args: Optional[ModeFindingArguments] = None,
+                  beta: Optional[np.ndarray] = None) -> FitResult:
+        args = args or ModeFindingArguments()
+        keep = []
+        ma = _mode_args(self.d, args, keep)
+        b = None if beta is None else np.ascontiguousarray(beta, np.float64).copy()
+        res = _FitResult()
+        _check(lib().ccdb_find_mode(self.h, C.byref(ma), _p(b), C.byref(res)))
+        out = b if b is not None else self.get_beta()
+        return FitResult(out, res.return_flag, res.iterations, res.log_likelihood, res.objective,
+                         res.coordinate_updates, res.device_seconds)
+
+
+def fit_model(ctx: Context, d: CyclopsData, args: Optional[ModeFindingArguments] = None,
+              weights: Optional[np.ndarray] = None, precision: int = PRECISION_FP64) -> FitResult:
+    """One call from host buffers: upload, find the mode, return beta
+    (the fitCyclopsModel-style entry point, ccdb_fit_model)."""
+    args = args or ModeFindingArguments()
+    keep = []
+    desc = _desc(d, precision, keep)
+    ma = _mode_args(d, args, keep)
+    arrs = [_c(d.col_start, np.int64), _c(d.rows, np.int32), _c(d.val_start, np.int64),
+            _c(d.vals, np.float64), _c(d.fmt, np.uint8)]
+    w = _c(weights, np.float64)
+    beta = np.zeros(d.J)
+    res = _FitResult()
+    _check(lib().ccdb_fit_model(ctx.h, d.K, d.J, *[_p(a) for a in arrs], C.byref(desc), _p(w),
+                                C.byref(ma), _p(beta), C.byref(res)))
+    return FitResult(beta, res.return_flag, res.iterations, res.log_likelihood, res.objective,
+                     res.coordinate_updates, res.device_seconds)

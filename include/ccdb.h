@@ -1,0 +1,145 @@
+/* ccdb.h -- C ABI of the B200 coordinate-descent engine (libccdb.so).
+ *
+ * The engine replaces the CPU implementation behind the reference Cyclops
+ * operator API: bsccs::AbstractModelSpecifics (engine/AbstractModelSpecifics.h:36-229)
+ * and the mode-finding loop of bsccs::CyclicCoordinateDescent
+ * (CyclicCoordinateDescent.cpp:586-615, 909-1216).  Every call takes plain
+ * pointers and sizes; no C++ or framework types cross this boundary, no
+ * exception escapes it.  All functions return CCDB_OK (0) or a negative status
+ * code; ccdb_last_error() gives the message of the last failure on the
+ * calling thread.
+ *
+ * Conventions shared with the reference:
+ *   - model_type uses the reference's ModelType numbering (Types.h:134-147):
+ *     POISSON=2, LOGISTIC=3, CONDITIONAL_LOGISTIC=4, CONDITIONAL_POISSON=6, COX=8.
+ *   - column formats use FormatType (CompressedDataMatrix.h:36-38):
+ *     DENSE=0, SPARSE=1, INDICATOR=2, INTERCEPT=3.
+ *   - prior types use priors::PriorType (Types.h:100-105): NONE=0, LAPLACE=1, NORMAL=2.
+ *   - convergence types use ConvergenceType (Types.h:108-114): GRADIENT=0, LANGE=1, MITTAL=2.
+ *   - return flags of a fit use UpdateReturnFlags (Types.h:124-130).
+ *   - column order is the reference's after ModelData::loadX/setOffsetCovariate
+ *     (ModelData.cpp:246-370, 640-651): [offset?, intercept?, covariates...];
+ *     with an offset, column 0's coefficient is fixed at 1.
+ *   - survival rows are sorted by (stratum, -time, y) (R/DataManagement.R:166).
+ */
+#ifndef CCDB_H
+#define CCDB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CCDB_OK 0
+#define CCDB_ERR_INVALID (-1)     /* bad argument or inconsistent data */
+#define CCDB_ERR_CUDA (-2)        /* CUDA runtime failure */
+#define CCDB_ERR_UNSUPPORTED (-3) /* model/format/option not implemented */
+#define CCDB_ERR_BUDGET (-4)      /* request exceeds the context's HBM budget */
+#define CCDB_ERR_TIMEOUT (-5)     /* a bounded device-side wait ran out */
+
+#define CCDB_PRECISION_FP64 0  /* all arithmetic in double, as the reference's RealType=double */
+#define CCDB_PRECISION_MIXED 1 /* FP32 row state and gathers, compensated sums, FP64 step */
+
+typedef struct ccdb_context ccdb_context;
+typedef struct ccdb_matrix ccdb_matrix;
+typedef struct ccdb_fit ccdb_fit;
+
+/* Thread-local text of the last failure. */
+const char* ccdb_last_error(void);
+
+/* One context per GPU.  hbm_budget_bytes = 0 means "no limit". */
+int ccdb_context_create(int device, size_t hbm_budget_bytes, ccdb_context** out);
+int ccdb_context_destroy(ccdb_context* ctx);
+/* Bytes of device memory currently held by matrices and fits of ctx. */
+int ccdb_context_memory(const ccdb_context* ctx, size_t* bytes_in_use);
+
+/* Upload a column-major CompressedDataMatrix (CompressedDataMatrix.h:40-452).
+ * col_start[J+1] offsets into rows[] (SPARSE/INDICATOR entries, row ids ascending);
+ * val_start[J+1] offsets into vals[] (SPARSE: one per entry; DENSE: K values);
+ * fmt[J] per-column FormatType.  The matrix is immutable and may be shared by
+ * any number of fits of the same context.  Replaces ModelData::loadX. */
+int ccdb_matrix_create(ccdb_context* ctx, int64_t K, int32_t J, const int64_t* col_start,
+                       const int32_t* rows, const int64_t* val_start, const double* vals,
+                       const uint8_t* fmt, ccdb_matrix** out);
+int ccdb_matrix_destroy(ccdb_matrix* m);
+
+typedef struct {
+    int32_t model_type;    /* ModelType */
+    int32_t precision;     /* CCDB_PRECISION_* */
+    const double* y;       /* K outcomes (Cox: event indicator) */
+    const double* time;    /* K survival times (Cox) or NULL */
+    const int64_t* stratum; /* K stratum ids (CLR, Cox) or NULL */
+    int32_t offset_col0;   /* column 0 is an offset with beta fixed at 1 */
+} ccdb_fit_desc;
+
+/* Per-fit state on the device (xBeta, offsExpXBeta, denominators, beta ...):
+ * the device counterpart of ModelSpecifics<Model,Real> constructed by
+ * AbstractModelSpecifics::factory (AbstractModelSpecifics.cpp:128-154) and
+ * ModelSpecifics::initialize (ModelSpecifics.hpp:1899-1952). */
+int ccdb_fit_create(ccdb_context* ctx, const ccdb_matrix* m, const ccdb_fit_desc* desc,
+                    ccdb_fit** out);
+int ccdb_fit_destroy(ccdb_fit* f);
+
+/* --- per-coordinate operator API (AbstractModelSpecifics) ------------------ */
+
+/* CV row weights, NULL = unweighted (ModelSpecifics::setWeights, ModelSpecifics.hpp:427-484,
+ * followed by computeFixedTermsInLogLikelihood/GradientAndHessian :570-587, :589-603). */
+int ccdb_set_weights(ccdb_fit* f, const double* weights);
+/* beta[J] -> xBeta, offsExpXBeta, denominators (computeXBeta + computeRemainingStatistics,
+ * CyclicCoordinateDescent.cpp:1452-1470, ModelSpecifics.hpp:1588-1633). */
+int ccdb_set_beta(ccdb_fit* f, const double* beta);
+/* computeNumeratorForGradient + computeGradientAndHessian for column j
+ * (ModelSpecifics.hpp:1353-1464, 711-766). */
+int ccdb_compute_gradient_hessian(ccdb_fit* f, int32_t j, double* gradient, double* hessian);
+/* beta[j] += delta and updateXBeta (ModelSpecifics.hpp:1466-1586). */
+int ccdb_update_xbeta(ccdb_fit* f, int32_t j, double delta);
+/* computeRemainingStatistics (ModelSpecifics.hpp:1588-1633). */
+int ccdb_compute_remaining_statistics(ccdb_fit* f);
+/* getLogLikelihood (ModelSpecifics.hpp:605-650). */
+int ccdb_get_log_likelihood(ccdb_fit* f, double* loglik);
+/* getXBeta (ModelSpecifics.hpp:286-289): K values. */
+int ccdb_get_xbeta(ccdb_fit* f, double* out);
+int ccdb_get_beta(ccdb_fit* f, double* out);
+
+/* --- mode finding (CyclicCoordinateDescent::update) ------------------------ */
+
+typedef struct {
+    const int32_t* prior_type; /* J, PriorType per column */
+    const double* prior_var;   /* J, prior variance per column */
+    int32_t convergence_type;  /* ConvergenceType */
+    double tolerance;          /* default 1e-6 (CcdInterface.h:83-93) */
+    int32_t max_iterations;    /* default 1000 */
+    double initial_bound;      /* default 2.0 */
+    int32_t max_bound_count;   /* default 5 */
+    int32_t per_coordinate;    /* 0: fused persistent sweep (default); 1: host loop over
+                                  the per-coordinate calls above (the reference's call pattern) */
+} ccdb_mode_args;
+
+typedef struct {
+    int32_t return_flag;        /* UpdateReturnFlags */
+    int32_t iterations;         /* sweeps of the last findMode */
+    double log_likelihood;
+    double objective;           /* last convergence objective */
+    int64_t coordinate_updates; /* ccdUpdateBeta calls over all sweeps */
+    double device_seconds;      /* time inside the sweep kernels */
+} ccdb_fit_result;
+
+/* Run CyclicCoordinateDescent::update (.cpp:586-615): findMode, with the
+ * ILLCONDITIONED retry shrinking the bound.  beta_inout[J]: starting values in,
+ * the mode out (NULL: start from 0 / offset 1, discard). */
+int ccdb_find_mode(ccdb_fit* f, const ccdb_mode_args* args, double* beta_inout,
+                   ccdb_fit_result* result);
+
+/* One-call fit from host buffers: upload, find the mode, copy beta back.  The
+ * reference-facing convenience used by fitCyclopsModel-style callers. */
+int ccdb_fit_model(ccdb_context* ctx, int64_t K, int32_t J, const int64_t* col_start,
+                   const int32_t* rows, const int64_t* val_start, const double* vals,
+                   const uint8_t* fmt, const ccdb_fit_desc* desc, const double* weights,
+                   const ccdb_mode_args* args, double* beta_out, ccdb_fit_result* result);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CCDB_H */
