@@ -1,0 +1,383 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 coordinate-descent engine.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: Poisson regression with offset, N=1,000,000 rows x P=100,000
+covariates (rank-Zipf(1.1) column sizes capped at 50,000, ~2e7 nonzeros, 80 %
+indicator / 20 % sparse LogNormal columns), offset log(t), intercept, Normal
+prior variance 1, FP64, the reference's default convergence (gradient, 1e-6).
+Seeded synthetic data of that shape (no public dataset exists for it).
+
+A step is one converged findMode from a cold start (beta = 0, offset 1): the
+whole coordinate-descent hot path over one input.  `value` is coordinate
+updates per second with the inputs resident in HBM (device-timed with CUDA
+events on the engine's stream, max over ranks, L2 flushed between steps);
+`e2e` is the same metric through the one-call C-ABI entry point
+(ccdb_fit_model) from pinned host buffers, uploads and the copy of beta back
+inside the timed span.  With --gpus N each rank fits its own replica (weak
+scaling; a single fit does not shard).
+
+--impl reference times the reference Cyclops engine compiled from source (or
+the plain-C restatement where it is absent) on the host cores, one sweep of
+the same workload per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from ccd_b200 import synthetic  # noqa: E402
+from ccd_b200.data import DENSE, GRADIENT, INDICATOR, INTERCEPT, SPARSE  # noqa: E402
+
+METRIC = "coord-updates/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--small", action="store_true", help="a 10x smaller problem (quick checks)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--max-sweeps", type=int, default=1000,
+                    help="cap on sweeps per findMode (profiling captures of one short launch)")
+    return ap.parse_args()
+
+
+def workload(rank: int, small: bool):
+    if small:
+        d = synthetic.poisson_offset(seed=2 + rank, K=100_000, P=10_000, total_nnz=2e6, cap=5_000)
+    else:
+        d = synthetic.poisson_offset(seed=2 + rank)
+    return d
+
+
+def config_of(d, small: bool) -> dict:
+    return {
+        "workload": "poisson_offset" + ("_small" if small else ""),
+        "model": "poisson",
+        "rows": d.K, "columns": d.J, "nnz": d.nnz,
+        "prior": "normal(1.0), none on offset/intercept",
+        "convergence": "gradient, tol 1e-6",
+        "precision": "fp64",
+        "step": "one converged findMode from a cold start",
+        "l2": "flushed between timed steps (512 MiB device write)",
+    }
+
+
+def cold_beta(d) -> np.ndarray:
+    b = np.zeros(d.J)
+    if d.offset_col0:
+        b[0] = 1.0
+    return b
+
+
+def active_columns(d) -> int:
+    return d.J - (1 if d.offset_col0 else 0)
+
+
+def sweep_bytes(d) -> float:
+    """Algorithmic bytes of one sweep (FP64, unweighted, every delta nonzero):
+    per entry the column index (4 B, SPARSE/INDICATOR) and value (8 B, SPARSE/
+    DENSE) read for the gradient and again for the update, plus one 8-byte row
+    state word read for the gradient and read+written by the update."""
+    total = 0.0
+    lo = 1 if d.offset_col0 else 0
+    cnt = np.diff(d.col_start)
+    for f, idx_b, val_b in ((INDICATOR, 4, 0), (SPARSE, 4, 8), (DENSE, 0, 8), (INTERCEPT, 0, 0)):
+        sel = d.fmt[lo:] == f
+        if f in (DENSE, INTERCEPT):
+            e = float(sel.sum()) * d.K
+        else:
+            e = float(cnt[lo:][sel].sum())
+        total += e * (idx_b + val_b) * 2 + e * 8 * 3
+    return total
+
+
+def objective_bytes(d) -> float:
+    """One convergence check: y and xBeta of every row."""
+    return d.K * 16.0
+
+
+def read_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            v = json.load(fh)
+        return float(v["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def read_traffic(workload_name: str):
+    """Per-launch DRAM bytes of the sweep kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", f"sweep_{workload_name}.md")
+    try:
+        with open(p) as fh:
+            for line in fh:
+                if line.strip().startswith("traffic_bytes_per_sweep:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax = float(parts[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def allreduce(vals, op, world):
+    if world == 1:
+        return vals
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(vals, dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=op)
+    return t.tolist()
+
+
+def cpu_reference_sample(d, target_s: float = 15.0):
+    """The reference CPU engine on a bounded sample of the same workload: the
+    first n sweeps of the cold-start fit, single thread."""
+    from oracle import checker
+    eng_cls = checker.best_engine()
+    kind = "reference" if eng_cls is checker.ReferenceEngine else "port"
+    eng = eng_cls(d)
+    t0 = time.perf_counter()
+    eng.fit(GRADIENT, 1e-6, max_iter=1)
+    t1 = time.perf_counter() - t0
+    n = int(max(1, min(20, round(target_s / max(t1, 1e-3)))))
+    if n > 1:
+        eng.set_beta(cold_beta(d))
+        t0 = time.perf_counter()
+        eng.fit(GRADIENT, 1e-6, max_iter=n)
+        tn = time.perf_counter() - t0
+    else:
+        tn = t1
+    eng.close()
+    rate = n * active_columns(d) / tn
+    return {"value": rate, "unit": METRIC, "cores": 1, "kind": kind,
+            "sample": f"first {n} sweep(s) of the cold-start fit ({n * active_columns(d)} coordinate "
+                      f"updates, {tn:.1f} s), single thread (the reference inner loop is serial)"}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from oracle import checker
+    d = workload(0, args.small)
+    eng_cls = checker.best_engine()
+    kind = "reference" if eng_cls is checker.ReferenceEngine else "port"
+    eng = eng_cls(d)
+    times = []
+    for i in range(args.warmup + args.steps):
+        eng.set_beta(cold_beta(d))
+        t0 = time.perf_counter()
+        eng.fit(GRADIENT, 1e-6, max_iter=1)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    eng.close()
+    total = float(np.sum(times))
+    v = args.steps * active_columns(d) / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded PCG64, workload shapes of the benchmark config)",
+        "config": {**config_of(d, args.small), "step": "one sweep of the cold-start fit (bounded sample)"},
+        "cpu_baseline": {"value": v, "unit": METRIC, "cores": 1, "kind": kind,
+                         "sample": "one sweep of the cold-start fit per step, single thread"},
+        "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from ccd_b200 import native
+    import torch.distributed as tdist
+
+    d = workload(rank, args.small)
+    ctx = native.Context(local)
+    m = native.Matrix(ctx, d)
+    f = native.Fit(ctx, m, d)
+    margs = native.ModeFindingArguments(convergence_type=GRADIENT, tolerance=1e-6,
+                                        max_iterations=args.max_sweeps)
+    cold = cold_beta(d)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    for _ in range(args.warmup):
+        f.set_beta(cold)
+        f.find_mode(margs)
+
+    clocks = Clocks(local)
+    if world > 1:
+        tdist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    dev_t, ker_t, updates, launches, sweeps, lat = 0.0, 0.0, 0, 0, 0, []
+    for _ in range(args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        f.set_beta(cold)
+        r = f.find_mode(margs)
+        dev_t += r.device_seconds
+        ker_t += r.kernel_seconds
+        updates += r.coordinate_updates
+        launches += r.kernel_launches
+        sweeps += r.iterations
+        lat.append(r.device_seconds)
+    torch.cuda.synchronize()
+    if world > 1:
+        tdist.barrier()
+    clk = clocks.stop()
+    last = r
+
+    # end to end through the one-call entry point, inputs in pinned host memory
+    def pinned(a):
+        t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        return t.numpy()
+    from ccd_b200.data import CyclopsData
+    dp = CyclopsData(d.model_type, pinned(d.y), pinned(d.col_start), pinned(d.rows),
+                     pinned(d.val_start), pinned(d.vals), pinned(d.fmt), d.prior_type, d.prior_var,
+                     time=d.time, stratum=d.stratum, offset_col0=d.offset_col0)
+    h2d = sum(a.nbytes for a in (dp.y, dp.col_start, dp.rows, dp.val_start, dp.vals, dp.fmt))
+    d2h = d.J * 8
+    e2e_t, e2e_updates = 0.0, 0
+    e2e_steps = args.steps
+    if world > 1:
+        tdist.barrier()
+    torch.cuda.synchronize()
+    for _ in range(e2e_steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        r2 = native.fit_model(ctx, dp, margs)
+        e2e_t += r2.device_seconds
+        e2e_updates += r2.coordinate_updates
+    torch.cuda.synchronize()
+
+    mx = allreduce([dev_t, e2e_t], tdist.ReduceOp.MAX if world > 1 else None, world)
+    sm = allreduce([float(updates), float(e2e_updates), float(launches)],
+                   tdist.ReduceOp.SUM if world > 1 else None, world)
+    dev_max, e2e_max = mx
+    tot_updates, tot_e2e, tot_launch = sm
+
+    if rank == 0:
+        peak, peak_kind = read_peaks()
+        per_launch_bytes = (sweep_bytes(d) * sweeps + objective_bytes(d) * (sweeps + args.steps)) / args.steps
+        achieved = (sweep_bytes(d) * sweeps + objective_bytes(d) * (sweeps + args.steps)) / ker_t / 1e9
+        wl = config_of(d, args.small)["workload"]
+        traffic = read_traffic(wl)
+        line = {
+            "metric": METRIC, "value": tot_updates / dev_max, "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dev_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded PCG64, workload shapes of the benchmark config)",
+            "config": {**config_of(d, args.small), "parallelism": f"replicas x{world}"},
+            "fits_per_s": world * args.steps / dev_max,
+            "fit_latency_ms": {"p50": 1e3 * float(np.percentile(lat, 50)),
+                               "p99": 1e3 * float(np.percentile(lat, 99))},
+            "sweeps_per_fit": sweeps / args.steps,
+            "return_flag": last.return_flag,
+            "e2e": {"value": tot_e2e / e2e_max, "unit": METRIC, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": per_launch_bytes,
+                         "kernel": "indep_sweep_kernel<POISSON> (one launch per findMode)",
+                         "traffic": traffic},
+            "gpu_launches": int(tot_launch),
+            "clocks": clk,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_reference_sample(d)
+        print(json.dumps(line), flush=True)
+    f.close()
+    m.close()
+    ctx.close()
+    if world > 1:
+        tdist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -130,8 +130,8 @@ Fit::~Fit() {
                     (void*)gh_parts, (void*)gh_out})
         ctx->release(p);
     release_schedule();
-    if (ev0) cudaEventDestroy(ev0);
-    if (ev1) cudaEventDestroy(ev1);
+    for (cudaEvent_t e : {ev0, ev1, evc0, evc1})
+        if (e) cudaEventDestroy(e);
 }
 
 void Fit::release_schedule() {
@@ -189,11 +189,19 @@ void Fit::apply_weights() {
     check_cuda(launch_xjy(m->d_col_ptr, m->d_rows, m->d_val_ptr, m->d_vals, m->d_fmt, y,
                           weighted ? w : nullptr, K, J, xjy, stream),
                "xjy");
+    ++launches;
     ll_fixed = 0.0;
-    if (model == M_POISSON) {  // PoissonRegression::logLikeFixedTermsContrib, ModelSpecifics.h:1596-1601
+    if (model == M_POISSON) {
+        // PoissonRegression::logLikeFixedTermsContrib (ModelSpecifics.h:1596-1601) sums
+        // -log(c) for c = 2..y in order; the running table reproduces each sum exactly.
+        std::vector<double> table(1, 0.0);
         for (int64_t i = 0; i < K; ++i) {
-            double t = 0.0;
-            for (int c = 2; c <= (int)y_h[i]; c++) t += -std::log((double)c);
+            const int yi = (int)y_h[i];
+            while ((int)table.size() <= yi) {
+                const int c = (int)table.size();
+                table.push_back(c >= 2 ? table.back() + -std::log((double)c) : 0.0);
+            }
+            const double t = yi >= 2 ? table[yi] : 0.0;
             ll_fixed += weighted ? t * wh[i] : t;
         }
     }
@@ -212,12 +220,17 @@ void Fit::compute_xbeta() {
         }
     if (nonzero == 0) {
         check_cuda(cudaMemsetAsync(xb_tmp, 0, sizeof(double) * K, stream), "xb zero");
+    } else if (nonzero == 1 && (m->fmt[only] == F_DENSE || m->fmt[only] == F_INTERCEPT)) {
+        // one dense-like column (the offset of a cold start): xBeta = 0 + b*x
+        const double* v = (m->fmt[only] == F_DENSE) ? m->d_vals + m->val_start[only] : nullptr;
+        check_cuda(launch_xbeta_dense(v, beta_h[only], K, xb_tmp, stream), "xbeta");
+        ++launches;
     } else {
         const_cast<Matrix*>(m)->ensure_csr(stream);
         check_cuda(launch_xbeta_csr(m->d_row_ptr, m->d_csr_col, m->d_csr_val, beta, K, xb_tmp, stream),
                    "xbeta");
+        ++launches;
     }
-    (void)only;
     xb_pending = true;
     xb_known = true;
     suff_known = false;
@@ -228,6 +241,7 @@ void Fit::remaining_statistics() {
     const double null_denom = (model == M_LOGISTIC) ? 1.0 : 0.0;
     check_cuda(launch_remaining_stats(row, xb_pending ? xb_tmp : nullptr, w, K, null_denom, stream),
                "remaining statistics");
+    ++launches;
     xb_pending = false;
     suff_known = true;
 }
@@ -284,6 +298,7 @@ void Fit::objective_terms(double* out4) {
     const int nb = ctx->n_sm;
     IndepParams P = params();
     check_cuda(launch_indep_objective(P, nb, stream), "objective");
+    ++launches;
     std::vector<double2> parts(2 * nb);
     check_cuda(cudaMemcpyAsync(parts.data(), red, sizeof(double2) * 2 * nb, cudaMemcpyDeviceToHost, stream),
                "objective copy");
@@ -317,6 +332,7 @@ void Fit::gradient_hessian(int j, double* g, double* h) {
     check_lazy();
     IndepParams P = params();
     check_cuda(launch_indep_gh(P, j, m->entries(j), gh_parts, kGhParts, gh_out, stream), "gh");
+    launches += 2;
     double2 r;
     check_cuda(cudaMemcpyAsync(&r, gh_out, sizeof(double2), cudaMemcpyDeviceToHost, stream), "gh copy");
     check_cuda(cudaStreamSynchronize(stream), "gh sync");
@@ -331,6 +347,7 @@ void Fit::update_xbeta(int j, double delta) {
                "beta j");
     IndepParams P = params();
     check_cuda(launch_indep_update(P, j, m->fmt[j], m->entries(j), delta, stream), "update");
+    launches += m->entries(j) > 0 ? 1 : 0;
     check_cuda(cudaStreamSynchronize(stream), "update sync");
 }
 
@@ -410,6 +427,7 @@ void Fit::find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* 
     P.max_iter = a.max_iterations;
     check_cuda(cudaEventRecord(ev0, stream), "event");
     check_cuda(launch_indep_sweep(P, sched->host.n_cta, stream), "sweep launch");
+    ++launches;
     check_cuda(cudaEventRecord(ev1, stream), "event");
     DevStatus out{};
     check_cuda(cudaMemcpyAsync(&out, st, sizeof(out), cudaMemcpyDeviceToHost, stream), "status");
@@ -442,6 +460,8 @@ void Fit::find_mode(const ccdb_mode_args& a, double* beta_inout, ccdb_fit_result
     }
     int active = 0;
     for (int j = 0; j < J; ++j) active += fixed[j] ? 0 : 1;
+    const int64_t launches0 = launches;
+    check_cuda(cudaEventRecord(evc0, stream), "event");
     double bound = a.initial_bound;
     int count = 0, flag = R_FAIL, iters = 0;
     double obj = 0.0, secs = 0.0;
@@ -468,13 +488,20 @@ void Fit::find_mode(const ccdb_mode_args& a, double* beta_inout, ccdb_fit_result
     }
     if (beta_inout)
         for (int j = 0; j < J; ++j) beta_inout[j] = beta_h[j];
+    const double ll = log_likelihood();
+    check_cuda(cudaEventRecord(evc1, stream), "event");
+    check_cuda(cudaEventSynchronize(evc1), "event sync");
+    float call_ms = 0.f;
+    check_cuda(cudaEventElapsedTime(&call_ms, evc0, evc1), "elapsed");
     if (res) {
         res->return_flag = flag;
         res->iterations = iters;
         res->objective = obj;
-        res->log_likelihood = log_likelihood();
+        res->log_likelihood = ll;
         res->coordinate_updates = updates;
-        res->device_seconds = secs;
+        res->device_seconds = call_ms * 1e-3;
+        res->kernel_seconds = secs;
+        res->kernel_launches = launches - launches0;
     }
 }
 
@@ -534,6 +561,8 @@ int ccdb_context_create(int device, size_t hbm_budget_bytes, ccdb_context** out)
             throw Error(CCDB_ERR_UNSUPPORTED, "device lacks cooperative launch");
         }
         check_cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream");
+        check_cuda(cudaEventCreate(&c->ev_a), "event");
+        check_cuda(cudaEventCreate(&c->ev_b), "event");
         *out = c;
     });
 }
@@ -543,6 +572,8 @@ int ccdb_context_destroy(ccdb_context* ctx) {
         if (!ctx) return;
         cudaSetDevice(ctx->device);
         cudaStreamSynchronize(ctx->stream);
+        cudaEventDestroy(ctx->ev_a);
+        cudaEventDestroy(ctx->ev_b);
         cudaStreamDestroy(ctx->stream);
         delete ctx;
     });
@@ -643,6 +674,8 @@ int ccdb_fit_create(ccdb_context* ctx, const ccdb_matrix* m, const ccdb_fit_desc
         f->gh_out = static_cast<double2*>(ctx->alloc(sizeof(double2)));
         check_cuda(cudaEventCreate(&f->ev0), "event");
         check_cuda(cudaEventCreate(&f->ev1), "event");
+        check_cuda(cudaEventCreate(&f->evc0), "event");
+        check_cuda(cudaEventCreate(&f->evc1), "event");
         // CyclicCoordinateDescent::init (.cpp:200-239)
         f->beta_h.assign(J, 0.0);
         f->fixed.assign(J, 0);
@@ -755,11 +788,26 @@ int ccdb_fit_model(ccdb_context* ctx, int64_t K, int32_t J, const int64_t* col_s
                    double* beta_out, ccdb_fit_result* result) {
     ccdb_matrix* m = nullptr;
     ccdb_fit* f = nullptr;
+    if (!ctx) {
+        g_last_error = "NULL context";
+        return CCDB_ERR_INVALID;
+    }
+    if (cudaSetDevice(ctx->device) != cudaSuccess || cudaEventRecord(ctx->ev_a, ctx->stream) != cudaSuccess) {
+        g_last_error = "cannot record on the context stream";
+        return CCDB_ERR_CUDA;
+    }
     int rc = ccdb_matrix_create(ctx, K, J, col_start, rows, val_start, vals, fmt, &m);
     if (rc == CCDB_OK) rc = ccdb_fit_create(ctx, m, desc, &f);
     if (rc == CCDB_OK && weights) rc = ccdb_set_weights(f, weights);
     if (rc == CCDB_OK) rc = ccdb_find_mode(f, args, nullptr, result);
     if (rc == CCDB_OK && beta_out) rc = ccdb_get_beta(f, beta_out);
+    if (rc == CCDB_OK && result) {
+        float ms = 0.f;
+        if (cudaEventRecord(ctx->ev_b, ctx->stream) == cudaSuccess &&
+            cudaEventSynchronize(ctx->ev_b) == cudaSuccess &&
+            cudaEventElapsedTime(&ms, ctx->ev_a, ctx->ev_b) == cudaSuccess)
+            result->device_seconds = ms * 1e-3;
+    }
     std::string err = g_last_error;
     if (f) ccdb_fit_destroy(f);
     if (m) ccdb_matrix_destroy(m);

@@ -28,6 +28,7 @@ struct Context {
     cudaStream_t stream = nullptr;
     std::mutex mu;
     std::map<void*, size_t> sizes;
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr;  // around a one-call fit
 
     void* alloc(size_t bytes);
     void release(void* p);
@@ -94,7 +95,9 @@ struct Fit {
     double* w = nullptr;
     double2* gh_parts = nullptr;
     double2* gh_out = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;    // around the sweep launches
+    cudaEvent_t evc0 = nullptr, evc1 = nullptr;  // around a whole find_mode
+    int64_t launches = 0;                        // engine kernels launched so far
     std::unique_ptr<DevSchedule> sched;
 
     // host mirror and lazy flags (CyclicCoordinateDescent.h:152-166)

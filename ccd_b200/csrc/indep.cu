@@ -443,9 +443,22 @@ __global__ void xbeta_csr_kernel(const int64_t* row_ptr, const int32_t* col_idx,
     }
 }
 
+// xBeta = 0 + b * x for a single dense-like column (x = 1 for an intercept).
+__global__ void xbeta_dense_kernel(const double* vals, double b, int64_t K, double* xb) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K;
+         k += (int64_t)gridDim.x * blockDim.x)
+        xb[k] = 0.0 + b * (vals ? vals[k] : 1.0);
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------- launchers
+
+cudaError_t launch_xbeta_dense(const double* vals, double b, int64_t K, double* xb,
+                               cudaStream_t stream) {
+    xbeta_dense_kernel<<<1184, 256, 0, stream>>>(vals, b, K, xb);
+    return cudaGetLastError();
+}
 
 int indep_threads() { return kThreads; }
 int indep_max_split() { return kMaxSplit; }

@@ -63,6 +63,8 @@ cudaError_t launch_indep_objective(const IndepParams& P, int n_blocks, cudaStrea
 cudaError_t launch_xjy(const int64_t* col_ptr, const int32_t* rows, const int64_t* val_ptr,
                        const double* vals, const uint8_t* fmt, const double* y, const double* w,
                        int64_t K, int32_t J, double* xjy, cudaStream_t stream);
+cudaError_t launch_xbeta_dense(const double* vals, double b, int64_t K, double* xb,
+                               cudaStream_t stream);
 cudaError_t launch_xbeta_csr(const int64_t* row_ptr, const int32_t* col_idx, const double* val,
                              const double* beta, int64_t K, double* xb, cudaStream_t stream);
 

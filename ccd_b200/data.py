@@ -137,7 +137,12 @@ def build_columns(K: int, columns, formats) -> tuple:
 def csc_from_coo(K: int, J: int, col: np.ndarray, row: np.ndarray) -> tuple:
     """Sorted, de-duplicated CSC (col_start, rows) from COO indices."""
     key = col.astype(np.int64) * K + row.astype(np.int64)
-    key = np.unique(key)
+    key.sort()
+    if key.size:
+        keep = np.empty(key.size, bool)
+        keep[0] = True
+        np.not_equal(key[1:], key[:-1], out=keep[1:])
+        key = key[keep]
     c = (key // K).astype(np.int64)
     r = (key % K).astype(np.int32)
     counts = np.bincount(c, minlength=J)

@@ -46,7 +46,8 @@ class _ModeArgs(C.Structure):
 class _FitResult(C.Structure):
     _fields_ = [("return_flag", C.c_int32), ("iterations", C.c_int32),
                 ("log_likelihood", C.c_double), ("objective", C.c_double),
-                ("coordinate_updates", C.c_int64), ("device_seconds", C.c_double)]
+                ("coordinate_updates", C.c_int64), ("device_seconds", C.c_double),
+                ("kernel_seconds", C.c_double), ("kernel_launches", C.c_int64)]
 
 
 @dataclass
@@ -69,6 +70,8 @@ class FitResult:
     objective: float
     coordinate_updates: int
     device_seconds: float
+    kernel_seconds: float = 0.0
+    kernel_launches: int = 0
 
 
 _lib = None
@@ -254,7 +257,8 @@ class Fit:
         _check(lib().ccdb_find_mode(self.h, C.byref(ma), _p(b), C.byref(res)))
         out = b if b is not None else self.get_beta()
         return FitResult(out, res.return_flag, res.iterations, res.log_likelihood, res.objective,
-                         res.coordinate_updates, res.device_seconds)
+                         res.coordinate_updates, res.device_seconds, res.kernel_seconds,
+                         res.kernel_launches)
 
 
 def fit_model(ctx: Context, d: CyclopsData, args: Optional[ModeFindingArguments] = None,
@@ -273,4 +277,5 @@ def fit_model(ctx: Context, d: CyclopsData, args: Optional[ModeFindingArguments]
     _check(lib().ccdb_fit_model(ctx.h, d.K, d.J, *[_p(a) for a in arrs], C.byref(desc), _p(w),
                                 C.byref(ma), _p(beta), C.byref(res)))
     return FitResult(beta, res.return_flag, res.iterations, res.log_likelihood, res.objective,
-                     res.coordinate_updates, res.device_seconds)
+                     res.coordinate_updates, res.device_seconds, res.kernel_seconds,
+                     res.kernel_launches)

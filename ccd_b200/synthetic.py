@@ -43,24 +43,32 @@ def _bernoulli_csc(rng, K: int, P: int, density: float):
 
 
 def _columns_with_counts(rng, K: int, counts: np.ndarray):
+    """CSC with exactly counts[j] distinct uniform rows in column j."""
     counts = np.minimum(np.asarray(counts, np.int64), K)
-    total = int(counts.sum())
-    col = np.repeat(np.arange(counts.size, dtype=np.int64), counts)
-    row = rng.integers(0, K, size=total, dtype=np.int64)
-    col_start, rows = csc_from_coo(K, counts.size, col, row)
-    # top up columns that lost entries to duplicate draws, until exact
-    for _ in range(64):
-        have = np.diff(col_start)
+    P = counts.size
+    col = np.repeat(np.arange(P, dtype=np.int64), counts)
+    key = col * K + rng.integers(0, K, size=col.size, dtype=np.int64)
+    key.sort()
+    key = key[np.concatenate([[True], key[1:] != key[:-1]])] if key.size else key
+    have = np.bincount(key // K, minlength=P)
+    # top up the columns that lost entries to duplicate draws, touching only them
+    for _ in range(100):
         short = np.nonzero(have < counts)[0]
         if short.size == 0:
             break
+        in_short = np.isin(key // K, short)
+        sub = key[in_short]
         need = (counts - have)[short]
-        c2 = np.repeat(short, need)
-        r2 = rng.integers(0, K, size=int(need.sum()), dtype=np.int64)
-        allc = np.concatenate([np.repeat(np.arange(counts.size), have), c2])
-        allr = np.concatenate([rows.astype(np.int64), r2])
-        col_start, rows = csc_from_coo(K, counts.size, allc, allr)
-    return col_start, rows
+        extra = np.repeat(short, need) * K + rng.integers(0, K, size=int(need.sum()), dtype=np.int64)
+        sub = np.concatenate([sub, extra])
+        sub.sort()
+        sub = sub[np.concatenate([[True], sub[1:] != sub[:-1]])]
+        key = np.concatenate([key[~in_short], sub])
+        key.sort()
+        have = np.bincount(key // K, minlength=P)
+    col_start = np.zeros(P + 1, np.int64)
+    np.cumsum(have, out=col_start[1:])
+    return col_start, (key % K).astype(np.int32)
 
 
 def _xbeta(K: int, col_start, rows, vals_per_entry, beta) -> np.ndarray:

@@ -123,7 +123,12 @@ typedef struct {
     double log_likelihood;
     double objective;           /* last convergence objective */
     int64_t coordinate_updates; /* ccdUpdateBeta calls over all sweeps */
-    double device_seconds;      /* time inside the sweep kernels */
+    double device_seconds;      /* device-timeline span of the call (CUDA events on the
+                                   engine's stream): ccdb_find_mode from its first to its last
+                                   device operation; ccdb_fit_model from the first upload to
+                                   the copy of beta back to the host */
+    double kernel_seconds;      /* span of the fused sweep launches alone */
+    int64_t kernel_launches;    /* engine kernels launched by the call */
 } ccdb_fit_result;
 
 /* Run CyclicCoordinateDescent::update (.cpp:586-615): findMode, with the
