@@ -6,6 +6,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -425,6 +427,17 @@ void Fit::find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* 
     P.conv = a.convergence_type;
     P.tol = a.tolerance;
     P.max_iter = a.max_iterations;
+    // CCDB_TRACE_FILE=<path>: dump per-segment timestamps of the first sweep
+    // together with the schedule (profiling aid; off by default)
+    const char* trace_path = std::getenv("CCDB_TRACE_FILE");
+    unsigned long long* d_trace = nullptr;
+    const size_t n_seg = sched->host.segs.size();
+    if (trace_path) {
+        d_trace = static_cast<unsigned long long*>(ctx->alloc(sizeof(unsigned long long) * 5 * n_seg));
+        check_cuda(cudaMemsetAsync(d_trace, 0, sizeof(unsigned long long) * 5 * n_seg, stream), "trace");
+        P.trace = d_trace;
+        P.trace2 = d_trace + 3 * n_seg;
+    }
     check_cuda(cudaEventRecord(ev0, stream), "event");
     check_cuda(launch_indep_sweep(P, sched->host.n_cta, stream), "sweep launch");
     ++launches;
@@ -433,6 +446,22 @@ void Fit::find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* 
     check_cuda(cudaMemcpyAsync(&out, st, sizeof(out), cudaMemcpyDeviceToHost, stream), "status");
     check_cuda(cudaStreamSynchronize(stream), "sweep");
     check_cuda(cudaEventElapsedTime(ms, ev0, ev1), "elapsed");
+    if (d_trace) {
+        std::vector<unsigned long long> tr(5 * n_seg);
+        check_cuda(cudaMemcpy(tr.data(), d_trace, sizeof(unsigned long long) * 5 * n_seg,
+                              cudaMemcpyDeviceToHost), "trace copy");
+        ctx->release(d_trace);
+        if (FILE* fh = std::fopen(trace_path, "wb")) {
+            const int64_t ns = (int64_t)n_seg, nt = (int64_t)sched->host.tasks.size();
+            std::fwrite(&ns, sizeof(ns), 1, fh);
+            std::fwrite(&nt, sizeof(nt), 1, fh);
+            std::fwrite(sched->host.segs.data(), sizeof(Seg), n_seg, fh);
+            std::fwrite(sched->host.cta_seg.data(), sizeof(int64_t), sched->host.cta_seg.size(), fh);
+            std::fwrite(sched->host.tasks.data(), sizeof(Task), nt, fh);
+            std::fwrite(tr.data(), sizeof(unsigned long long), tr.size(), fh);
+            std::fclose(fh);
+        }
+    }
     if (out.error != E_NONE)
         throw Error(CCDB_ERR_TIMEOUT, "device wait timed out (code " + std::to_string(out.error) +
                                           " at " + std::to_string(out.error_where) + ")");

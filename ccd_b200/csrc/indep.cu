@@ -181,6 +181,157 @@ __device__ __forceinline__ double objective_of(const IndepParams& P, double4 t, 
     return ll + t.w;
 }
 
+// ---------------------------------------------------------------- staged tasks
+// A task's entries are staged into registers (row id, value) before its level
+// is released: they are immutable, so only the row-state gather remains on the
+// dependency chain.  kE entries per thread cover every task the scheduler
+// builds (warp tasks <= 32*kE entries, CTA tasks and chunks <= kThreads*kE);
+// longer chunks (a column longer than n_cta * kThreads * kE) take the loop path.
+constexpr int kE = 8;   // entries per thread of a CTA-level task
+constexpr int kEw = 4;  // entries per lane of a warp task (warp tasks <= 128 entries)
+
+template <int N>
+struct Staged {
+    int32_t k[N];
+    double x[N];
+};
+
+struct ColMeta {
+    double xjy, pvar, beta, hd;
+    int32_t ptype;
+    int32_t fmt;
+};
+
+template <int N>
+__device__ __forceinline__ bool stageable(const Task& t, int nthr) {
+    return (t.p1 - t.p0) <= N * nthr;
+}
+
+// Hint the task's row ids and values into L1 ahead of its level.
+__device__ __forceinline__ void prefetch_entries(const IndepParams& P, const Task& t, int tid, int nthr) {
+    const uint8_t f = P.fmt[t.col];
+    const int64_t cb = P.col_ptr[t.col], vb = P.val_ptr[t.col];
+    const bool has_rows = (f == F_SPARSE || f == F_INDICATOR);
+    const bool has_vals = (f == F_SPARSE || f == F_DENSE);
+    for (int p = t.p0 + tid * 8; p < t.p1; p += nthr * 8) {  // 8 values per 64-byte stride
+        if (has_rows) asm volatile("prefetch.global.L1 [%0];" ::"l"(P.rows + cb + p));
+        if (has_vals) asm volatile("prefetch.global.L1 [%0];" ::"l"(P.vals + vb + p));
+    }
+}
+
+template <int N>
+__device__ __forceinline__ void stage_entries(const IndepParams& P, const Task& t, int tid, int nthr,
+                                              Staged<N>& s) {
+    const uint8_t f = P.fmt[t.col];
+    const int64_t cb = P.col_ptr[t.col], vb = P.val_ptr[t.col];
+    const bool has_rows = (f == F_SPARSE || f == F_INDICATOR);
+    const bool has_vals = (f == F_SPARSE || f == F_DENSE);
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        const int p = t.p0 + tid + i * nthr;
+        if (p < t.p1) {
+            s.k[i] = has_rows ? __ldg(P.rows + cb + p) : p;
+            s.x[i] = has_vals ? __ldg(P.vals + vb + p) : 1.0;
+        } else {
+            s.k[i] = -1;
+            s.x[i] = 0.0;
+        }
+    }
+}
+
+__device__ __forceinline__ ColMeta load_meta(const IndepParams& P, int j) {
+    ColMeta m;
+    m.xjy = P.xjy[j];
+    m.pvar = P.pvar[j];
+    m.ptype = P.ptype[j];
+    m.beta = __ldcg(P.beta + j);
+    m.hd = __ldcg(P.hdelta + j);
+    m.fmt = P.fmt[j];
+    return m;
+}
+
+// Hint the row state of staged entries into L2 before the level opens.  L2 is
+// the point of coherence, so the lines are current when read after the wait.
+template <int N>
+__device__ __forceinline__ void prefetch_rows_l2(const IndepParams& P, const Staged<N>& s) {
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+        if (s.k[i] >= 0) asm volatile("prefetch.global.L2 [%0];" ::"l"(P.row + 2 * (int64_t)s.k[i]));
+}
+
+// gather + gradient/Hessian of the staged entries; the gathered state stays
+// in registers for the update.
+template <int MODEL, int N>
+__device__ __forceinline__ void staged_gh(const IndepParams& P, bool ind, const Staged<N>& s,
+                                          double2 (&A)[N], double (&Dn)[N], double& g, double& h) {
+    double Wt[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        if (s.k[i] >= 0) {
+            A[i] = __ldcg(P.row + 2 * (int64_t)s.k[i]);
+            const double2 b = __ldcg(P.row + 2 * (int64_t)s.k[i] + 1);
+            Dn[i] = b.x;
+            Wt[i] = b.y;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        if (s.k[i] < 0) continue;
+        const double x = s.x[i];
+        const double n1 = A[i].y * x;
+        if (MODEL == M_LOGISTIC) {
+            const double gg = n1 / Dn[i];
+            g += Wt[i] * gg;
+            if (ind) h += Wt[i] * gg * (1.0 - gg);
+            else h += Wt[i] * ((n1 * x) / Dn[i] - gg * gg);
+        } else {
+            if (ind) {
+                const double v = Wt[i] * n1;
+                g += v;
+                h += v;
+            } else {
+                g += Wt[i] * n1;
+                h += Wt[i] * (n1 * x);
+            }
+        }
+    }
+}
+
+template <int N>
+__device__ __forceinline__ void staged_update(const IndepParams& P, const Staged<N>& s,
+                                              const double2 (&A)[N], const double (&Dn)[N],
+                                              double delta) {
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        if (s.k[i] < 0) continue;
+        const double xb = A[i].x + delta * s.x[i];
+        const double en = exp(xb);
+        const double dn = Dn[i] + (en - A[i].y);
+        __stcg(P.row + 2 * (int64_t)s.k[i], make_double2(xb, en));
+        __stcg(reinterpret_cast<double*>(P.row + 2 * (int64_t)s.k[i] + 1), dn);
+    }
+}
+
+__device__ __forceinline__ double meta_step(const ColMeta& m, int64_t entries, double gsum,
+                                            double hsum, double& hd_out) {
+    double g = 0.0, h = 0.0;
+    if (entries > 0) {
+        g = gsum - m.xjy;
+        h = hsum;
+    }
+    double delta = newton_prior_delta(g, h, m.beta, m.ptype, m.pvar);
+    double hd = m.hd;
+    delta = apply_bounds(delta, hd);
+    hd_out = hd;
+    return delta;
+}
+
+__device__ __forceinline__ void meta_write(const IndepParams& P, int j, const ColMeta& m, double delta,
+                                           double hd) {
+    P.hdelta[j] = hd;
+    if (delta != 0.0) P.beta[j] = m.beta + delta;
+}
+
 template <int MODEL>
 __global__ void __launch_bounds__(kThreads, 1) indep_sweep_kernel(IndepParams P) {
     __shared__ double4 s_red4[kWarps];
@@ -189,6 +340,10 @@ __global__ void __launch_bounds__(kThreads, 1) indep_sweep_kernel(IndepParams P)
     __shared__ double s_delta;
     __shared__ int32_t s_fail;
     __shared__ int32_t s_done;
+    // staged before a level opens: column metadata (slot kWarps = the CTA-level task)
+    // and each lane's entries of its warp task
+    __shared__ ColMeta s_meta[kWarps + 1];
+    __shared__ Staged<kEw> s_wstage[kThreads];
 
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     unsigned epoch = 0;
@@ -207,6 +362,52 @@ __global__ void __launch_bounds__(kThreads, 1) indep_sweep_kernel(IndepParams P)
     for (int it = 0; it < P.max_iter; ++it) {
         for (int64_t si = seg0; si < seg1; ++si) {
             const Seg sg = P.segs[si];
+            const Task* T = P.tasks + sg.t0;
+            const int n_cl = sg.n_chunk + sg.n_cta;  // CTA-level tasks
+            const int qw0 = n_cl, qw1 = qw0 + sg.n_warp;
+
+            // ---- before the level opens: stage everything that is immutable
+            Task tc{}, tw{};
+            bool c_staged = false, w_has = false, w_staged = false;
+            int qw_first = -1;
+            if (n_cl > 0) {
+                tc = T[0];
+                c_staged = stageable<kE>(tc, blockDim.x);
+                if (c_staged) {
+                    Staged<kE> st;  // row ids for the L2 prefetch; re-read from L1 after the wait
+                    stage_entries(P, tc, tid, blockDim.x, st);
+                    prefetch_rows_l2(P, st);
+                } else {
+                    prefetch_entries(P, tc, tid, blockDim.x);
+                }
+                if (tid == 0) s_meta[kWarps] = load_meta(P, tc.col);
+            }
+            if (sg.n_warp > 0) {
+                // first warp task of this warp (tasks of one segment are few)
+                for (int q0 = qw0; q0 < qw1 && qw_first < 0; q0 += 32) {
+                    const int q = q0 + lane;
+                    const bool mine = (q < qw1) && (T[q].warp == wid);
+                    const unsigned bal = __ballot_sync(0xffffffffu, mine);
+                    if (bal) qw_first = q0 + __ffs(bal) - 1;
+                }
+                if (qw_first >= 0) {
+                    w_has = true;
+                    tw = T[qw_first];
+                    w_staged = stageable<kEw>(tw, 32);
+                    if (w_staged) {
+                        Staged<kEw> st;
+                        stage_entries(P, tw, lane, 32, st);
+                        prefetch_rows_l2(P, st);
+                        s_wstage[tid] = st;
+                    } else {
+                        prefetch_entries(P, tw, lane, 32);
+                    }
+                    if (lane == 0) s_meta[wid] = load_meta(P, tw.col);
+                }
+            }
+
+            // ---- wait for the previous level
+            if (P.trace && it == 0 && tid == 0) P.trace[3 * si] = global_ns();
             if (sg.level > 0) {
                 if (tid == 0) {
                     const unsigned target = (unsigned)(it + 1) * (unsigned)P.level_need[sg.level - 1];
@@ -216,55 +417,89 @@ __global__ void __launch_bounds__(kThreads, 1) indep_sweep_kernel(IndepParams P)
                 __syncthreads();
                 if (s_fail) return;
             }
-            const Task* T = P.tasks + sg.t0;
-            // phase 1: partial sums of split columns, published without waiting
-            for (int q = 0; q < sg.n_chunk; ++q) {
-                const Task t = T[q];
-                const uint8_t f = P.fmt[t.col];
+
+            if (P.trace && it == 0 && tid == 0) P.trace[3 * si + 1] = global_ns();
+            // ---- phase 1: CTA-level tasks (split-column partials are published, not awaited)
+            for (int q = 0; q < n_cl; ++q) {
+                const Task t = (q == 0) ? tc : T[q];
+                const uint8_t f = (q == 0) ? (uint8_t)s_meta[kWarps].fmt : P.fmt[t.col];
+                const bool ind = (f == F_INDICATOR || f == F_INTERCEPT);
+                const bool staged = (q == 0) && c_staged;
                 double g = 0.0, h = 0.0;
-                gh_dispatch<MODEL>(P, t.col, f, t.p0, t.p1, tid, blockDim.x, g, h);
+                Staged<kE> sc;
+                double2 A[kE];
+                double Dn[kE];
+                if (staged) {
+                    stage_entries(P, t, tid, blockDim.x, sc);  // L1 hits after the prefetch
+                    staged_gh<MODEL>(P, ind, sc, A, Dn, g, h);
+                } else {
+                    gh_dispatch<MODEL>(P, t.col, f, t.p0, t.p1, tid, blockDim.x, g, h);
+                }
                 const double2 s = block_sum2<kWarps>(make_double2(g, h), s_red2);
-                if (tid == 0) {
-                    s_stash[q] = make_double2(__ldcg(P.beta + t.col), __ldcg(P.hdelta + t.col));
-                    __stcg(P.partials + t.part_base + t.chunk, s);
-                    __threadfence();
-                    atomicAdd(P.col_arrive + t.col, 1u);
+                if (t.kind == 2) {
+                    if (tid == 0) {
+                        const ColMeta m = (q == 0) ? s_meta[kWarps] : load_meta(P, t.col);
+                        s_stash[q] = make_double2(m.beta, m.hd);
+                        __stcg(P.partials + t.part_base + t.chunk, s);
+                        red_release_gpu_add(P.col_arrive + t.col, 1u);
+                    }
+                } else {
+                    if (tid == 0) {
+                        const ColMeta m = (q == 0) ? s_meta[kWarps] : load_meta(P, t.col);
+                        double hd;
+                        const double d = meta_step(m, t.p1, s.x, s.y, hd);
+                        meta_write(P, t.col, m, d, hd);
+                        s_delta = d;
+                    }
+                    __syncthreads();
+                    const double d = s_delta;
+                    if (d != 0.0) {
+                        if (staged) staged_update(P, sc, A, Dn, d);
+                        else update_dispatch(P, t.col, f, t.p0, t.p1, tid, blockDim.x, d);
+                    }
+                    __syncthreads();
                 }
             }
-            // phase 2a: whole-CTA columns
-            for (int q = sg.n_chunk; q < sg.n_chunk + sg.n_cta; ++q) {
-                const Task t = T[q];
-                const uint8_t f = P.fmt[t.col];
-                double g = 0.0, h = 0.0;
-                gh_dispatch<MODEL>(P, t.col, f, t.p0, t.p1, tid, blockDim.x, g, h);
-                const double2 s = block_sum2<kWarps>(make_double2(g, h), s_red2);
-                if (tid == 0)
-                    s_delta = column_step(P, t.col, t.p1, s.x, s.y, __ldcg(P.beta + t.col),
-                                          __ldcg(P.hdelta + t.col), true);
-                __syncthreads();
-                const double d = s_delta;
-                if (d != 0.0) update_dispatch(P, t.col, f, t.p0, t.p1, tid, blockDim.x, d);
-                __syncthreads();
+
+            if (P.trace2 && it == 0 && tid == 0) P.trace2[2 * si] = global_ns();
+            // ---- phase 2: warp tasks
+            if (sg.n_warp > 0) {
+                for (int q = (w_has ? qw_first : qw1); q < qw1; ++q) {
+                    const Task t = (q == qw_first) ? tw : T[q];
+                    if (t.warp != wid) continue;
+                    const uint8_t f = (q == qw_first) ? (uint8_t)s_meta[wid].fmt : P.fmt[t.col];
+                    const bool ind = (f == F_INDICATOR || f == F_INTERCEPT);
+                    const bool staged = (q == qw_first) && w_staged;
+                    double g = 0.0, h = 0.0;
+                    double2 A[kEw];
+                    double Dn[kEw];
+                    Staged<kEw> sw;
+                    if (staged) {
+                        sw = s_wstage[tid];
+                        staged_gh<MODEL>(P, ind, sw, A, Dn, g, h);
+                    } else {
+                        gh_dispatch<MODEL>(P, t.col, f, t.p0, t.p1, lane, 32, g, h);
+                    }
+                    const double2 s = warp_sum2(make_double2(g, h));
+                    double d = 0.0;
+                    if (lane == 0) {
+                        const ColMeta m = (q == qw_first) ? s_meta[wid] : load_meta(P, t.col);
+                        double hd;
+                        d = meta_step(m, t.p1, s.x, s.y, hd);
+                        meta_write(P, t.col, m, d, hd);
+                    }
+                    d = __shfl_sync(0xffffffffu, d, 0);
+                    if (d != 0.0) {
+                        if (staged) staged_update(P, sw, A, Dn, d);
+                        else update_dispatch(P, t.col, f, t.p0, t.p1, lane, 32, d);
+                    }
+                }
             }
-            // phase 2b: one warp per short column
-            const int qw0 = sg.n_chunk + sg.n_cta, qw1 = qw0 + sg.n_warp;
-            for (int q = qw0; q < qw1; ++q) {
-                const Task t = T[q];
-                if (t.warp != wid) continue;
-                const uint8_t f = P.fmt[t.col];
-                double g = 0.0, h = 0.0;
-                gh_dispatch<MODEL>(P, t.col, f, t.p0, t.p1, lane, 32, g, h);
-                const double2 s = warp_sum2(make_double2(g, h));
-                double d = 0.0;
-                if (lane == 0)
-                    d = column_step(P, t.col, t.p1, s.x, s.y, __ldcg(P.beta + t.col),
-                                    __ldcg(P.hdelta + t.col), true);
-                d = __shfl_sync(0xffffffffu, d, 0);
-                if (d != 0.0) update_dispatch(P, t.col, f, t.p0, t.p1, lane, 32, d);
-            }
-            // phase 3: split columns -- combine partials, step, scatter own chunk
+
+            if (P.trace2 && it == 0 && lane == 0) atomicMax(P.trace2 + 2 * si + 1, global_ns());
+            // ---- phase 3: split columns -- combine partials, step, scatter own chunk
             for (int q = 0; q < sg.n_chunk; ++q) {
-                const Task t = T[q];
+                const Task t = (q == 0) ? tc : T[q];
                 if (tid == 0) {
                     const unsigned target = (unsigned)(it + 1) * (unsigned)t.nchunks;
                     if (!wait_geq(P.col_arrive + t.col, target, P.wait_limit_ns, P.st, E_WAIT_COLUMN,
@@ -278,22 +513,38 @@ __global__ void __launch_bounds__(kThreads, 1) indep_sweep_kernel(IndepParams P)
                             s.x += v.x;
                             s.y += v.y;
                         }
-                        // split columns are never empty
-                        s_delta = column_step(P, t.col, 1, s.x, s.y, s_stash[q].x,
-                                              s_stash[q].y, t.chunk == 0);
+                        ColMeta m = (q == 0) ? s_meta[kWarps] : load_meta(P, t.col);
+                        m.beta = s_stash[q].x;  // values read before this CTA arrived
+                        m.hd = s_stash[q].y;
+                        double hd;
+                        const double d = meta_step(m, 1, s.x, s.y, hd);  // split columns are never empty
+                        if (t.chunk == 0) meta_write(P, t.col, m, d, hd);
+                        s_delta = d;
                     }
                 }
                 __syncthreads();
                 if (s_fail) return;
                 const double d = s_delta;
-                if (d != 0.0) update_dispatch(P, t.col, P.fmt[t.col], t.p0, t.p1, tid, blockDim.x, d);
+                if (d != 0.0) {
+                    if (q == 0 && c_staged) {
+                        // re-stage (cache hits) and re-gather this chunk: keeping phase 1's
+                        // registers alive across phase 2 would spill
+                        Staged<kE> s2;
+                        stage_entries(P, t, tid, blockDim.x, s2);
+                        double2 A[kE];
+                        double Dn[kE];
+                        double g = 0.0, h = 0.0;
+                        staged_gh<MODEL>(P, true, s2, A, Dn, g, h);
+                        staged_update(P, s2, A, Dn, d);
+                    } else {
+                        update_dispatch(P, t.col, P.fmt[t.col], t.p0, t.p1, tid, blockDim.x, d);
+                    }
+                }
                 __syncthreads();
             }
             __syncthreads();
-            if (tid == 0) {
-                __threadfence();
-                atomicAdd(P.level_done + sg.level, 1u);
-            }
+            if (tid == 0) red_release_gpu_add(P.level_done + sg.level, 1u);
+            if (P.trace && it == 0 && tid == 0) P.trace[3 * si + 2] = global_ns();
         }
         // the objective reads every row: wait until the last level is complete
         if (tid == 0) {

@@ -46,6 +46,11 @@ struct IndepParams {
     double ll_fixed;
     DevStatus* st;
     long long wait_limit_ns;  // bound on any single device-side wait
+    // optional per-segment timestamps of the first sweep (profiling aid):
+    // trace[3*si + {0,1,2}] = globaltimer at wait start, wait end, arrival
+    unsigned long long* trace;
+    // finer points: trace2[2*si] = end of phase 1, trace2[2*si+1] = last warp's end of phase 2
+    unsigned long long* trace2;
 };
 
 int indep_threads();
