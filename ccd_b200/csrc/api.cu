@@ -132,6 +132,7 @@ Fit::~Fit() {
                     (void*)gh_parts, (void*)gh_out})
         ctx->release(p);
     release_schedule();
+    if (is_cox()) cox_release();
     for (cudaEvent_t e : {ev0, ev1, evc0, evc1})
         if (e) cudaEventDestroy(e);
 }
@@ -184,6 +185,10 @@ IndepParams Fit::params() const {
 // (ModelSpecifics.hpp:427-484, 570-587, 486-524).  Independent rows: the
 // N-weights equal the row weights (observationCount = 1).
 void Fit::apply_weights() {
+    if (is_cox()) {
+        cox_apply_weights();
+        return;
+    }
     std::vector<double> wh(K, 1.0);
     if (weighted) wh = w_h;
     check_cuda(cudaMemcpyAsync(w, wh.data(), sizeof(double) * K, cudaMemcpyHostToDevice, stream),
@@ -240,6 +245,10 @@ void Fit::compute_xbeta() {
 
 // computeRemainingStatistics (ModelSpecifics.hpp:1588-1633).
 void Fit::remaining_statistics() {
+    if (is_cox()) {
+        cox_remaining();
+        return;
+    }
     const double null_denom = (model == M_LOGISTIC) ? 1.0 : 0.0;
     check_cuda(launch_remaining_stats(row, xb_pending ? xb_tmp : nullptr, w, K, null_denom, stream),
                "remaining statistics");
@@ -297,6 +306,10 @@ void Fit::ensure_schedule() {
 // current state, reduced in a fixed order.
 void Fit::objective_terms(double* out4) {
     check_lazy();
+    if (is_cox()) {
+        cox_objective_terms(out4);
+        return;
+    }
     const int nb = ctx->n_sm;
     IndepParams P = params();
     check_cuda(launch_indep_objective(P, nb, stream), "objective");
@@ -332,6 +345,14 @@ double Fit::objective(int conv) {
 
 void Fit::gradient_hessian(int j, double* g, double* h) {
     check_lazy();
+    if (is_cox()) {
+        const int32_t col = j;
+        double2 r;
+        cox_gh_batch(&col, 1, &r);
+        *g = r.x;
+        *h = r.y;
+        return;
+    }
     IndepParams P = params();
     check_cuda(launch_indep_gh(P, j, m->entries(j), gh_parts, kGhParts, gh_out, stream), "gh");
     launches += 2;
@@ -347,6 +368,11 @@ void Fit::update_xbeta(int j, double delta) {
     beta_h[j] += delta;
     check_cuda(cudaMemcpyAsync(beta + j, &beta_h[j], sizeof(double), cudaMemcpyHostToDevice, stream),
                "beta j");
+    if (is_cox()) {
+        cox_update(j, delta);
+        check_cuda(cudaStreamSynchronize(stream), "update sync");
+        return;
+    }
     IndepParams P = params();
     check_cuda(launch_indep_update(P, j, m->fmt[j], m->entries(j), delta, stream), "update");
     launches += m->entries(j) > 0 ? 1 : 0;
@@ -404,6 +430,12 @@ void Fit::find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* 
         *ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
         check_cuda(cudaMemcpyAsync(hdelta, hd.data(), sizeof(double) * J, cudaMemcpyHostToDevice, stream),
                    "bounds");
+        return;
+    }
+    if (is_cox()) {
+        auto t0 = std::chrono::steady_clock::now();
+        find_mode_batched(a, bound, flag, iters, obj);
+        *ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
         return;
     }
     ensure_schedule();
@@ -469,6 +501,72 @@ void Fit::find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* 
     *iters = out.iterations;
     *obj = out.objective;
     beta_dirty_host = true;
+}
+
+// findMode with speculative batches: the gradients of a run of consecutive
+// coordinates are computed together against the same state; walking them in
+// order, every zero step leaves the state untouched, so the next coordinate's
+// gradient is exactly what a sequential sweep would compute.  At the first
+// nonzero step the update is applied and the batch restarts after it.  The
+// visiting order and every step are those of the sequential cycle
+// (CyclicCoordinateDescent.cpp:1008-1021); only the wasted speculative
+// gradients cost extra.  Batches shrink after a restart and grow while steps
+// stay zero.
+void Fit::find_mode_batched(const ccdb_mode_args& a, double bound, int* flag, int* iters, double* obj) {
+    std::vector<double> hd(J, bound);
+    std::vector<int32_t> cols;
+    for (int j = 0; j < J; ++j)
+        if (!fixed[j]) cols.push_back(j);
+    const int n_active = (int)cols.size();
+    std::vector<double2> gh(kBatchMax);
+    double last = objective(a.convergence_type);
+    int iteration = 0;
+    bool done = false;
+    while (!done) {
+        int pos = 0, batch = 32;
+        while (pos < n_active) {
+            const int nb = std::min(batch, n_active - pos);
+            cox_gh_batch(cols.data() + pos, nb, gh.data());
+            int advanced = nb;
+            for (int i = 0; i < nb; ++i) {
+                const int j = cols[pos + i];
+                double delta = newton_prior_delta(gh[i].x, gh[i].y, beta_h[j], ptype_h[j], pvar_h[j]);
+                delta = apply_bounds(delta, hd[j]);
+                if (delta != 0.0) {
+                    beta_h[j] += delta;
+                    cox_update(j, delta);
+                    advanced = i + 1;
+                    break;
+                }
+            }
+            pos += advanced;
+            batch = (advanced == nb) ? std::min(2 * batch, (int)kBatchMax) : 32;
+        }
+        upload_beta();
+        ++iteration;
+        const double cur = objective(a.convergence_type);
+        double conv;
+        bool ill = false;
+        if (cur != cur) {
+            conv = 0.0;
+            ill = true;
+        } else {
+            conv = std::fabs(cur - last) / (std::fabs(cur) + 1.0);
+        }
+        last = cur;
+        if (a.tolerance > 0 && conv < a.tolerance) {
+            *flag = ill ? R_ILLCONDITIONED : R_SUCCESS;
+            done = true;
+        } else if (iteration == a.max_iterations) {
+            *flag = R_MAX_ITERATIONS;
+            done = true;
+        }
+    }
+    check_cuda(cudaMemcpyAsync(hdelta, hd.data(), sizeof(double) * J, cudaMemcpyHostToDevice, stream),
+               "bounds");
+    check_cuda(cudaStreamSynchronize(stream), "batched sync");
+    *iters = iteration;
+    *obj = last;
 }
 
 void Fit::find_mode(const ccdb_mode_args& a, double* beta_inout, ccdb_fit_result* res) {
@@ -670,8 +768,10 @@ int ccdb_fit_create(ccdb_context* ctx, const ccdb_matrix* m, const ccdb_fit_desc
     return guard([&] {
         require(ctx && m && d && out && d->y, "NULL argument");
         require(m->ctx == ctx, "matrix belongs to another context");
-        if (d->model_type != M_LOGISTIC && d->model_type != M_POISSON)
+        if (d->model_type != M_LOGISTIC && d->model_type != M_POISSON && d->model_type != M_COX)
             throw Error(CCDB_ERR_UNSUPPORTED, "model type not supported by this engine");
+        if (d->model_type == M_COX && !d->time)
+            throw Error(CCDB_ERR_INVALID, "Cox fits need survival times");
         if (d->precision != CCDB_PRECISION_FP64)
             throw Error(CCDB_ERR_UNSUPPORTED, "precision not supported for this model");
         check_cuda(cudaSetDevice(ctx->device), "cudaSetDevice");
@@ -687,7 +787,10 @@ int ccdb_fit_create(ccdb_context* ctx, const ccdb_matrix* m, const ccdb_fit_desc
         f->y_h.assign(d->y, d->y + m->K);
         const int64_t K = m->K;
         const int J = m->J;
-        f->row = static_cast<double2*>(ctx->alloc(sizeof(double2) * 2 * K));
+        if (d->time) f->time_h.assign(d->time, d->time + K);
+        if (d->stratum) f->stratum_h.assign(d->stratum, d->stratum + K);
+        else f->stratum_h.assign(K, 0);  // one stratum, as R's rep(1, n) for unstratified Cox
+        if (f->model != M_COX) f->row = static_cast<double2*>(ctx->alloc(sizeof(double2) * 2 * K));
         f->y = upload(ctx, d->y, K, f->stream);
         f->beta = static_cast<double*>(ctx->alloc(sizeof(double) * J));
         f->hdelta = static_cast<double*>(ctx->alloc(sizeof(double) * J));
@@ -718,6 +821,7 @@ int ccdb_fit_create(ccdb_context* ctx, const ccdb_matrix* m, const ccdb_fit_desc
             f->xb_known = false;  // xBeta = 0: computed (zero-filled) on first use
         }
         f->upload_beta();
+        if (f->model == M_COX) f->cox_allocate();
         check_cuda(cudaStreamSynchronize(f->stream), "fit upload");
         *out = f.release();
     });
@@ -788,11 +892,13 @@ int ccdb_get_xbeta(ccdb_fit* f, double* out) {
     return guard([&] {
         require(f && out, "NULL argument");
         f->check_lazy();
-        std::vector<double2> r(2 * f->K);
-        check_cuda(cudaMemcpyAsync(r.data(), f->row, sizeof(double2) * 2 * f->K, cudaMemcpyDeviceToHost,
+        const int stride = f->is_cox() ? 1 : 2;
+        const double2* src = f->is_cox() ? f->cox.xbe : f->row;
+        std::vector<double2> r(stride * f->K);
+        check_cuda(cudaMemcpyAsync(r.data(), src, sizeof(double2) * stride * f->K, cudaMemcpyDeviceToHost,
                                    f->stream), "xbeta copy");
         check_cuda(cudaStreamSynchronize(f->stream), "sync");
-        for (int64_t k = 0; k < f->K; ++k) out[k] = r[2 * k].x;
+        for (int64_t k = 0; k < f->K; ++k) out[k] = r[stride * k].x;
     });
 }
 

@@ -12,17 +12,6 @@
 
 namespace ccdb {
 
-// log-density of one coefficient (priors/CovariatePrior.h:220-224, :404-408).
-__device__ __forceinline__ double log_prior_one(double x, int ptype, double var) {
-    if (ptype == 1) {
-        const double lambda = sqrt(2.0 / var);
-        return log(0.5 * lambda) - lambda * fabs(x);
-    } else if (ptype == 2) {
-        return -0.5 * log(2.0 * 3.14159265358979323846 * var) - 0.5 * x * x / var;
-    }
-    return 0.0;
-}
-
 // ---------------------------------------------------------------- reductions
 __device__ __forceinline__ double2 warp_sum2(double2 v) {
 #pragma unroll

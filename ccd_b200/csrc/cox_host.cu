@@ -1,0 +1,236 @@
+// cox_host.cu -- host side of the Breslow Cox engine: risk-set grouping,
+// per-group tables, and the per-coordinate calls on the device.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "cox.h"
+#include "engine.h"
+
+namespace ccdb {
+
+// setPidForAccumulation (ModelSpecifics.hpp:1809-1868) on rows sorted by
+// (stratum, -time, y): group id per row (N for rows dropped by a zero weight)
+// and the number of groups N.  Integer work, identical to the reference.
+int64_t cox_group_rows(const std::vector<int32_t>& pid0, const std::vector<double>& time,
+                       const std::vector<double>& y, const double* weights,
+                       std::vector<int32_t>& grp) {
+    const int64_t K = (int64_t)y.size();
+    const int ignore = -1;
+    grp.assign(K, 0);
+    for (int64_t k = 0; k < K; ++k) grp[k] = pid0[k];
+    int64_t index = 0;
+    while (weights != nullptr && index < K && weights[index] == 0.0) {
+        grp[index] = ignore;
+        index++;
+    }
+    if (index >= K) {  // every row dropped
+        for (int64_t k = 0; k < K; ++k) grp[k] = 0;
+        return 0;
+    }
+    int lastPid = grp[index];
+    double lastTime = time[index];
+    double lastEvent = y[index];
+    int pid = grp[index] = 0;
+    for (int64_t k = index + 1; k < K; ++k) {
+        if (weights == nullptr || weights[k] != 0.0) {
+            const int nextPid = grp[k];
+            if (nextPid != lastPid) {
+                pid++;
+                lastPid = nextPid;
+            } else if (!(lastEvent == 1.0 && lastTime == time[k] && lastEvent == y[k])) {
+                pid++;
+            }
+            lastTime = time[k];
+            lastEvent = y[k];
+            grp[k] = pid;
+        } else {
+            grp[k] = ignore;
+        }
+    }
+    const int64_t N = (int64_t)pid + 1;
+    for (int64_t k = 0; k < K; ++k)
+        if (grp[k] == ignore) grp[k] = (int32_t)N;
+    return N;
+}
+
+CoxParams Fit::cox_params() const {
+    CoxParams P{};
+    P.col_ptr = m->d_col_ptr;
+    P.rows = m->d_rows;
+    P.val_ptr = m->d_val_ptr;
+    P.vals = m->d_vals;
+    P.fmt = m->d_fmt;
+    P.K = K;
+    P.N = cox.N;
+    P.xbe = cox.xbe;
+    P.w = w;
+    P.y = y;
+    P.grp = cox.grp;
+    P.rstrat = cox.rstrat;
+    P.weighted = weighted ? 1 : 0;
+    P.denom = cox.denom;
+    P.D = cox.D;
+    P.S1 = cox.S1;
+    P.S2 = cox.S2;
+    P.nEv = cox.nEv;
+    P.gfirst = cox.gfirst;
+    P.glast = cox.glast;
+    P.grow = cox.grow;
+    P.xjy = xjy;
+    P.st = st;
+    P.wait_limit_ns = wait_limit_ns;
+    return P;
+}
+
+void Fit::cox_allocate() {
+    const size_t G = (size_t)K + 1;  // the most groups any weighting can produce, + slot N
+    cox.xbe = static_cast<double2*>(ctx->alloc(sizeof(double2) * K));
+    cox.grp = static_cast<int32_t*>(ctx->alloc(sizeof(int32_t) * K));
+    cox.rstrat = static_cast<int32_t*>(ctx->alloc(sizeof(int32_t) * K));
+    cox.denom = static_cast<double*>(ctx->alloc(sizeof(double) * G));
+    cox.D = static_cast<double*>(ctx->alloc(sizeof(double) * G));
+    cox.S1 = static_cast<double*>(ctx->alloc(sizeof(double) * G));
+    cox.S2 = static_cast<double*>(ctx->alloc(sizeof(double) * G));
+    cox.nEv = static_cast<double*>(ctx->alloc(sizeof(double) * G));
+    cox.gfirst = static_cast<uint8_t*>(ctx->alloc(G));
+    cox.glast = static_cast<uint8_t*>(ctx->alloc(G));
+    cox.grow = static_cast<int64_t*>(ctx->alloc(sizeof(int64_t) * (G + 1)));
+    const int tiles = cox_scan_tiles((int64_t)G);
+    cox.tickets = static_cast<unsigned*>(ctx->alloc(2 * sizeof(unsigned)));
+    cox.status = static_cast<int*>(ctx->alloc(sizeof(int) * 2 * std::max(1, tiles)));
+    cox.tails = ctx->alloc(cox_tail_bytes() * 2 * std::max(1, tiles));
+    cox.batch_cols = static_cast<int32_t*>(ctx->alloc(sizeof(int32_t) * kBatchMax));
+    cox.batch_out = static_cast<double2*>(ctx->alloc(sizeof(double2) * kBatchMax));
+    check_cuda(cudaMemsetAsync(cox.status, 0, sizeof(int) * 2 * std::max(1, tiles), stream), "status");
+    check_cuda(cudaMemsetAsync(cox.S1, 0, sizeof(double) * G, stream), "S1");
+    check_cuda(cudaMemsetAsync(cox.S2, 0, sizeof(double) * G, stream), "S2");
+    check_cuda(cudaMemsetAsync(cox.xbe, 0, sizeof(double2) * K, stream), "xbe");
+    // stratum index of each row, as ModelData::loadY numbers them (ModelData.cpp:96-125)
+    std::vector<int32_t> rs(K);
+    int32_t p = 0;
+    for (int64_t k = 0; k < K; ++k) {
+        if (k > 0 && stratum_h[k] != stratum_h[k - 1]) p++;
+        rs[k] = p;
+    }
+    pid0_h = rs;
+    check_cuda(cudaMemcpyAsync(cox.rstrat, rs.data(), sizeof(int32_t) * K, cudaMemcpyHostToDevice, stream),
+               "rstrat");
+    check_cuda(cudaStreamSynchronize(stream), "cox alloc");
+}
+
+void Fit::cox_release() {
+    for (void* p : {(void*)cox.xbe, (void*)cox.grp, (void*)cox.rstrat, (void*)cox.denom, (void*)cox.D,
+                    (void*)cox.S1, (void*)cox.S2, (void*)cox.nEv, (void*)cox.gfirst, (void*)cox.glast,
+                    (void*)cox.grow, (void*)cox.tickets, (void*)cox.status, cox.tails,
+                    (void*)cox.batch_cols, (void*)cox.batch_out})
+        ctx->release(p);
+}
+
+// setWeights for the Cox model (ModelSpecifics.hpp:427-484): regroup with the
+// weights, N-weights = events (observationCount = y) times weight per group,
+// then computeXjY (x * y * w; survival models use observationCount(y) = y).
+void Fit::cox_apply_weights() {
+    std::vector<double> wh(K, 1.0);
+    if (weighted) wh = w_h;
+    std::vector<int32_t> grp;
+    const int64_t N = cox_group_rows(pid0_h, time_h, y_h, weighted ? w_h.data() : nullptr, grp);
+    cox.N = N;
+    std::vector<double> nev(N + 1, 0.0);
+    for (int64_t k = 0; k < K; ++k) nev[grp[k]] += y_h[k] * wh[k];
+    std::vector<uint8_t> gf(N + 1, 0), gl(N + 1, 0);
+    std::vector<int64_t> grow(N + 2, K);
+    std::vector<int32_t> gstrat(N + 1, -1);
+    for (int64_t k = K - 1; k >= 0; --k)
+        if (grp[k] < N) {
+            grow[grp[k]] = k;
+            gstrat[grp[k]] = pid0_h[k];
+        }
+    for (int64_t g = N - 1; g >= 0; --g)
+        if (grow[g] == K) grow[g] = grow[g + 1];
+    for (int64_t g = 0; g < N; ++g) {
+        gf[g] = (g == 0 || gstrat[g] != gstrat[g - 1]) ? 1 : 0;
+        gl[g] = (g == N - 1 || gstrat[g] != gstrat[g + 1]) ? 1 : 0;
+    }
+    grow[N] = K;
+    check_cuda(cudaMemcpyAsync(w, wh.data(), sizeof(double) * K, cudaMemcpyHostToDevice, stream), "w");
+    check_cuda(cudaMemcpyAsync(cox.grp, grp.data(), sizeof(int32_t) * K, cudaMemcpyHostToDevice, stream), "grp");
+    check_cuda(cudaMemcpyAsync(cox.nEv, nev.data(), sizeof(double) * (N + 1), cudaMemcpyHostToDevice, stream), "nev");
+    check_cuda(cudaMemcpyAsync(cox.gfirst, gf.data(), N + 1, cudaMemcpyHostToDevice, stream), "gfirst");
+    check_cuda(cudaMemcpyAsync(cox.glast, gl.data(), N + 1, cudaMemcpyHostToDevice, stream), "glast");
+    check_cuda(cudaMemcpyAsync(cox.grow, grow.data(), sizeof(int64_t) * (N + 1), cudaMemcpyHostToDevice, stream),
+               "grow");
+    check_cuda(cudaMemsetAsync(cox.S1 + N, 0, sizeof(double), stream), "S1N");
+    check_cuda(cudaMemsetAsync(cox.S2 + N, 0, sizeof(double), stream), "S2N");
+    check_cuda(launch_xjy(m->d_col_ptr, m->d_rows, m->d_val_ptr, m->d_vals, m->d_fmt, y,
+                          weighted ? w : nullptr, K, J, xjy, stream),
+               "xjy");
+    ++launches;
+    ll_fixed = 0.0;
+    check_cuda(cudaStreamSynchronize(stream), "cox weights");
+    valid_weights = true;
+    suff_known = false;
+}
+
+void Fit::cox_scans() {
+    ++cox.epoch;
+    CoxParams P = cox_params();
+    check_cuda(launch_cox_scans(P, cox.tickets, cox.status, cox.tails, cox.epoch, stream), "cox scans");
+    launches += 2;
+}
+
+// computeRemainingStatistics (ModelSpecifics.hpp:1588-1617) + the accumulated scans.
+void Fit::cox_remaining() {
+    if (xb_pending) {  // xBeta computed into xb_tmp: place it into {xBeta, e}
+        check_cuda(cudaMemcpy2DAsync(cox.xbe, sizeof(double2), xb_tmp, sizeof(double), sizeof(double), K,
+                                     cudaMemcpyDeviceToDevice, stream),
+                   "xb place");
+        xb_pending = false;
+    }
+    CoxParams P = cox_params();
+    check_cuda(launch_cox_remaining(P, stream), "cox remaining");
+    launches += 2;
+    cox_scans();
+    suff_known = true;
+}
+
+void Fit::cox_objective_terms(double* out4) {
+    const int nb = ctx->n_sm;
+    CoxParams P = cox_params();
+    check_cuda(launch_cox_objective(P, red, nb, stream), "cox objective");
+    ++launches;
+    std::vector<double2> parts(2 * nb);
+    check_cuda(cudaMemcpyAsync(parts.data(), red, sizeof(double2) * 2 * nb, cudaMemcpyDeviceToHost, stream),
+               "objective copy");
+    check_cuda(cudaStreamSynchronize(stream), "objective sync");
+    double t[4] = {0, 0, 0, 0};
+    for (int c = 0; c < nb; ++c) {
+        t[0] += parts[2 * c].x;
+        t[1] += parts[2 * c].y;
+        t[2] += parts[2 * c + 1].x;
+    }
+    // log prior on the host (JointPrior.h:121-128)
+    for (int j = 0; j < J; ++j) t[3] += log_prior_host(beta_h[j], ptype_h[j], pvar_h[j]);
+    for (int i = 0; i < 4; ++i) out4[i] = t[i];
+}
+
+void Fit::cox_gh_batch(const int32_t* cols, int n, double2* out) {
+    check_cuda(cudaMemcpyAsync(cox.batch_cols, cols, sizeof(int32_t) * n, cudaMemcpyHostToDevice, stream),
+               "batch cols");
+    CoxParams P = cox_params();
+    check_cuda(launch_cox_gh(P, cox.batch_cols, n, cox.batch_out, stream), "cox gh");
+    ++launches;
+    check_cuda(cudaMemcpyAsync(out, cox.batch_out, sizeof(double2) * n, cudaMemcpyDeviceToHost, stream),
+               "gh copy");
+    check_cuda(cudaStreamSynchronize(stream), "gh sync");
+}
+
+void Fit::cox_update(int j, double delta) {
+    CoxParams P = cox_params();
+    check_cuda(launch_cox_update(P, j, delta, stream), "cox update");
+    ++launches;
+    cox_scans();
+}
+
+}  // namespace ccdb

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/ccdb.h"
+#include "cox.h"
 #include "indep.h"
 #include "schedule.h"
 #include "step.h"
@@ -69,8 +70,29 @@ struct DevSchedule {
     double2* partials = nullptr;
 };
 
+// Device tables of the Breslow Cox engine (cox.cu).
+struct CoxDev {
+    int64_t N = 0;  // risk-set groups
+    int epoch = 0;  // scan epoch (status words are never reset)
+    double2* xbe = nullptr;
+    int32_t* grp = nullptr;
+    int32_t* rstrat = nullptr;
+    double *denom = nullptr, *D = nullptr, *S1 = nullptr, *S2 = nullptr, *nEv = nullptr;
+    uint8_t *gfirst = nullptr, *glast = nullptr;
+    int64_t* grow = nullptr;
+    unsigned* tickets = nullptr;
+    int* status = nullptr;
+    void* tails = nullptr;
+    int32_t* batch_cols = nullptr;
+    double2* batch_out = nullptr;
+};
+
+int64_t cox_group_rows(const std::vector<int32_t>& pid0, const std::vector<double>& time,
+                       const std::vector<double>& y, const double* weights, std::vector<int32_t>& grp);
+
 struct Fit {
     static constexpr int kGhParts = 1024;
+    static constexpr int kBatchMax = 1024;  // columns per speculative gradient batch
     Context* ctx = nullptr;
     const Matrix* m = nullptr;
     int model = 0, precision = 0;
@@ -99,9 +121,12 @@ struct Fit {
     cudaEvent_t evc0 = nullptr, evc1 = nullptr;  // around a whole find_mode
     int64_t launches = 0;                        // engine kernels launched so far
     std::unique_ptr<DevSchedule> sched;
+    CoxDev cox;
 
     // host mirror and lazy flags (CyclicCoordinateDescent.h:152-166)
-    std::vector<double> y_h, w_h, beta_h, pvar_h;
+    std::vector<double> y_h, w_h, beta_h, pvar_h, time_h;
+    std::vector<int64_t> stratum_h;
+    std::vector<int32_t> pid0_h;
     std::vector<int32_t> ptype_h;
     std::vector<uint8_t> fixed;
     bool weighted = false;
@@ -127,6 +152,19 @@ struct Fit {
     void find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* iters, double* obj,
                         float* ms);
     void find_mode(const ccdb_mode_args& a, double* beta_inout, ccdb_fit_result* res);
+    // speculative batched sweeps (models without a fused sweep kernel)
+    void find_mode_batched(const ccdb_mode_args& a, double bound, int* flag, int* iters, double* obj);
+    bool is_cox() const { return model == M_COX; }
+    // Cox engine (cox_host.cu)
+    CoxParams cox_params() const;
+    void cox_allocate();
+    void cox_release();
+    void cox_apply_weights();
+    void cox_scans();
+    void cox_remaining();
+    void cox_objective_terms(double* out4);
+    void cox_gh_batch(const int32_t* cols, int n, double2* out);
+    void cox_update(int j, double delta);
 };
 
 }  // namespace ccdb

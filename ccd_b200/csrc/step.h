@@ -55,4 +55,18 @@ CCDB_HD double apply_bounds(double delta, double& hd) {
     return delta;
 }
 
+// log-density of one coefficient (priors/CovariatePrior.h:220-224, :404-408).
+CCDB_HD double log_prior_one(double x, int ptype, double var) {
+    if (ptype == 1) {
+        const double lambda = sqrt(2.0 / var);
+        return log(0.5 * lambda) - lambda * fabs(x);
+    } else if (ptype == 2) {
+        return -0.5 * log(2.0 * 3.14159265358979323846 * var) - 0.5 * x * x / var;
+    }
+    return 0.0;
+}
+
+// host alias used by the host-side objective
+inline double log_prior_host(double x, int ptype, double var) { return log_prior_one(x, ptype, var); }
+
 }  // namespace ccdb
