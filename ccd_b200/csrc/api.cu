@@ -132,7 +132,7 @@ Fit::~Fit() {
                     (void*)gh_parts, (void*)gh_out})
         ctx->release(p);
     release_schedule();
-    if (is_cox()) cox_release();
+    if (group_engine()) cox_release();
     for (cudaEvent_t e : {ev0, ev1, evc0, evc1})
         if (e) cudaEventDestroy(e);
 }
@@ -185,7 +185,7 @@ IndepParams Fit::params() const {
 // (ModelSpecifics.hpp:427-484, 570-587, 486-524).  Independent rows: the
 // N-weights equal the row weights (observationCount = 1).
 void Fit::apply_weights() {
-    if (is_cox()) {
+    if (group_engine()) {
         cox_apply_weights();
         return;
     }
@@ -245,7 +245,7 @@ void Fit::compute_xbeta() {
 
 // computeRemainingStatistics (ModelSpecifics.hpp:1588-1633).
 void Fit::remaining_statistics() {
-    if (is_cox()) {
+    if (group_engine()) {
         cox_remaining();
         return;
     }
@@ -306,7 +306,7 @@ void Fit::ensure_schedule() {
 // current state, reduced in a fixed order.
 void Fit::objective_terms(double* out4) {
     check_lazy();
-    if (is_cox()) {
+    if (group_engine()) {
         cox_objective_terms(out4);
         return;
     }
@@ -345,7 +345,7 @@ double Fit::objective(int conv) {
 
 void Fit::gradient_hessian(int j, double* g, double* h) {
     check_lazy();
-    if (is_cox()) {
+    if (group_engine()) {
         const int32_t col = j;
         double2 r;
         cox_gh_batch(&col, 1, &r);
@@ -368,7 +368,7 @@ void Fit::update_xbeta(int j, double delta) {
     beta_h[j] += delta;
     check_cuda(cudaMemcpyAsync(beta + j, &beta_h[j], sizeof(double), cudaMemcpyHostToDevice, stream),
                "beta j");
-    if (is_cox()) {
+    if (group_engine()) {
         cox_update(j, delta);
         check_cuda(cudaStreamSynchronize(stream), "update sync");
         return;
@@ -432,7 +432,7 @@ void Fit::find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* 
                    "bounds");
         return;
     }
-    if (is_cox()) {
+    if (group_engine()) {
         auto t0 = std::chrono::steady_clock::now();
         find_mode_batched(a, bound, flag, iters, obj);
         *ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -768,8 +768,11 @@ int ccdb_fit_create(ccdb_context* ctx, const ccdb_matrix* m, const ccdb_fit_desc
     return guard([&] {
         require(ctx && m && d && out && d->y, "NULL argument");
         require(m->ctx == ctx, "matrix belongs to another context");
-        if (d->model_type != M_LOGISTIC && d->model_type != M_POISSON && d->model_type != M_COX)
+        if (d->model_type != M_LOGISTIC && d->model_type != M_POISSON && d->model_type != M_COX &&
+            d->model_type != M_CLR && d->model_type != M_CPR)
             throw Error(CCDB_ERR_UNSUPPORTED, "model type not supported by this engine");
+        if ((d->model_type == M_CLR || d->model_type == M_CPR) && !d->stratum)
+            throw Error(CCDB_ERR_INVALID, "conditional models need stratum ids");
         if (d->model_type == M_COX && !d->time)
             throw Error(CCDB_ERR_INVALID, "Cox fits need survival times");
         if (d->precision != CCDB_PRECISION_FP64)
@@ -790,7 +793,8 @@ int ccdb_fit_create(ccdb_context* ctx, const ccdb_matrix* m, const ccdb_fit_desc
         if (d->time) f->time_h.assign(d->time, d->time + K);
         if (d->stratum) f->stratum_h.assign(d->stratum, d->stratum + K);
         else f->stratum_h.assign(K, 0);  // one stratum, as R's rep(1, n) for unstratified Cox
-        if (f->model != M_COX) f->row = static_cast<double2*>(ctx->alloc(sizeof(double2) * 2 * K));
+        const bool grp_engine = (f->model == M_COX || f->model == M_CLR || f->model == M_CPR);
+        if (!grp_engine) f->row = static_cast<double2*>(ctx->alloc(sizeof(double2) * 2 * K));
         f->y = upload(ctx, d->y, K, f->stream);
         f->beta = static_cast<double*>(ctx->alloc(sizeof(double) * J));
         f->hdelta = static_cast<double*>(ctx->alloc(sizeof(double) * J));
@@ -821,7 +825,7 @@ int ccdb_fit_create(ccdb_context* ctx, const ccdb_matrix* m, const ccdb_fit_desc
             f->xb_known = false;  // xBeta = 0: computed (zero-filled) on first use
         }
         f->upload_beta();
-        if (f->model == M_COX) f->cox_allocate();
+        if (grp_engine) f->cox_allocate();
         check_cuda(cudaStreamSynchronize(f->stream), "fit upload");
         *out = f.release();
     });
@@ -892,8 +896,8 @@ int ccdb_get_xbeta(ccdb_fit* f, double* out) {
     return guard([&] {
         require(f && out, "NULL argument");
         f->check_lazy();
-        const int stride = f->is_cox() ? 1 : 2;
-        const double2* src = f->is_cox() ? f->cox.xbe : f->row;
+        const int stride = f->group_engine() ? 1 : 2;
+        const double2* src = f->group_engine() ? f->cox.xbe : f->row;
         std::vector<double2> r(stride * f->K);
         check_cuda(cudaMemcpyAsync(r.data(), src, sizeof(double2) * stride * f->K, cudaMemcpyDeviceToHost,
                                    f->stream), "xbeta copy");
@@ -948,6 +952,20 @@ int ccdb_fit_model(ccdb_context* ctx, int64_t K, int32_t J, const int64_t* col_s
     if (m) ccdb_matrix_destroy(m);
     g_last_error = err;
     return rc;
+}
+
+int ccdb_sweep_levels(int64_t K, int32_t J, const int64_t* col_start, const int32_t* rows,
+                      const uint8_t* fmt, const uint8_t* fixed, int32_t* level_out, int32_t* n_levels) {
+    return guard([&] {
+        require(col_start && fmt && level_out && n_levels && K > 0 && J > 0, "bad argument");
+        std::vector<int64_t> entries(J);
+        for (int j = 0; j < J; ++j)
+            entries[j] = (fmt[j] == F_DENSE || fmt[j] == F_INTERCEPT) ? K : col_start[j + 1] - col_start[j];
+        ScheduleParams sp;
+        const Schedule s = build_schedule(K, J, col_start, rows, fmt, fixed, nullptr, K, entries.data(), sp);
+        std::copy(s.level_of.begin(), s.level_of.end(), level_out);
+        *n_levels = s.n_levels;
+    });
 }
 
 }  // extern "C"

@@ -459,6 +459,183 @@ __global__ void __launch_bounds__(kT) cox_objective_kernel(CoxParams P, double2*
     }
 }
 
+// ================================================================== grouped models
+// ConditionalLogisticRegression / ConditionalPoissonRegression (GroupedData,
+// ModelSpecifics.h:329-342, :712-880): one denominator per stratum, no
+// accumulation.  The column's entries are walked in row order; numerators
+// accumulate per stratum and each stratum run contributes
+// t = numer / denom, g += nEv t, h += nEv t (1 - t) (indicator) or
+// nEv (numer2 / denom - t^2) (ModelSpecifics.hpp:1101-1179).  Numerators are
+// not weighted; CV weights act through nEv and XjY only.
+
+__global__ void __launch_bounds__(kT) grouped_gh_kernel(CoxParams P, const int32_t* cols, int ncols,
+                                                         double2* out) {
+    __shared__ Seg2 s_w[kW], s_w2[kW];
+    __shared__ Seg2 s_agg, s_agg2;
+    __shared__ double2 s_red[kW];
+    __shared__ int32_t s_key[kT + 1];
+    __shared__ double s_carry1, s_carry2;
+    __shared__ int32_t s_carry_key;
+
+    for (int c = blockIdx.x; c < ncols; c += gridDim.x) {
+        const int j = cols[c];
+        const uint8_t f = P.fmt[j];
+        const bool has_rows = (f == F_SPARSE || f == F_INDICATOR);
+        const bool has_vals = (f == F_SPARSE || f == F_DENSE);
+        const bool ind = (f == F_INDICATOR || f == F_INTERCEPT);
+        const int64_t cb = P.col_ptr[j], vb = P.val_ptr[j];
+        const int64_t n = has_rows ? (P.col_ptr[j + 1] - cb) : P.K;
+        double g = 0.0, h = 0.0;
+        if (threadIdx.x == 0) {
+            s_carry1 = 0.0;
+            s_carry2 = 0.0;
+            s_carry_key = -1;
+        }
+        __syncthreads();
+        for (int64_t base = 0; base < n; base += kT) {
+            const int64_t p = base + threadIdx.x;
+            double n1 = 0.0, n2 = 0.0;
+            int32_t key = 0x7fffffff;
+            if (p < n) {
+                const int64_t k = has_rows ? (int64_t)__ldg(P.rows + cb + p) : p;
+                const double x = has_vals ? __ldg(P.vals + vb + p) : 1.0;
+                const double e = __ldcg(P.xbe + k).y;
+                n1 = e * x;
+                if (!ind) n2 = e * x * x;
+                key = P.grp[k];
+            }
+            s_key[threadIdx.x] = key;
+            if (threadIdx.x == 0) s_key[kT] = 0x7fffffff;
+            __syncthreads();
+            // the run continues across tiles when the next tile starts with the same key
+            const int32_t carry_key = s_carry_key;
+            const int32_t prev_key = (threadIdx.x == 0) ? carry_key : s_key[threadIdx.x - 1];
+            const int start = (key != prev_key) ? 1 : 0;
+            Seg2 e1{start, n1}, e2{start, n2};
+            if (threadIdx.x == 0 && !start) {
+                e1.v = s_carry1 + n1;
+                e2.v = s_carry2 + n2;
+            }
+            __syncthreads();
+            const Seg2 r1 = block_seg_scan(e1, s_w, &s_agg);
+            const Seg2 r2 = block_seg_scan(e2, s_w2, &s_agg2);
+            // last entry of a stratum run (the next entry, possibly in the next tile, differs)
+            bool run_end = false;
+            if (p < n) {
+                if (threadIdx.x < kT - 1) {
+                    run_end = (s_key[threadIdx.x + 1] != key) || (p + 1 >= n);
+                } else if (p + 1 >= n) {
+                    run_end = true;
+                } else {
+                    // peek the next tile's first key
+                    const int64_t k2 = has_rows ? (int64_t)__ldg(P.rows + cb + p + 1) : p + 1;
+                    run_end = (P.grp[k2] != key);
+                }
+            }
+            if (run_end) {
+                const double numer = r1.v, numer2 = r2.v;
+                const double denom = __ldcg(P.denom + key);
+                const double nev = P.nEv[key];
+                const double t = numer / denom;
+                const double gg = nev * t;
+                g += gg;
+                if (ind) h += gg * (1.0 - t);
+                else h += nev * (numer2 / denom - t * t);
+            }
+            __syncthreads();
+            if (threadIdx.x == kT - 1) {
+                s_carry1 = r1.v;
+                s_carry2 = r2.v;
+                s_carry_key = key;
+            }
+            __syncthreads();
+        }
+        double2 v = warp_sum2(make_double2(g, h));
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        if (lane == 0) s_red[wid] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double G = 0.0, H = 0.0;
+            for (int w = 0; w < kW; ++w) {
+                G += s_red[w].x;
+                H += s_red[w].y;
+            }
+            out[c] = (n > 0) ? make_double2(G - P.xjy[j], H) : make_double2(0.0, 0.0);
+        }
+        __syncthreads();
+    }
+}
+
+// updateXBetaImpl, non-Cox branch (ModelSpecifics.hpp:1561-1571): the
+// stratum denominator takes e_new - e_old per row, in row order.
+__global__ void __launch_bounds__(kT) grouped_update_kernel(CoxParams P, int j, double delta) {
+    __shared__ double s_d[kT];
+    __shared__ int32_t s_g[kT];
+    const uint8_t f = P.fmt[j];
+    const bool has_rows = (f == F_SPARSE || f == F_INDICATOR);
+    const bool has_vals = (f == F_SPARSE || f == F_DENSE);
+    const int64_t cb = P.col_ptr[j], vb = P.val_ptr[j];
+    const int64_t n = has_rows ? (P.col_ptr[j + 1] - cb) : P.K;
+    for (int64_t base = 0; base < n; base += kT) {
+        const int64_t p = base + threadIdx.x;
+        int32_t grp = -1;
+        double dd = 0.0;
+        if (p < n) {
+            const int64_t k = has_rows ? (int64_t)__ldg(P.rows + cb + p) : p;
+            const double x = has_vals ? __ldg(P.vals + vb + p) : 1.0;
+            const double2 xe = P.xbe[k];
+            const double xb = xe.x + delta * x;
+            const double en = exp(xb);
+            P.xbe[k] = make_double2(xb, en);
+            grp = P.grp[k];
+            dd = en - xe.y;
+        }
+        s_d[threadIdx.x] = dd;
+        s_g[threadIdx.x] = grp;
+        __syncthreads();
+        if (p < n && (threadIdx.x == 0 || s_g[threadIdx.x - 1] != grp)) {
+            double d = P.denom[grp];
+            for (int q = threadIdx.x; q < kT && base + q < n && s_g[q] == grp; ++q) d = d + s_d[q];
+            P.denom[grp] = d;
+        }
+        __syncthreads();
+    }
+}
+
+// computeRemainingStatisticsImpl, non-Cox branch: denom[s] = 0 + sum of e over
+// the stratum's rows in row order.  grow holds each stratum's first row.
+__global__ void grouped_denom_kernel(CoxParams P) {
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < P.N;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        double d = 0.0;
+        for (int64_t k = P.grow[s]; k < P.grow[s + 1]; ++k) d += P.xbe[k].y;
+        P.denom[s] = d;
+    }
+}
+
+// {sum w*y*xBeta, sum nEv*log(denom), sum w*y*xBeta, 0}
+__global__ void __launch_bounds__(kT) grouped_objective_kernel(CoxParams P, double2* red) {
+    __shared__ double4 s_red4[kW];
+    double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
+    const int64_t G = gridDim.x, b = blockIdx.x;
+    const int64_t k0 = P.K * b / G, k1 = P.K * (b + 1) / G;
+    for (int64_t k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+        const double xb = __ldcg(P.xbe + k).x;
+        const double yk = P.y[k];
+        const int yi = (int)yk;
+        acc.x += P.weighted ? (yi * xb) * P.w[k] : yi * xb;
+        acc.z += P.weighted ? xb * yk * P.w[k] : xb * yk;
+    }
+    const int64_t g0 = P.N * b / G, g1 = P.N * (b + 1) / G;
+    for (int64_t g = g0 + threadIdx.x; g < g1; g += blockDim.x)
+        acc.y += P.nEv[g] * log(__ldcg(P.denom + g));
+    acc = block_sum4<kW>(acc, s_red4);
+    if (threadIdx.x == 0) {
+        red[2 * b] = make_double2(acc.x, acc.y);
+        red[2 * b + 1] = make_double2(acc.z, 0.0);
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------- launchers
@@ -495,6 +672,29 @@ cudaError_t launch_cox_scans(const CoxParams& P, unsigned* tickets, int* status,
 }
 
 size_t cox_tail_bytes() { return sizeof(ScanStatus); }
+
+cudaError_t launch_grouped_gh(const CoxParams& P, const int32_t* cols, int ncols, double2* out,
+                              cudaStream_t s) {
+    if (ncols <= 0) return cudaSuccess;
+    grouped_gh_kernel<<<ncols, kT, 0, s>>>(P, cols, ncols, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grouped_update(const CoxParams& P, int j, double delta, cudaStream_t s) {
+    grouped_update_kernel<<<1, kT, 0, s>>>(P, j, delta);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grouped_remaining(const CoxParams& P, cudaStream_t s) {
+    cox_exp_kernel<<<1184, 256, 0, s>>>(P);
+    grouped_denom_kernel<<<1184, 256, 0, s>>>(P);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grouped_objective(const CoxParams& P, double2* red, int nblocks, cudaStream_t s) {
+    grouped_objective_kernel<<<nblocks, kT, 0, s>>>(P, red);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_cox_objective(const CoxParams& P, double2* red, int nblocks, cudaStream_t s) {
     cox_objective_kernel<<<nblocks, kT, 0, s>>>(P, red);

@@ -52,4 +52,12 @@ cudaError_t launch_cox_scans(const CoxParams& P, unsigned* tickets, int* status,
                              int epoch, cudaStream_t s);
 cudaError_t launch_cox_objective(const CoxParams& P, double2* red, int nblocks, cudaStream_t s);
 
+// Grouped models (conditional logistic / Poisson): grp = stratum, N = strata,
+// denom per stratum, grow = first row of each stratum.
+cudaError_t launch_grouped_gh(const CoxParams& P, const int32_t* cols, int ncols, double2* out,
+                              cudaStream_t s);
+cudaError_t launch_grouped_update(const CoxParams& P, int j, double delta, cudaStream_t s);
+cudaError_t launch_grouped_remaining(const CoxParams& P, cudaStream_t s);
+cudaError_t launch_grouped_objective(const CoxParams& P, double2* red, int nblocks, cudaStream_t s);
+
 }  // namespace ccdb

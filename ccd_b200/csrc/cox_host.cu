@@ -85,7 +85,17 @@ CoxParams Fit::cox_params() const {
 }
 
 void Fit::cox_allocate() {
-    const size_t G = (size_t)K + 1;  // the most groups any weighting can produce, + slot N
+    // stratum index of each row, as ModelData::loadY numbers them (ModelData.cpp:96-125)
+    std::vector<int32_t> rs(K);
+    int32_t p = 0;
+    for (int64_t k = 0; k < K; ++k) {
+        if (k > 0 && stratum_h[k] != stratum_h[k - 1]) p++;
+        rs[k] = p;
+    }
+    pid0_h = rs;
+    const int64_t n_strata = K > 0 ? (int64_t)p + 1 : 0;
+    // Cox: the most groups any weighting can produce; grouped models: the strata; + slot N
+    const size_t G = is_cox() ? (size_t)K + 1 : (size_t)n_strata + 1;
     cox.xbe = static_cast<double2*>(ctx->alloc(sizeof(double2) * K));
     cox.grp = static_cast<int32_t*>(ctx->alloc(sizeof(int32_t) * K));
     cox.rstrat = static_cast<int32_t*>(ctx->alloc(sizeof(int32_t) * K));
@@ -107,16 +117,19 @@ void Fit::cox_allocate() {
     check_cuda(cudaMemsetAsync(cox.S1, 0, sizeof(double) * G, stream), "S1");
     check_cuda(cudaMemsetAsync(cox.S2, 0, sizeof(double) * G, stream), "S2");
     check_cuda(cudaMemsetAsync(cox.xbe, 0, sizeof(double2) * K, stream), "xbe");
-    // stratum index of each row, as ModelData::loadY numbers them (ModelData.cpp:96-125)
-    std::vector<int32_t> rs(K);
-    int32_t p = 0;
-    for (int64_t k = 0; k < K; ++k) {
-        if (k > 0 && stratum_h[k] != stratum_h[k - 1]) p++;
-        rs[k] = p;
-    }
-    pid0_h = rs;
     check_cuda(cudaMemcpyAsync(cox.rstrat, rs.data(), sizeof(int32_t) * K, cudaMemcpyHostToDevice, stream),
                "rstrat");
+    if (is_grouped()) {  // the group of a row is its stratum (GroupedData::getGroup)
+        cox.N = n_strata;
+        std::vector<int64_t> grow(n_strata + 1, K);
+        for (int64_t k = K - 1; k >= 0; --k) grow[rs[k]] = k;
+        grow[n_strata] = K;
+        check_cuda(cudaMemcpyAsync(cox.grp, rs.data(), sizeof(int32_t) * K, cudaMemcpyHostToDevice, stream),
+                   "grp");
+        check_cuda(cudaMemcpyAsync(cox.grow, grow.data(), sizeof(int64_t) * (n_strata + 1),
+                                   cudaMemcpyHostToDevice, stream), "grow");
+        cox_grow_h = grow;
+    }
     check_cuda(cudaStreamSynchronize(stream), "cox alloc");
 }
 
@@ -134,6 +147,31 @@ void Fit::cox_release() {
 void Fit::cox_apply_weights() {
     std::vector<double> wh(K, 1.0);
     if (weighted) wh = w_h;
+    if (is_grouped()) {
+        // setWeights (ModelSpecifics.hpp:427-484): nEv per stratum = y * w
+        // (observationCount = y); computeXjY: x * y * w; fixed terms for CPR.
+        const int64_t N = cox.N;
+        std::vector<double> nev(N + 1, 0.0);
+        for (int64_t k = 0; k < K; ++k) nev[pid0_h[k]] += y_h[k] * wh[k];
+        check_cuda(cudaMemcpyAsync(w, wh.data(), sizeof(double) * K, cudaMemcpyHostToDevice, stream), "w");
+        check_cuda(cudaMemcpyAsync(cox.nEv, nev.data(), sizeof(double) * (N + 1), cudaMemcpyHostToDevice,
+                                   stream), "nev");
+        check_cuda(launch_xjy(m->d_col_ptr, m->d_rows, m->d_val_ptr, m->d_vals, m->d_fmt, y,
+                              weighted ? w : nullptr, K, J, xjy, stream), "xjy");
+        ++launches;
+        ll_fixed = 0.0;
+        if (model == M_CPR) {  // ConditionalPoissonRegression::logLikeFixedTermsContrib (ModelSpecifics.h:722-727)
+            for (int64_t i = 0; i < K; ++i) {
+                double t = 0.0;
+                for (int c = 2; c <= (int)y_h[i]; c++) t -= std::log((double)c);
+                ll_fixed += weighted ? t * wh[i] : t;
+            }
+        }
+        check_cuda(cudaStreamSynchronize(stream), "grouped weights");
+        valid_weights = true;
+        suff_known = false;
+        return;
+    }
     std::vector<int32_t> grp;
     const int64_t N = cox_group_rows(pid0_h, time_h, y_h, weighted ? w_h.data() : nullptr, grp);
     cox.N = N;
@@ -174,6 +212,7 @@ void Fit::cox_apply_weights() {
 }
 
 void Fit::cox_scans() {
+    if (!is_cox()) return;
     ++cox.epoch;
     CoxParams P = cox_params();
     check_cuda(launch_cox_scans(P, cox.tickets, cox.status, cox.tails, cox.epoch, stream), "cox scans");
@@ -189,7 +228,8 @@ void Fit::cox_remaining() {
         xb_pending = false;
     }
     CoxParams P = cox_params();
-    check_cuda(launch_cox_remaining(P, stream), "cox remaining");
+    if (is_cox()) check_cuda(launch_cox_remaining(P, stream), "cox remaining");
+    else check_cuda(launch_grouped_remaining(P, stream), "grouped remaining");
     launches += 2;
     cox_scans();
     suff_known = true;
@@ -198,7 +238,8 @@ void Fit::cox_remaining() {
 void Fit::cox_objective_terms(double* out4) {
     const int nb = ctx->n_sm;
     CoxParams P = cox_params();
-    check_cuda(launch_cox_objective(P, red, nb, stream), "cox objective");
+    if (is_cox()) check_cuda(launch_cox_objective(P, red, nb, stream), "cox objective");
+    else check_cuda(launch_grouped_objective(P, red, nb, stream), "grouped objective");
     ++launches;
     std::vector<double2> parts(2 * nb);
     check_cuda(cudaMemcpyAsync(parts.data(), red, sizeof(double2) * 2 * nb, cudaMemcpyDeviceToHost, stream),
@@ -219,7 +260,8 @@ void Fit::cox_gh_batch(const int32_t* cols, int n, double2* out) {
     check_cuda(cudaMemcpyAsync(cox.batch_cols, cols, sizeof(int32_t) * n, cudaMemcpyHostToDevice, stream),
                "batch cols");
     CoxParams P = cox_params();
-    check_cuda(launch_cox_gh(P, cox.batch_cols, n, cox.batch_out, stream), "cox gh");
+    if (is_cox()) check_cuda(launch_cox_gh(P, cox.batch_cols, n, cox.batch_out, stream), "cox gh");
+    else check_cuda(launch_grouped_gh(P, cox.batch_cols, n, cox.batch_out, stream), "grouped gh");
     ++launches;
     check_cuda(cudaMemcpyAsync(out, cox.batch_out, sizeof(double2) * n, cudaMemcpyDeviceToHost, stream),
                "gh copy");
@@ -228,7 +270,8 @@ void Fit::cox_gh_batch(const int32_t* cols, int n, double2* out) {
 
 void Fit::cox_update(int j, double delta) {
     CoxParams P = cox_params();
-    check_cuda(launch_cox_update(P, j, delta, stream), "cox update");
+    if (is_cox()) check_cuda(launch_cox_update(P, j, delta, stream), "cox update");
+    else check_cuda(launch_grouped_update(P, j, delta, stream), "grouped update");
     ++launches;
     cox_scans();
 }

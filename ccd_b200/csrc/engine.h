@@ -127,6 +127,7 @@ struct Fit {
     std::vector<double> y_h, w_h, beta_h, pvar_h, time_h;
     std::vector<int64_t> stratum_h;
     std::vector<int32_t> pid0_h;
+    std::vector<int64_t> cox_grow_h;
     std::vector<int32_t> ptype_h;
     std::vector<uint8_t> fixed;
     bool weighted = false;
@@ -155,6 +156,9 @@ struct Fit {
     // speculative batched sweeps (models without a fused sweep kernel)
     void find_mode_batched(const ccdb_mode_args& a, double bound, int* flag, int* iters, double* obj);
     bool is_cox() const { return model == M_COX; }
+    bool is_grouped() const { return model == M_CLR || model == M_CPR; }
+    // models served by the group engine (cox.cu) rather than the fused sweep
+    bool group_engine() const { return is_cox() || is_grouped(); }
     // Cox engine (cox_host.cu)
     CoxParams cox_params() const;
     void cox_allocate();

@@ -104,6 +104,7 @@ def lib() -> C.CDLL:
         L.ccdb_find_mode.argtypes = [_P, C.POINTER(_ModeArgs), _P, C.POINTER(_FitResult)]
         L.ccdb_fit_model.argtypes = [_P, C.c_int64, C.c_int32, _P, _P, _P, _P, _P, C.POINTER(_FitDesc),
                                      _P, C.POINTER(_ModeArgs), _P, C.POINTER(_FitResult)]
+        L.ccdb_sweep_levels.argtypes = [C.c_int64, C.c_int32, _P, _P, _P, _P, _P, _P]
         _lib = L
     return _lib
 
@@ -279,3 +280,15 @@ def fit_model(ctx: Context, d: CyclopsData, args: Optional[ModeFindingArguments]
     return FitResult(beta, res.return_flag, res.iterations, res.log_likelihood, res.objective,
                      res.coordinate_updates, res.device_seconds, res.kernel_seconds,
                      res.kernel_launches)
+
+
+def sweep_levels(d: CyclopsData, fixed: Optional[np.ndarray] = None):
+    """Dependency level of every column in a fused sweep (host-only)."""
+    fx = np.zeros(d.J, np.uint8) if fixed is None else np.ascontiguousarray(fixed, np.uint8)
+    if fixed is None and d.offset_col0:
+        fx[0] = 1
+    out = np.zeros(d.J, np.int32)
+    n = C.c_int32()
+    cs, rows, fmt = _c(d.col_start, np.int64), _c(d.rows, np.int32), _c(d.fmt, np.uint8)
+    _check(lib().ccdb_sweep_levels(d.K, d.J, _p(cs), _p(rows), _p(fmt), _p(fx), _p(out), C.byref(n)))
+    return out, n.value

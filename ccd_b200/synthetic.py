@@ -25,7 +25,8 @@ from __future__ import annotations
 
 import numpy as np
 
-from .data import (DENSE, INDICATOR, INTERCEPT, MODEL_CONDITIONAL_LOGISTIC, MODEL_COX,
+from .data import (DENSE, INDICATOR, INTERCEPT, MODEL_CONDITIONAL_LOGISTIC,
+                   MODEL_CONDITIONAL_POISSON, MODEL_COX,
                    MODEL_LOGISTIC, MODEL_POISSON, PRIOR_LAPLACE, PRIOR_NONE, PRIOR_NORMAL,
                    SPARSE, CyclopsData, build_columns, cox_sort_order, csc_from_coo)
 
@@ -261,6 +262,10 @@ def small(model: int, seed: int = 0, K: int = 300, P: int = 12, density: float =
         for s in np.unique(stratum):
             idx = np.nonzero(stratum == s)[0]
             y[idx[rng.integers(0, idx.size)]] = 1.0
+        intercept = False
+    elif model == MODEL_CONDITIONAL_POISSON:
+        stratum = np.sort(rng.integers(0, n_strata, size=K)).astype(np.int64)
+        y = rng.poisson(np.exp(0.3 * xb)).astype(np.float64)
         intercept = False
     elif model == MODEL_COX:
         stratum = np.sort(rng.integers(0, n_strata, size=K)).astype(np.int64)

@@ -144,6 +144,18 @@ int ccdb_fit_model(ccdb_context* ctx, int64_t K, int32_t J, const int64_t* col_s
                    const uint8_t* fmt, const ccdb_fit_desc* desc, const double* weights,
                    const ccdb_mode_args* args, double* beta_out, ccdb_fit_result* result);
 
+/* --- inspection (no reference counterpart) ---------------------------------- */
+
+/* Dependency level of every column in one fused sweep over this matrix
+ * (independent-row models: columns conflict when they share a row).  Columns
+ * on one level touch disjoint rows; running levels in order reproduces the
+ * reference's visiting order j = 0..J-1 (CyclicCoordinateDescent.cpp:1008-1021).
+ * fixed[j] != 0 marks columns the sweep skips (level -1).  Host-only: needs no
+ * GPU. */
+int ccdb_sweep_levels(int64_t K, int32_t J, const int64_t* col_start, const int32_t* rows,
+                      const uint8_t* fmt, const uint8_t* fixed, int32_t* level_out,
+                      int32_t* n_levels);
+
 #ifdef __cplusplus
 }
 #endif

@@ -753,11 +753,16 @@ int orc_grad_hess(void* hp, int j, double* g, double* h) {
     return 0;
 }
 
+/* beta[j] += delta through CyclicCoordinateDescent::setBeta(int, double)
+ * (CyclicCoordinateDescent.cpp:719-733), which re-derives the step as
+ * (beta + delta) - beta before updateXBeta. */
 int orc_update_beta(void* hp, int j, double delta) {
     Orc* o = (Orc*)hp;
     check_lazy(o);
-    o->beta[j] += delta;
-    update_xbeta_ms(o, j, delta);
+    const double target = o->beta[j] + delta;
+    const double applied = target - o->beta[j];
+    o->beta[j] += applied;
+    update_xbeta_ms(o, j, applied);
     return 0;
 }
 
