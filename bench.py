@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--max-sweeps", type=int, default=1000,
                     help="cap on sweeps per findMode (profiling captures of one short launch)")
+    ap.add_argument("--trace", default=None,
+                    help="write a per-level timestamp trace of the last timed findMode's first "
+                         "sweep to this file (summarise with python -m ccd_b200.trace)")
     return ap.parse_args()
 
 
@@ -287,11 +290,14 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     clocks.start()
     dev_t, ker_t, updates, launches, sweeps, lat = 0.0, 0.0, 0, 0, 0, []
-    for _ in range(args.steps):
+    for i in range(args.steps):
         flush.fill_(1)
         torch.cuda.synchronize()
         f.set_beta(cold)
+        if args.trace and i == args.steps - 1:
+            os.environ["CCDB_TRACE_FILE"] = args.trace
         r = f.find_mode(margs)
+        os.environ.pop("CCDB_TRACE_FILE", None)
         dev_t += r.device_seconds
         ker_t += r.kernel_seconds
         updates += r.coordinate_updates

@@ -906,6 +906,15 @@ int ccdb_get_xbeta(ccdb_fit* f, double* out) {
     });
 }
 
+int ccdb_get_gradient_objective(ccdb_fit* f, double* out) {
+    return guard([&] {
+        require(f && out, "NULL argument");
+        double t[4];
+        f->objective_terms(t);
+        *out = t[2];
+    });
+}
+
 int ccdb_get_beta(ccdb_fit* f, double* out) {
     return guard([&] {
         require(f && out, "NULL argument");

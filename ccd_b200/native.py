@@ -101,6 +101,7 @@ def lib() -> C.CDLL:
         L.ccdb_get_log_likelihood.argtypes = [_P, _P]
         L.ccdb_get_xbeta.argtypes = [_P, _P]
         L.ccdb_get_beta.argtypes = [_P, _P]
+        L.ccdb_get_gradient_objective.argtypes = [_P, _P]
         L.ccdb_find_mode.argtypes = [_P, C.POINTER(_ModeArgs), _P, C.POINTER(_FitResult)]
         L.ccdb_fit_model.argtypes = [_P, C.c_int64, C.c_int32, _P, _P, _P, _P, _P, C.POINTER(_FitDesc),
                                      _P, C.POINTER(_ModeArgs), _P, C.POINTER(_FitResult)]
@@ -241,6 +242,11 @@ class Fit:
         out = np.zeros(self.d.K)
         _check(lib().ccdb_get_xbeta(self.h, _p(out)))
         return out
+
+    def get_gradient_objective(self) -> float:
+        v = C.c_double()
+        _check(lib().ccdb_get_gradient_objective(self.h, C.byref(v)))
+        return v.value
 
     def get_beta(self) -> np.ndarray:
         out = np.zeros(self.d.J)

@@ -1,0 +1,71 @@
+"""Summarise a sweep timestamp trace written by the engine.
+
+Setting ``CCDB_TRACE_FILE=<path>`` before a fused findMode makes libccdb write,
+for the first sweep, the schedule (segments, tasks) and per CTA segment the
+global timer at: wait start, level open, end of the CTA-wide phase, end of
+the warp phase, arrival.  ``python -m ccd_b200.trace <path>`` prints where the
+time of a sweep goes: level-to-level detection, per-level span, and the phase
+breakdown by segment kind.
+"""
+from __future__ import annotations
+
+import sys
+
+import numpy as np
+
+SEG = np.dtype([("level", "i4"), ("n_chunk", "i4"), ("n_cta", "i4"), ("n_warp", "i4"), ("t0", "i8")])
+TASK = np.dtype([("col", "i4"), ("kind", "i2"), ("warp", "i2"), ("chunk", "i4"), ("nchunks", "i4"),
+                 ("part_base", "i4"), ("p0", "i4"), ("p1", "i4"), ("pad", "i4")])
+
+
+def load(path: str):
+    raw = open(path, "rb").read()
+    ns, nt = np.frombuffer(raw[:16], np.int64)
+    off = 16
+    segs = np.frombuffer(raw[off:off + SEG.itemsize * ns], SEG)
+    off += SEG.itemsize * ns
+    rest = len(raw) - off - TASK.itemsize * nt - 40 * ns
+    G = rest // 8 - 1
+    cta_seg = np.frombuffer(raw[off:off + 8 * (G + 1)], np.int64)
+    off += 8 * (G + 1)
+    tasks = np.frombuffer(raw[off:off + TASK.itemsize * nt], TASK)
+    off += TASK.itemsize * nt
+    allt = np.frombuffer(raw[off:], np.uint64).astype(np.int64)
+    return segs, cta_seg, tasks, allt[:3 * ns].reshape(-1, 3), allt[3 * ns:5 * ns].reshape(-1, 2)
+
+
+def summarise(path: str) -> str:
+    segs, cta_seg, tasks, tr, tr2 = load(path)
+    ns = len(segs)
+    t0 = tr[tr[:, 0] > 0, 0].min()
+    tr = tr - t0
+    tr2 = np.where(tr2 > 0, tr2 - t0, 0)
+    L = segs["level"]
+    nl = int(L.max()) + 1
+    first = np.full(nl, 1 << 62)
+    last = np.zeros(nl, np.int64)
+    for i in range(ns):
+        first[L[i]] = min(first[L[i]], tr[i, 1])
+        last[L[i]] = max(last[L[i]], tr[i, 2])
+    gap = first[1:] - last[:-1]
+    span = last - first
+    out = [f"segments {ns}, tasks {len(tasks)}, CTAs {len(cta_seg) - 1}, levels {nl}",
+           f"sweep span {last[-1] / 1e3:.1f} us, {last[-1] / 1e3 / nl:.2f} us per level",
+           f"level-to-level detection: median {np.median(gap) / 1e3:.2f} us",
+           f"level span (open -> last arrival): median {np.median(span) / 1e3:.2f} us, "
+           f"p90 {np.percentile(span, 90) / 1e3:.2f} us"]
+    p1 = tr2[:, 0] - tr[:, 1]
+    p2 = np.where(tr2[:, 1] > 0, tr2[:, 1] - tr2[:, 0], 0)
+    p3 = tr[:, 2] - np.maximum(tr2[:, 0], tr2[:, 1])
+    kinds = (("CTA-task segments", (segs["n_cta"] > 0) & (segs["n_warp"] == 0) & (segs["n_chunk"] == 0)),
+             ("warp-only segments", (segs["n_warp"] > 0) & (segs["n_cta"] == 0) & (segs["n_chunk"] == 0)),
+             ("split-column segments", segs["n_chunk"] > 0))
+    for name, sel in kinds:
+        if sel.sum():
+            out.append(f"{name}: {int(sel.sum())}, median phase1 {np.median(p1[sel]) / 1e3:.2f} us, "
+                       f"phase2 {np.median(p2[sel]) / 1e3:.2f} us, tail {np.median(p3[sel]) / 1e3:.2f} us")
+    return "\n".join(out)
+
+
+if __name__ == "__main__":
+    print(summarise(sys.argv[1]))

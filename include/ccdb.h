@@ -102,6 +102,8 @@ int ccdb_get_log_likelihood(ccdb_fit* f, double* loglik);
 /* getXBeta (ModelSpecifics.hpp:286-289): K values. */
 int ccdb_get_xbeta(ccdb_fit* f, double* out);
 int ccdb_get_beta(ccdb_fit* f, double* out);
+/* getGradientObjective (ModelSpecifics.hpp:103-120): sum of y * xBeta (* weight). */
+int ccdb_get_gradient_objective(ccdb_fit* f, double* out);
 
 /* --- mode finding (CyclicCoordinateDescent::update) ------------------------ */
 

@@ -22,6 +22,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libccd_ref.so")
+REF_B200_LIB = os.path.join(HERE, "_ref", "libccd_ref_b200.so")
 PORT_LIB = os.path.join(HERE, "_build", "libccd_oracle.so")
 
 _P = C.c_void_p
@@ -43,6 +44,7 @@ def reference_available() -> bool:
 class _Engine:
     prefix = ""
     libpath = ""
+    create_name = None
     _lib_cache: dict = {}
 
     @classmethod
@@ -55,8 +57,9 @@ class _Engine:
                     raise FileNotFoundError(cls.libpath)
             lib = C.CDLL(cls.libpath)
             p = cls.prefix
-            getattr(lib, p + "create").restype = _P
-            getattr(lib, p + "create").argtypes = [C.c_int, C.c_int, C.c_int64, C.c_int] + [_P] * 8 + [
+            cname = cls.create_name or (p + "create")
+            getattr(lib, cname).restype = _P
+            getattr(lib, cname).argtypes = [C.c_int, C.c_int, C.c_int64, C.c_int] + [_P] * 8 + [
                 C.c_int, _P, _P, C.c_char_p, C.c_int]
             getattr(lib, p + "destroy").argtypes = [_P]
             getattr(lib, p + "fit").argtypes = [_P, C.c_int, C.c_double, C.c_int, C.c_double, C.c_int,
@@ -83,7 +86,7 @@ class _Engine:
 
         lib = self.lib()
         err = C.create_string_buffer(512)
-        self.h = getattr(lib, self.prefix + "create")(
+        self.h = getattr(lib, self.create_name or (self.prefix + "create"))(
             d.model_type, int(fp32), d.K, d.J, _ptr(arr(d.y, np.float64)),
             _ptr(arr(d.time, np.float64)), _ptr(arr(d.stratum, np.int64)),
             _ptr(arr(d.col_start, np.int64)), _ptr(arr(d.rows, np.int32)),
@@ -168,6 +171,14 @@ class _Engine:
 class ReferenceEngine(_Engine):
     prefix = "ref_"
     libpath = REF_LIB
+
+
+class ReferenceOnB200Engine(_Engine):
+    """The reference's own CyclicCoordinateDescent driving the B200 engine
+    through ccd_b200/integration/B200ModelSpecifics.h (the drop-in)."""
+    prefix = "ref_"
+    libpath = REF_B200_LIB
+    create_name = "ref_create_b200"
 
 
 class RestatementEngine(_Engine):

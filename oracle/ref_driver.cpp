@@ -26,6 +26,9 @@
 #include "CyclicCoordinateDescent.h"
 #include "priors/JointPrior.h"
 #include "priors/CovariatePrior.h"
+#ifdef CCDB_B200_ADAPTER
+#include "B200ModelSpecifics.h"
+#endif
 
 using namespace bsccs;
 
@@ -128,10 +131,11 @@ extern "C" {
 // Build ModelData + ModelSpecifics + MixtureJointPrior + CyclicCoordinateDescent.
 // model_type uses the reference's ModelType numbering (Types.h:134-147).
 // prior_type per column: 0 none, 1 Laplace, 2 Normal (priors::PriorType, Types.h:100-105).
-void* ref_create(int model_type, int fp32, int64_t K, int J, const double* y, const double* time,
-                 const int64_t* stratum, const int64_t* col_start, const int32_t* rows,
-                 const int64_t* val_start, const double* vals, const uint8_t* fmt, int offset_col0,
-                 const int32_t* prior_type, const double* prior_var, char* err, int errlen) {
+static void* create_impl(bool on_b200, int model_type, int fp32, int64_t K, int J, const double* y,
+                         const double* time, const int64_t* stratum, const int64_t* col_start,
+                         const int32_t* rows, const int64_t* val_start, const double* vals,
+                         const uint8_t* fmt, int offset_col0, const int32_t* prior_type,
+                         const double* prior_var, char* err, int errlen) {
     try {
         auto h = new RefHandle();
         h->log = std::make_shared<QuietLogger>();
@@ -146,7 +150,16 @@ void* ref_create(int model_type, int fp32, int64_t K, int J, const double* y, co
             h->data.reset(build_data<double>(mt, K, J, y, time, stratum, col_start, rows, val_start,
                                              vals, fmt, offset_col0, h->log, h->err));
         }
-        h->ms.reset(AbstractModelSpecifics::factory(mt, *h->data, DeviceType::CPU, "native"));
+        if (on_b200) {
+#ifdef CCDB_B200_ADAPTER
+            if (fp32) throw std::runtime_error("the B200 adapter is built for ModelData<double>");
+            h->ms.reset(new B200ModelSpecifics(static_cast<const ModelData<double>&>(*h->data), mt));
+#else
+            throw std::runtime_error("built without the B200 adapter");
+#endif
+        } else {
+            h->ms.reset(AbstractModelSpecifics::factory(mt, *h->data, DeviceType::CPU, "native"));
+        }
         if (!h->ms) throw std::runtime_error("factory returned nullptr (unsupported model)");
 
         std::map<std::pair<int, double>, priors::PriorPtr> unique;
@@ -171,6 +184,24 @@ void* ref_create(int model_type, int fp32, int64_t K, int J, const double* y, co
         set_err(err, errlen, e.what());
         return nullptr;
     }
+}
+
+void* ref_create(int model_type, int fp32, int64_t K, int J, const double* y, const double* time,
+                 const int64_t* stratum, const int64_t* col_start, const int32_t* rows,
+                 const int64_t* val_start, const double* vals, const uint8_t* fmt, int offset_col0,
+                 const int32_t* prior_type, const double* prior_var, char* err, int errlen) {
+    return create_impl(false, model_type, fp32, K, J, y, time, stratum, col_start, rows, val_start,
+                       vals, fmt, offset_col0, prior_type, prior_var, err, errlen);
+}
+
+// The reference's own CyclicCoordinateDescent driving B200ModelSpecifics
+// (ccd_b200/integration/B200ModelSpecifics.h) in place of ModelSpecifics.
+void* ref_create_b200(int model_type, int fp32, int64_t K, int J, const double* y, const double* time,
+                      const int64_t* stratum, const int64_t* col_start, const int32_t* rows,
+                      const int64_t* val_start, const double* vals, const uint8_t* fmt, int offset_col0,
+                      const int32_t* prior_type, const double* prior_var, char* err, int errlen) {
+    return create_impl(true, model_type, fp32, K, J, y, time, stratum, col_start, rows, val_start,
+                       vals, fmt, offset_col0, prior_type, prior_var, err, errlen);
 }
 
 void ref_destroy(void* hp) {
