@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/ccdb.h"
+#include "batch.h"
 #include "engine.h"
 
 namespace ccdb {
@@ -129,7 +130,7 @@ void Matrix::ensure_csr(cudaStream_t s) {
 Fit::~Fit() {
     for (void* p : {(void*)row, (void*)y, (void*)beta, (void*)hdelta, (void*)xjy, (void*)ptype,
                     (void*)pvar, (void*)st, (void*)grid_bar, (void*)red, (void*)xb_tmp, (void*)w,
-                    (void*)gh_parts, (void*)gh_out})
+                    (void*)gh_parts, (void*)gh_out, (void*)d_batch_cols, (void*)d_batch_out})
         ctx->release(p);
     release_schedule();
     if (group_engine()) cox_release();
@@ -432,7 +433,7 @@ void Fit::find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* 
                    "bounds");
         return;
     }
-    if (group_engine()) {
+    if (group_engine() || use_speculative(a)) {
         auto t0 = std::chrono::steady_clock::now();
         find_mode_batched(a, bound, flag, iters, obj);
         *ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -526,7 +527,7 @@ void Fit::find_mode_batched(const ccdb_mode_args& a, double bound, int* flag, in
         int pos = 0, batch = 32;
         while (pos < n_active) {
             const int nb = std::min(batch, n_active - pos);
-            cox_gh_batch(cols.data() + pos, nb, gh.data());
+            gh_batch(cols.data() + pos, nb, gh.data());
             int advanced = nb;
             for (int i = 0; i < nb; ++i) {
                 const int j = cols[pos + i];
@@ -534,7 +535,7 @@ void Fit::find_mode_batched(const ccdb_mode_args& a, double bound, int* flag, in
                 delta = apply_bounds(delta, hd[j]);
                 if (delta != 0.0) {
                     beta_h[j] += delta;
-                    cox_update(j, delta);
+                    apply_step(j, delta);
                     advanced = i + 1;
                     break;
                 }
@@ -567,6 +568,50 @@ void Fit::find_mode_batched(const ccdb_mode_args& a, double bound, int* flag, in
     check_cuda(cudaStreamSynchronize(stream), "batched sync");
     *iters = iteration;
     *obj = last;
+}
+
+void Fit::gh_batch(const int32_t* cols, int n, double2* out) {
+    if (group_engine()) {
+        cox_gh_batch(cols, n, out);
+        return;
+    }
+    if (!d_batch_cols) {
+        d_batch_cols = static_cast<int32_t*>(ctx->alloc(sizeof(int32_t) * kBatchMax));
+        d_batch_out = static_cast<double2*>(ctx->alloc(sizeof(double2) * kBatchMax));
+    }
+    check_cuda(cudaMemcpyAsync(d_batch_cols, cols, sizeof(int32_t) * n, cudaMemcpyHostToDevice, stream),
+               "batch cols");
+    IndepParams P = params();
+    check_cuda(launch_indep_gh_batch(P, d_batch_cols, n, d_batch_out, stream), "gh batch");
+    ++launches;
+    check_cuda(cudaMemcpyAsync(out, d_batch_out, sizeof(double2) * n, cudaMemcpyDeviceToHost, stream),
+               "gh copy");
+    check_cuda(cudaStreamSynchronize(stream), "gh sync");
+}
+
+void Fit::apply_step(int j, double delta) {
+    if (group_engine()) {
+        cox_update(j, delta);
+        return;
+    }
+    IndepParams P = params();
+    check_cuda(launch_indep_update(P, j, m->fmt[j], m->entries(j), delta, stream), "update");
+    launches += m->entries(j) > 0 ? 1 : 0;
+}
+
+// Levels suit dense steps (every coordinate moves); speculative batches suit
+// L1 fits, where most steps are zero and a batch of gradients advances many
+// coordinates per launch.
+bool Fit::use_speculative(const ccdb_mode_args& a) const {
+    if (a.strategy == CCDB_SWEEP_LEVELS) return false;
+    if (a.strategy == CCDB_SWEEP_SPECULATIVE) return true;
+    int active = 0, laplace = 0;
+    for (int j = 0; j < J; ++j) {
+        if (fixed[j]) continue;
+        ++active;
+        laplace += (ptype_h[j] == 1) ? 1 : 0;
+    }
+    return active > 0 && 2 * laplace >= active;
 }
 
 void Fit::find_mode(const ccdb_mode_args& a, double* beta_inout, ccdb_fit_result* res) {
@@ -961,6 +1006,105 @@ int ccdb_fit_model(ccdb_context* ctx, int64_t K, int32_t J, const int64_t* col_s
     if (m) ccdb_matrix_destroy(m);
     g_last_error = err;
     return rc;
+}
+
+int ccdb_batch_find_mode(ccdb_fit* f, const ccdb_batch_desc* b, const ccdb_mode_args* a, double* beta_out,
+                         ccdb_batch_result* results, double* device_seconds) {
+    return guard([&] {
+        require(f && b && a && a->prior_type && b->variance && b->n_instances > 0, "NULL argument");
+        if (f->model != M_LOGISTIC && f->model != M_POISSON)
+            throw Error(CCDB_ERR_UNSUPPORTED, "batched fits support logistic and Poisson models");
+        if (a->convergence_type < C_GRADIENT || a->convergence_type > C_MITTAL)
+            throw Error(CCDB_ERR_UNSUPPORTED, "convergence type");
+        Context* ctx = f->ctx;
+        check_cuda(cudaSetDevice(ctx->device), "cudaSetDevice");
+        const int n = b->n_instances;
+        const int64_t K = f->K;
+        const int J = f->J;
+        const Matrix* m = f->m;
+        cudaStream_t s = f->stream;
+        std::vector<void*> owned;
+        auto keep = [&](void* p) { owned.push_back(p); return p; };
+        struct Release {
+            Context* c;
+            std::vector<void*>* v;
+            ~Release() { for (void* p : *v) c->release(p); }
+        } rel{ctx, &owned};
+        BatchParams P{};
+        P.col_ptr = m->d_col_ptr;
+        P.rows = m->d_rows;
+        P.val_ptr = m->d_val_ptr;
+        P.vals = m->d_vals;
+        P.fmt = m->d_fmt;
+        P.K = K;
+        P.J = J;
+        P.model = f->model;
+        P.n_inst = n;
+        P.conv = a->convergence_type;
+        P.max_iter = a->max_iterations;
+        P.tol = a->tolerance;
+        P.initial_bound = a->initial_bound;
+        P.y = f->y;
+        if (b->row_fold) P.row_fold = (const int32_t*)keep(upload(ctx, b->row_fold, (size_t)K, s));
+        std::vector<int32_t> hold(n, -1);
+        if (b->holdout) hold.assign(b->holdout, b->holdout + n);
+        P.holdout = (const int32_t*)keep(upload(ctx, hold.data(), (size_t)n, s));
+        P.variance = (const double*)keep(upload(ctx, b->variance, (size_t)n, s));
+        P.ptype = (const int32_t*)keep(upload(ctx, a->prior_type, (size_t)J, s));
+        if (f->offset_col0) {
+            if (m->fmt[0] != F_DENSE) throw Error(CCDB_ERR_UNSUPPORTED, "offset column must be DENSE");
+            P.offset_vals = m->d_vals + m->val_start[0];
+        }
+        if (f->model == M_POISSON) {  // fixed terms per instance (ModelSpecifics.h:1596-1601)
+            std::vector<double> table(1, 0.0), fixed(n, 0.0);
+            for (int i = 0; i < n; ++i) {
+                double acc = 0.0;
+                for (int64_t k = 0; k < K; ++k) {
+                    const int yi = (int)f->y_h[k];
+                    while ((int)table.size() <= yi) {
+                        const int c = (int)table.size();
+                        table.push_back(c >= 2 ? table.back() + -std::log((double)c) : 0.0);
+                    }
+                    const double t = yi >= 2 ? table[yi] : 0.0;
+                    const double w = (b->row_fold && b->row_fold[k] == hold[i]) ? 0.0 : 1.0;
+                    acc += t * w;
+                }
+                fixed[i] = acc;
+            }
+            P.ll_fixed = (const double*)keep(upload(ctx, fixed.data(), (size_t)n, s));
+        }
+        P.row = (double2*)keep(ctx->alloc(sizeof(double2) * 2 * (size_t)K * n));
+        P.beta = (double*)keep(ctx->alloc(sizeof(double) * (size_t)J * n));
+        P.hdelta = (double*)keep(ctx->alloc(sizeof(double) * (size_t)J * n));
+        P.xjy = (double*)keep(ctx->alloc(sizeof(double) * (size_t)J * n));
+        P.results = (BatchResult*)keep(ctx->alloc(sizeof(BatchResult) * n));
+        cudaEvent_t e0, e1;
+        check_cuda(cudaEventCreate(&e0), "event");
+        check_cuda(cudaEventCreate(&e1), "event");
+        check_cuda(cudaEventRecord(e0, s), "event");
+        check_cuda(launch_batch_sweep(P, s), "batch sweep");
+        check_cuda(cudaEventRecord(e1, s), "event");
+        std::vector<BatchResult> res(n);
+        check_cuda(cudaMemcpyAsync(res.data(), P.results, sizeof(BatchResult) * n, cudaMemcpyDeviceToHost, s),
+                   "results");
+        if (beta_out)
+            check_cuda(cudaMemcpyAsync(beta_out, P.beta, sizeof(double) * (size_t)J * n, cudaMemcpyDeviceToHost, s),
+                       "beta");
+        check_cuda(cudaStreamSynchronize(s), "batch sync");
+        float ms = 0.f;
+        check_cuda(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (device_seconds) *device_seconds = ms * 1e-3;
+        if (results)
+            for (int i = 0; i < n; ++i) {
+                results[i].return_flag = res[i].flag;
+                results[i].iterations = res[i].iterations;
+                results[i].log_likelihood = res[i].loglik;
+                results[i].objective = res[i].objective;
+                results[i].predictive_loglik = res[i].pred_loglik;
+            }
+    });
 }
 
 int ccdb_sweep_levels(int64_t K, int32_t J, const int64_t* col_start, const int32_t* rows,

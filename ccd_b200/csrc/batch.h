@@ -1,0 +1,50 @@
+// batch.h -- parameters of the instance-batched sweep (batch.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "types.h"
+
+namespace ccdb {
+
+struct BatchResult {
+    int32_t flag;
+    int32_t iterations;
+    double loglik;
+    double objective;
+    double pred_loglik;  // held-out rows' predictive log-likelihood
+};
+
+struct BatchParams {
+    const int64_t* col_ptr;
+    const int32_t* rows;
+    const int64_t* val_ptr;
+    const double* vals;
+    const uint8_t* fmt;
+    int64_t K;
+    int32_t J;
+    int32_t model;
+    int32_t n_inst;
+    int32_t conv;
+    int32_t max_iter;
+    int32_t pad0;
+    double tol;
+    double initial_bound;
+    const double* y;
+    const int32_t* row_fold;   // K or NULL
+    const int32_t* holdout;    // n_inst or NULL
+    const double* variance;    // n_inst
+    const int32_t* ptype;      // J
+    const double* offset_vals; // K values of an offset column 0, or NULL
+    const double* ll_fixed;    // n_inst (Poisson) or NULL
+    double2* row;              // n_inst x 2K
+    double* beta;              // n_inst x J
+    double* hdelta;            // n_inst x J
+    double* xjy;               // n_inst x J
+    BatchResult* results;      // n_inst
+};
+
+cudaError_t launch_batch_sweep(const BatchParams& P, cudaStream_t stream);
+
+}  // namespace ccdb

@@ -155,6 +155,12 @@ struct Fit {
     void find_mode(const ccdb_mode_args& a, double* beta_inout, ccdb_fit_result* res);
     // speculative batched sweeps (models without a fused sweep kernel)
     void find_mode_batched(const ccdb_mode_args& a, double bound, int* flag, int* iters, double* obj);
+    // (g, h) of several columns against the current state; nonzero step of one column
+    void gh_batch(const int32_t* cols, int n, double2* out);
+    void apply_step(int j, double delta);
+    bool use_speculative(const ccdb_mode_args& a) const;
+    int32_t* d_batch_cols = nullptr;  // independent-row models
+    double2* d_batch_out = nullptr;
     bool is_cox() const { return model == M_COX; }
     bool is_grouped() const { return model == M_CLR || model == M_CPR; }
     // models served by the group engine (cox.cu) rather than the fused sweep

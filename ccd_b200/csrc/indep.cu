@@ -607,6 +607,23 @@ __global__ void __launch_bounds__(256) gh_column_kernel(IndepParams P, int j, in
     if (threadIdx.x == 0) out[blockIdx.x] = s;
 }
 
+// (g, h) of a list of columns, one CTA per column (speculative batches).
+template <int MODEL>
+__global__ void __launch_bounds__(512) gh_batch_kernel(IndepParams P, const int32_t* cols, int ncols,
+                                                       double2* out) {
+    __shared__ double2 s_red2[kWarps];
+    for (int c = blockIdx.x; c < ncols; c += gridDim.x) {
+        const int j = cols[c];
+        const uint8_t f = P.fmt[j];
+        const int64_t entries = (f == F_DENSE || f == F_INTERCEPT) ? P.K : P.col_ptr[j + 1] - P.col_ptr[j];
+        double g = 0.0, h = 0.0;
+        gh_dispatch<MODEL>(P, j, f, 0, entries, threadIdx.x, blockDim.x, g, h);
+        const double2 s = block_sum2<kWarps>(make_double2(g, h), s_red2);
+        if (threadIdx.x == 0)
+            out[c] = (entries > 0) ? make_double2(s.x - P.xjy[j], s.y) : make_double2(0.0, 0.0);
+    }
+}
+
 __global__ void gh_finish_kernel(const double2* parts, int n, const double* xjy, int j,
                                  int64_t entries, double2* out) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
@@ -744,6 +761,14 @@ cudaError_t launch_indep_gh(const IndepParams& P, int j, int64_t entries, double
     else
         gh_column_kernel<M_POISSON><<<nb, 256, 0, stream>>>(P, j, entries, per_block, parts);
     gh_finish_kernel<<<1, 32, 0, stream>>>(parts, nb, P.xjy, j, entries, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_indep_gh_batch(const IndepParams& P, const int32_t* cols, int ncols, double2* out,
+                                  cudaStream_t stream) {
+    if (ncols <= 0) return cudaSuccess;
+    if (P.model == M_LOGISTIC) gh_batch_kernel<M_LOGISTIC><<<ncols, 512, 0, stream>>>(P, cols, ncols, out);
+    else gh_batch_kernel<M_POISSON><<<ncols, 512, 0, stream>>>(P, cols, ncols, out);
     return cudaGetLastError();
 }
 

@@ -59,6 +59,8 @@ cudaError_t indep_sweep_occupancy(int model, int* blocks_per_sm);
 cudaError_t launch_indep_sweep(const IndepParams& P, int n_cta, cudaStream_t stream);
 cudaError_t launch_indep_gh(const IndepParams& P, int j, int64_t entries, double2* parts,
                             int max_parts, double2* out, cudaStream_t stream);
+cudaError_t launch_indep_gh_batch(const IndepParams& P, const int32_t* cols, int ncols, double2* out,
+                                  cudaStream_t stream);
 cudaError_t launch_indep_update(const IndepParams& P, int j, uint8_t fmt, int64_t entries,
                                 double delta, cudaStream_t stream);
 cudaError_t launch_remaining_stats(double2* row, const double* xb, const double* w, int64_t K,

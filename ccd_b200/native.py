@@ -23,6 +23,7 @@ LIB_PATH = os.path.join(HERE, "libccdb.so")
 OK = 0
 ERR_INVALID, ERR_CUDA, ERR_UNSUPPORTED, ERR_BUDGET, ERR_TIMEOUT = -1, -2, -3, -4, -5
 PRECISION_FP64, PRECISION_MIXED = 0, 1
+SWEEP_AUTO, SWEEP_LEVELS, SWEEP_SPECULATIVE = 0, 1, 2
 
 
 class CcdbError(RuntimeError):
@@ -40,7 +41,19 @@ class _ModeArgs(C.Structure):
     _fields_ = [("prior_type", C.c_void_p), ("prior_var", C.c_void_p),
                 ("convergence_type", C.c_int32), ("tolerance", C.c_double),
                 ("max_iterations", C.c_int32), ("initial_bound", C.c_double),
-                ("max_bound_count", C.c_int32), ("per_coordinate", C.c_int32)]
+                ("max_bound_count", C.c_int32), ("per_coordinate", C.c_int32),
+                ("strategy", C.c_int32)]
+
+
+class _BatchDesc(C.Structure):
+    _fields_ = [("n_instances", C.c_int32), ("row_fold", C.c_void_p), ("holdout", C.c_void_p),
+                ("variance", C.c_void_p)]
+
+
+class _BatchResult(C.Structure):
+    _fields_ = [("return_flag", C.c_int32), ("iterations", C.c_int32),
+                ("log_likelihood", C.c_double), ("objective", C.c_double),
+                ("predictive_loglik", C.c_double)]
 
 
 class _FitResult(C.Structure):
@@ -59,6 +72,7 @@ class ModeFindingArguments:
     initial_bound: float = 2.0
     max_bound_count: int = 5
     per_coordinate: bool = False
+    strategy: int = 0  # SWEEP_AUTO / SWEEP_LEVELS / SWEEP_SPECULATIVE
 
 
 @dataclass
@@ -105,6 +119,7 @@ def lib() -> C.CDLL:
         L.ccdb_find_mode.argtypes = [_P, C.POINTER(_ModeArgs), _P, C.POINTER(_FitResult)]
         L.ccdb_fit_model.argtypes = [_P, C.c_int64, C.c_int32, _P, _P, _P, _P, _P, C.POINTER(_FitDesc),
                                      _P, C.POINTER(_ModeArgs), _P, C.POINTER(_FitResult)]
+        L.ccdb_batch_find_mode.argtypes = [_P, C.POINTER(_BatchDesc), C.POINTER(_ModeArgs), _P, _P, _P]
         L.ccdb_sweep_levels.argtypes = [C.c_int64, C.c_int32, _P, _P, _P, _P, _P, _P]
         _lib = L
     return _lib
@@ -186,7 +201,7 @@ def _mode_args(d: CyclopsData, a: ModeFindingArguments, keep: list) -> _ModeArgs
     pv = _c(d.prior_var, np.float64)
     keep += [pt, pv]
     return _ModeArgs(_p(pt), _p(pv), a.convergence_type, a.tolerance, a.max_iterations,
-                     a.initial_bound, a.max_bound_count, int(a.per_coordinate))
+                     a.initial_bound, a.max_bound_count, int(a.per_coordinate), int(a.strategy))
 
 
 class Fit:
@@ -252,6 +267,28 @@ class Fit:
         out = np.zeros(self.d.J)
         _check(lib().ccdb_get_beta(self.h, _p(out)))
         return out
+
+    # --- the cross-validation grid: many instances in one launch
+    def batch_find_mode(self, variance, holdout=None, row_fold=None,
+                        args: Optional[ModeFindingArguments] = None):
+        """Fit len(variance) instances (fold held out, prior variance) together.
+        Returns (beta[n, J], list of per-instance dicts, device seconds)."""
+        args = args or ModeFindingArguments()
+        keep = []
+        ma = _mode_args(self.d, args, keep)
+        var = _c(variance, np.float64)
+        n = var.shape[0]
+        hold = None if holdout is None else _c(holdout, np.int32)
+        fold = None if row_fold is None else _c(row_fold, np.int32)
+        bd = _BatchDesc(n, _p(fold), _p(hold), _p(var))
+        beta = np.zeros((n, self.d.J))
+        res = (_BatchResult * n)()
+        secs = C.c_double()
+        _check(lib().ccdb_batch_find_mode(self.h, C.byref(bd), C.byref(ma), _p(beta),
+                                          C.cast(res, C.c_void_p), C.byref(secs)))
+        out = [{"flag": r.return_flag, "iterations": r.iterations, "loglik": r.log_likelihood,
+                "objective": r.objective, "pred_loglik": r.predictive_loglik} for r in res]
+        return beta, out, secs.value
 
     # --- CyclicCoordinateDescent::update
     def find_mode(self, args: Optional[ModeFindingArguments] = None,

@@ -310,3 +310,33 @@ def small(model: int, seed: int = 0, K: int = 300, P: int = 12, density: float =
                     meta={"workload": "small", "seed": seed})
     d.validate()
     return d
+
+
+def cv_folds(K: int, n_folds: int = 10, seed: int = 7) -> np.ndarray:
+    """Row -> fold: a seeded permutation cut into contiguous intervals whose sizes
+    follow CrossValidationSelector (drivers/CrossValidationSelector.cpp:31-45):
+    K // n_folds rows each, one extra for the first K % n_folds folds."""
+    rng = _rng(seed)
+    perm = rng.permutation(K)
+    sizes = np.full(n_folds, K // n_folds)
+    sizes[:K % n_folds] += 1
+    fold = np.empty(K, np.int32)
+    start = 0
+    for f, n in enumerate(sizes):
+        fold[perm[start:start + n]] = f
+        start += n
+    return fold
+
+
+def cv_grid(n_folds: int = 10, n_vars: int = 20, lower: float = 1e-4, upper: float = 1.0):
+    """(holdout fold, variance) of every instance of a fold x variance grid.  Variances
+    are log-uniform between lower and upper as GridSearchCrossValidationDriver::
+    computeGridPoint places them (drivers/GridSearchCrossValidationDriver.cpp:38-50)."""
+    if n_vars == 1:
+        grid = np.array([upper])
+    else:
+        step = (np.log(upper) - np.log(lower)) / (n_vars - 1)
+        grid = np.exp(np.log(lower) + step * np.arange(n_vars))
+    hold = np.repeat(np.arange(n_folds, dtype=np.int32), n_vars)
+    var = np.tile(grid, n_folds)
+    return hold, var

@@ -115,9 +115,18 @@ typedef struct {
     int32_t max_iterations;    /* default 1000 */
     double initial_bound;      /* default 2.0 */
     int32_t max_bound_count;   /* default 5 */
-    int32_t per_coordinate;    /* 0: fused persistent sweep (default); 1: host loop over
+    int32_t per_coordinate;    /* 0: on-device mode finding (default); 1: host loop over
                                   the per-coordinate calls above (the reference's call pattern) */
+    int32_t strategy;          /* on-device sweep strategy for logistic/Poisson:
+                                  CCDB_SWEEP_AUTO, _LEVELS (fused persistent kernel over
+                                  dependency levels) or _SPECULATIVE (batched gradients,
+                                  restart after each nonzero step); other models always
+                                  use speculative batches */
 } ccdb_mode_args;
+
+#define CCDB_SWEEP_AUTO 0
+#define CCDB_SWEEP_LEVELS 1
+#define CCDB_SWEEP_SPECULATIVE 2
 
 typedef struct {
     int32_t return_flag;        /* UpdateReturnFlags */
@@ -145,6 +154,33 @@ int ccdb_fit_model(ccdb_context* ctx, int64_t K, int32_t J, const int64_t* col_s
                    const int32_t* rows, const int64_t* val_start, const double* vals,
                    const uint8_t* fmt, const ccdb_fit_desc* desc, const double* weights,
                    const ccdb_mode_args* args, double* beta_out, ccdb_fit_result* result);
+
+/* --- batched fits: the cross-validation grid ------------------------------- */
+
+typedef struct {
+    int32_t n_instances;
+    const int32_t* row_fold; /* K fold id per row, or NULL (no row held out) */
+    const int32_t* holdout;  /* n_instances: fold held out by each instance (-1: none) */
+    const double* variance;  /* n_instances: prior variance of the regularised columns */
+} ccdb_batch_desc;
+
+typedef struct {
+    int32_t return_flag;
+    int32_t iterations;
+    double log_likelihood;     /* on the instance's training rows */
+    double objective;
+    double predictive_loglik;  /* on its held-out rows (getPredictiveLogLikelihood,
+                                  ModelSpecifics.hpp:652-690) */
+} ccdb_batch_result;
+
+/* Fit n_instances models over the fit's matrix and outcomes in one launch:
+ * instance i weights rows 0 on fold holdout[i] and 1 elsewhere (the weights
+ * CrossValidationSelector::getWeights gives, drivers/CrossValidationSelector.cpp:72-130),
+ * uses args->prior_type per column with variance[i], and starts from beta = 0.
+ * Each instance runs the sequential sweep of a standalone fit; instances do not
+ * interact.  Logistic and Poisson models.  beta_out: n_instances x J. */
+int ccdb_batch_find_mode(ccdb_fit* f, const ccdb_batch_desc* batch, const ccdb_mode_args* args,
+                         double* beta_out, ccdb_batch_result* results, double* device_seconds);
 
 /* --- inspection (no reference counterpart) ---------------------------------- */
 

@@ -52,25 +52,28 @@ def test_per_coordinate_gradient_hessian(gpu_ctx, oracle_engine, model, kw):
 
 @pytest.mark.parametrize("model,kw", CASES)
 @pytest.mark.parametrize("conv", [GRADIENT, MITTAL, LANGE])
-@pytest.mark.parametrize("per_coordinate", [False, True])
-def test_find_mode_matches_oracle(gpu_ctx, oracle_engine, model, kw, conv, per_coordinate):
+@pytest.mark.parametrize("mode", ["levels", "speculative", "per_coordinate"])
+def test_find_mode_matches_oracle(gpu_ctx, oracle_engine, model, kw, conv, mode):
     d = synthetic.small(model, **kw)
     want = oracle_engine(d).fit(conv, 1e-6)
     m = native.Matrix(gpu_ctx, d)
     f = native.Fit(gpu_ctx, m, d)
-    got = f.find_mode(native.ModeFindingArguments(convergence_type=conv,
-                                                  per_coordinate=per_coordinate))
+    strategy = {"levels": native.SWEEP_LEVELS, "speculative": native.SWEEP_SPECULATIVE}.get(mode, 0)
+    got = f.find_mode(native.ModeFindingArguments(convergence_type=conv, strategy=strategy,
+                                                  per_coordinate=(mode == "per_coordinate")))
     assert got.return_flag == want["flag"]
     assert got.iterations == want["iterations"]
     assert rel_beta(got.beta, want["beta"]) <= BETA_TOL
     assert abs(got.log_likelihood - want["loglik"]) <= LL_TOL * abs(want["loglik"])
 
 
-def test_logistic_l1_benchmark_problem(gpu_ctx, oracle_engine):
+@pytest.mark.parametrize("strategy", [1, 2])
+def test_logistic_l1_benchmark_problem(gpu_ctx, oracle_engine, strategy):
     """10,000 x 1,000 L1 logistic, MITTAL 1e-6, the reference's CPU-runnable case."""
     d = synthetic.logistic_l1(seed=1)
     want = oracle_engine(d).fit(MITTAL, 1e-6)
-    got = native.fit_model(gpu_ctx, d, native.ModeFindingArguments(convergence_type=MITTAL))
+    got = native.fit_model(gpu_ctx, d, native.ModeFindingArguments(convergence_type=MITTAL,
+                                                                   strategy=strategy))
     assert got.return_flag == want["flag"]
     assert got.iterations == want["iterations"]
     assert rel_beta(got.beta, want["beta"]) <= BETA_TOL
