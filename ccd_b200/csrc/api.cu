@@ -1078,6 +1078,12 @@ int ccdb_batch_find_mode(ccdb_fit* f, const ccdb_batch_desc* b, const ccdb_mode_
         P.hdelta = (double*)keep(ctx->alloc(sizeof(double) * (size_t)J * n));
         P.xjy = (double*)keep(ctx->alloc(sizeof(double) * (size_t)J * n));
         P.results = (BatchResult*)keep(ctx->alloc(sizeof(BatchResult) * n));
+        // weakest priors first: they need the most sweeps, so they start in the first wave
+        std::vector<int32_t> order(n);
+        for (int i = 0; i < n; ++i) order[i] = i;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int32_t x, int32_t y) { return b->variance[x] > b->variance[y]; });
+        P.order = (const int32_t*)keep(upload(ctx, order.data(), (size_t)n, s));
         cudaEvent_t e0, e1;
         check_cuda(cudaEventCreate(&e0), "event");
         check_cuda(cudaEventCreate(&e1), "event");
@@ -1103,6 +1109,10 @@ int ccdb_batch_find_mode(ccdb_fit* f, const ccdb_batch_desc* b, const ccdb_mode_
                 results[i].log_likelihood = res[i].loglik;
                 results[i].objective = res[i].objective;
                 results[i].predictive_loglik = res[i].pred_loglik;
+                results[i].steps = res[i].steps;
+                results[i].updates = res[i].updates;
+                results[i].update_entries = res[i].update_entries;
+                results[i].gradient_entries = res[i].sweep_entries;
             }
     });
 }

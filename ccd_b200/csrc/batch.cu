@@ -23,7 +23,7 @@ namespace ccdb {
 
 namespace {
 
-constexpr int kBT = 256;
+constexpr int kBT = 512;
 constexpr int kBW = kBT / 32;
 
 template <int FMT>
@@ -99,14 +99,41 @@ __device__ __forceinline__ double b_xjy(const BatchParams& P, const double2* row
     return s;
 }
 
+// One column of the sweep with its entries staged in shared memory (row ids,
+// values) and the gathered row state kept in registers between the gradient
+// and the update.  Columns longer than kBT * kBE entries take the loop path.
+constexpr int kBE = 6;  // staged entries per thread: columns up to 3,072 entries
+
+struct ColStage {
+    int32_t k[kBT * kBE];
+    double x[kBT * kBE];
+};
+
+__device__ __forceinline__ void stage_column(const BatchParams& P, const double2* row, int j,
+                                             ColStage& st, int64_t n) {
+    const uint8_t f = P.fmt[j];
+    const int64_t cb = P.col_ptr[j], vb = P.val_ptr[j];
+    const bool has_rows = (f == F_SPARSE || f == F_INDICATOR);
+    const bool has_vals = (f == F_SPARSE || f == F_DENSE);
+    for (int p = threadIdx.x; p < n; p += kBT) {
+        const int32_t k = has_rows ? __ldg(P.rows + cb + p) : p;
+        st.k[p] = k;
+        st.x[p] = has_vals ? __ldg(P.vals + vb + p) : 1.0;
+        // L2 is the point of coherence: the lines are current when read later
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(row + 2 * (int64_t)k));
+    }
+}
+
 template <int MODEL>
-__global__ void __launch_bounds__(kBT, 2) batch_sweep_kernel(BatchParams P) {
+__global__ void __launch_bounds__(kBT, 1) batch_sweep_kernel(BatchParams P) {
     __shared__ double2 s_red2[kBW];
     __shared__ double4 s_red4[kBW];
     __shared__ double s_delta;
     __shared__ int32_t s_done;
-    const int inst = blockIdx.x;
-    if (inst >= P.n_inst) return;
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    ColStage* s_stage = reinterpret_cast<ColStage*>(s_dyn);  // two stages (double buffer)
+    const int inst = P.order ? P.order[blockIdx.x] : blockIdx.x;
+    if (blockIdx.x >= P.n_inst) return;
     double2* row = P.row + (size_t)inst * 2 * P.K;
     double* beta = P.beta + (size_t)inst * P.J;
     double* hd = P.hdelta + (size_t)inst * P.J;
@@ -168,46 +195,128 @@ __global__ void __launch_bounds__(kBT, 2) batch_sweep_kernel(BatchParams P) {
         return ll_out + t.w;
     };
 
+    auto col_len = [&](int j) -> int64_t {
+        const uint8_t f = P.fmt[j];
+        return (f == F_DENSE || f == F_INTERCEPT) ? P.K : P.col_ptr[j + 1] - P.col_ptr[j];
+    };
+    const int j0 = P.offset_vals ? 1 : 0;
+    constexpr int64_t kStageMax = kBT * kBE;
+
     double ll = 0.0, lp = 0.0;
     double last = objective(ll, lp);
     int iteration = 0, flag = R_FAIL;
+    long long steps = 0, updates = 0, upd_entries = 0, gh_entries = 0;
     for (int it = 0; it < P.max_iter; ++it) {
-        for (int j = (P.offset_vals ? 1 : 0); j < P.J; ++j) {
+        int buf = 0;
+        if (j0 < P.J && col_len(j0) <= kStageMax) stage_column(P, row, j0, s_stage[0], col_len(j0));
+        __syncthreads();
+        for (int j = j0; j < P.J; ++j) {
             const uint8_t f = P.fmt[j];
-            const int64_t n = (f == F_DENSE || f == F_INTERCEPT) ? P.K : P.col_ptr[j + 1] - P.col_ptr[j];
+            const int64_t n = col_len(j);
+            const bool staged = n <= kStageMax;
+            // metadata of this column (thread 0) and staging of the next one
+            double m_beta = 0.0, m_hd = 0.0, m_xjy = 0.0;
+            if (threadIdx.x == 0) {
+                m_beta = beta[j];
+                m_hd = hd[j];
+                m_xjy = xjy[j];
+            }
+            if (j + 1 < P.J && col_len(j + 1) <= kStageMax)
+                stage_column(P, row, j + 1, s_stage[buf ^ 1], col_len(j + 1));
             double g = 0.0, h = 0.0;
-            switch (f) {
-            case F_INDICATOR: b_gh<MODEL, F_INDICATOR>(P, row, j, n, g, h); break;
-            case F_SPARSE: b_gh<MODEL, F_SPARSE>(P, row, j, n, g, h); break;
-            case F_DENSE: b_gh<MODEL, F_DENSE>(P, row, j, n, g, h); break;
-            default: b_gh<MODEL, F_INTERCEPT>(P, row, j, n, g, h); break;
+            double2 A[kBE];
+            double Dn[kBE];
+            const ColStage& st = s_stage[buf];
+            const bool ind = (f == F_INDICATOR || f == F_INTERCEPT);
+            if (staged) {
+                double Wt[kBE];
+#pragma unroll
+                for (int i = 0; i < kBE; ++i) {
+                    const int p = threadIdx.x + i * kBT;
+                    if (p < n) {
+                        const int64_t k = st.k[p];
+                        A[i] = row[2 * k];
+                        const double2 b = row[2 * k + 1];
+                        Dn[i] = b.x;
+                        Wt[i] = b.y;
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < kBE; ++i) {
+                    const int p = threadIdx.x + i * kBT;
+                    if (p >= n) continue;
+                    const double x = st.x[p];
+                    const double n1 = A[i].y * x;
+                    if (MODEL == M_LOGISTIC) {
+                        const double gg = n1 / Dn[i];
+                        g += Wt[i] * gg;
+                        if (ind) h += Wt[i] * gg * (1.0 - gg);
+                        else h += Wt[i] * ((n1 * x) / Dn[i] - gg * gg);
+                    } else {
+                        if (ind) {
+                            const double v = Wt[i] * n1;
+                            g += v;
+                            h += v;
+                        } else {
+                            g += Wt[i] * n1;
+                            h += Wt[i] * (n1 * x);
+                        }
+                    }
+                }
+            } else {
+                switch (f) {
+                case F_INDICATOR: b_gh<MODEL, F_INDICATOR>(P, row, j, n, g, h); break;
+                case F_SPARSE: b_gh<MODEL, F_SPARSE>(P, row, j, n, g, h); break;
+                case F_DENSE: b_gh<MODEL, F_DENSE>(P, row, j, n, g, h); break;
+                default: b_gh<MODEL, F_INTERCEPT>(P, row, j, n, g, h); break;
+                }
             }
             const double2 s = block_sum2<kBW>(make_double2(g, h), s_red2);
             if (threadIdx.x == 0) {
                 double G = 0.0, H = 0.0;
                 if (n > 0) {
-                    G = s.x - xjy[j];
+                    G = s.x - m_xjy;
                     H = s.y;
                 }
                 const int pt = P.ptype[j];
-                double d = newton_prior_delta(G, H, beta[j], pt, pt == 0 ? 1.0 : var);
-                double b = hd[j];
+                double d = newton_prior_delta(G, H, m_beta, pt, pt == 0 ? 1.0 : var);
+                double b = m_hd;
                 d = apply_bounds(d, b);
                 hd[j] = b;
-                if (d != 0.0) beta[j] = beta[j] + d;
+                if (d != 0.0) {
+                    beta[j] = m_beta + d;
+                    ++updates;
+                    upd_entries += n;
+                }
+                ++steps;
+                gh_entries += n;
                 s_delta = d;
             }
             __syncthreads();
             const double d = s_delta;
             if (d != 0.0) {
-                switch (f) {
-                case F_INDICATOR: b_update<F_INDICATOR>(P, row, j, n, d); break;
-                case F_SPARSE: b_update<F_SPARSE>(P, row, j, n, d); break;
-                case F_DENSE: b_update<F_DENSE>(P, row, j, n, d); break;
-                default: b_update<F_INTERCEPT>(P, row, j, n, d); break;
+                if (staged) {
+#pragma unroll
+                    for (int i = 0; i < kBE; ++i) {
+                        const int p = threadIdx.x + i * kBT;
+                        if (p >= n) continue;
+                        const int64_t k = st.k[p];
+                        const double xb = A[i].x + d * st.x[p];
+                        const double en = exp(xb);
+                        row[2 * k] = make_double2(xb, en);
+                        reinterpret_cast<double*>(row + 2 * k + 1)[0] = Dn[i] + (en - A[i].y);
+                    }
+                } else {
+                    switch (f) {
+                    case F_INDICATOR: b_update<F_INDICATOR>(P, row, j, n, d); break;
+                    case F_SPARSE: b_update<F_SPARSE>(P, row, j, n, d); break;
+                    case F_DENSE: b_update<F_DENSE>(P, row, j, n, d); break;
+                    default: b_update<F_INTERCEPT>(P, row, j, n, d); break;
+                    }
                 }
-                __syncthreads();
             }
+            __syncthreads();
+            buf ^= 1;
         }
         iteration = it + 1;
         const double cur = objective(ll, lp);
@@ -251,6 +360,10 @@ __global__ void __launch_bounds__(kBT, 2) batch_sweep_kernel(BatchParams P) {
         r.loglik = ll;
         r.objective = last;
         r.pred_loglik = pt.x;
+        r.steps = steps;
+        r.updates = updates;
+        r.update_entries = upd_entries;
+        r.sweep_entries = gh_entries;
         P.results[inst] = r;
     }
 }
@@ -258,8 +371,13 @@ __global__ void __launch_bounds__(kBT, 2) batch_sweep_kernel(BatchParams P) {
 }  // namespace
 
 cudaError_t launch_batch_sweep(const BatchParams& P, cudaStream_t stream) {
-    if (P.model == M_LOGISTIC) batch_sweep_kernel<M_LOGISTIC><<<P.n_inst, kBT, 0, stream>>>(P);
-    else batch_sweep_kernel<M_POISSON><<<P.n_inst, kBT, 0, stream>>>(P);
+    const size_t smem = sizeof(ColStage) * 2;
+    const void* fn = (P.model == M_LOGISTIC) ? (const void*)batch_sweep_kernel<M_LOGISTIC>
+                                             : (const void*)batch_sweep_kernel<M_POISSON>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if (P.model == M_LOGISTIC) batch_sweep_kernel<M_LOGISTIC><<<P.n_inst, kBT, smem, stream>>>(P);
+    else batch_sweep_kernel<M_POISSON><<<P.n_inst, kBT, smem, stream>>>(P);
     return cudaGetLastError();
 }
 

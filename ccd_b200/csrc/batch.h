@@ -14,6 +14,10 @@ struct BatchResult {
     double loglik;
     double objective;
     double pred_loglik;  // held-out rows' predictive log-likelihood
+    int64_t steps;       // coordinate steps taken (all sweeps)
+    int64_t updates;     // nonzero steps
+    int64_t update_entries;  // entries touched by the nonzero steps
+    int64_t sweep_entries;   // entries gathered by the gradient passes
 };
 
 struct BatchParams {
@@ -43,6 +47,7 @@ struct BatchParams {
     double* hdelta;            // n_inst x J
     double* xjy;               // n_inst x J
     BatchResult* results;      // n_inst
+    const int32_t* order;      // launch order of the instances (CTA b runs order[b]), or NULL
 };
 
 cudaError_t launch_batch_sweep(const BatchParams& P, cudaStream_t stream);

@@ -53,7 +53,8 @@ class _BatchDesc(C.Structure):
 class _BatchResult(C.Structure):
     _fields_ = [("return_flag", C.c_int32), ("iterations", C.c_int32),
                 ("log_likelihood", C.c_double), ("objective", C.c_double),
-                ("predictive_loglik", C.c_double)]
+                ("predictive_loglik", C.c_double), ("steps", C.c_int64), ("updates", C.c_int64),
+                ("update_entries", C.c_int64), ("gradient_entries", C.c_int64)]
 
 
 class _FitResult(C.Structure):
@@ -287,7 +288,9 @@ class Fit:
         _check(lib().ccdb_batch_find_mode(self.h, C.byref(bd), C.byref(ma), _p(beta),
                                           C.cast(res, C.c_void_p), C.byref(secs)))
         out = [{"flag": r.return_flag, "iterations": r.iterations, "loglik": r.log_likelihood,
-                "objective": r.objective, "pred_loglik": r.predictive_loglik} for r in res]
+                "objective": r.objective, "pred_loglik": r.predictive_loglik, "steps": r.steps,
+                "updates": r.updates, "update_entries": r.update_entries,
+                "gradient_entries": r.gradient_entries} for r in res]
         return beta, out, secs.value
 
     # --- CyclicCoordinateDescent::update

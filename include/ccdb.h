@@ -171,6 +171,10 @@ typedef struct {
     double objective;
     double predictive_loglik;  /* on its held-out rows (getPredictiveLogLikelihood,
                                   ModelSpecifics.hpp:652-690) */
+    int64_t steps;             /* coordinate steps over all sweeps */
+    int64_t updates;           /* nonzero steps */
+    int64_t update_entries;    /* column entries touched by the nonzero steps */
+    int64_t gradient_entries;  /* column entries gathered for gradients */
 } ccdb_batch_result;
 
 /* Fit n_instances models over the fit's matrix and outcomes in one launch:
