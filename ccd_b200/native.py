@@ -121,6 +121,8 @@ def lib() -> C.CDLL:
         L.ccdb_fit_model.argtypes = [_P, C.c_int64, C.c_int32, _P, _P, _P, _P, _P, C.POINTER(_FitDesc),
                                      _P, C.POINTER(_ModeArgs), _P, C.POINTER(_FitResult)]
         L.ccdb_batch_find_mode.argtypes = [_P, C.POINTER(_BatchDesc), C.POINTER(_ModeArgs), _P, _P, _P]
+        L.ccdb_column_gradient_hessian_noalloc.argtypes = [C.c_int32, C.c_int32, C.c_int64, _P, _P, _P,
+                                                           C.c_double, _P, _P]
         L.ccdb_sweep_levels.argtypes = [C.c_int64, C.c_int32, _P, _P, _P, _P, _P, _P]
         _lib = L
     return _lib

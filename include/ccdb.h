@@ -186,6 +186,36 @@ typedef struct {
 int ccdb_batch_find_mode(ccdb_fit* f, const ccdb_batch_desc* batch, const ccdb_mode_args* args,
                          double* beta_out, ccdb_batch_result* results, double* device_seconds);
 
+/* --- allocation-free gradient (no reference counterpart) -------------------- */
+
+/* For callers that cannot allocate device memory -- code running while a
+ * stream is captured into a CUDA graph, hosts whose device memory belongs to
+ * a pool they must not grow, embedders given a fixed device arena: the
+ * gradient and Hessian of one column of a logistic or Poisson model, computed
+ * from device buffers the caller owns.  This entry point has no counterpart
+ * in the reference; it allocates nothing.
+ *   rows[n_entries] (SPARSE/INDICATOR) and vals[n_entries] (SPARSE/DENSE):
+ *     the column, device memory; fmt is its FormatType; DENSE/INTERCEPT
+ *     columns cover rows 0..n_entries-1.
+ *   row_state: device array of 4 doubles per row {xBeta, offsExpXBeta,
+ *     denominator, weight} (weight 1 when unweighted).
+ *   xjy: the column's sum of x*y*weight.  out: device array of 2 doubles,
+ *     receives (gradient, Hessian) as computeGradientAndHessian defines them.
+ *   stream: a cudaStream_t (NULL: the default stream); the call only enqueues
+ *     work and returns, so synchronise before reading out.
+ * Partial sums go to a fixed scratch array compiled into the library (2,048
+ * slots; columns of at most 16,777,216 entries -- longer ones are rejected with
+ * CCDB_ERR_INVALID before anything is launched).  Every GPU that loads the
+ * library holds that array until the process exits.  All calls share it and
+ * it keeps the last call's contents (each call overwrites the slots it
+ * reads); calls whose kernels overlap on the GPU race on it.  The first call
+ * on each device looks up the array's device address (no allocation): make
+ * it before any stream capture. */
+int ccdb_column_gradient_hessian_noalloc(int32_t model_type, int32_t fmt, int64_t n_entries,
+                                         const int32_t* rows, const double* vals,
+                                         const double* row_state, double xjy, double* out,
+                                         void* stream);
+
 /* --- inspection (no reference counterpart) ---------------------------------- */
 
 /* Dependency level of every column in one fused sweep over this matrix
