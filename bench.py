@@ -54,7 +54,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--max-sweeps", type=int, default=1000,
                     help="cap on sweeps per findMode (profiling captures of one short launch)")
-    ap.add_argument("--workload", choices=["poisson_offset", "cv_grid"], default="poisson_offset",
+    ap.add_argument("--workload", choices=["poisson_offset", "cv_grid", "cox_breslow"],
+                    default="poisson_offset",
                     help="poisson_offset: plain fits (default); cv_grid: 10 folds x 20 Laplace "
                          "variances = 200 logistic fits over one shared 5e5 x 2e4 matrix")
     ap.add_argument("--plain-sample", type=int, default=3,
@@ -65,7 +66,14 @@ def parse():
     return ap.parse_args()
 
 
+WORKLOAD = "poisson_offset"
+
+
 def workload(rank: int, small: bool):
+    if WORKLOAD == "cox_breslow":
+        if small:
+            return synthetic.cox_breslow(seed=3 + rank, K=100_000, n_strata=100, P=5_000)
+        return synthetic.cox_breslow(seed=3 + rank)
     if small:
         d = synthetic.poisson_offset(seed=2 + rank, K=100_000, P=10_000, total_nnz=2e6, cap=5_000)
     else:
@@ -74,6 +82,14 @@ def workload(rank: int, small: bool):
 
 
 def config_of(d, small: bool) -> dict:
+    if WORKLOAD == "cox_breslow":
+        return {
+            "workload": "cox_breslow" + ("_small" if small else ""), "model": "cox (Breslow ties)",
+            "rows": d.K, "columns": d.J, "nnz": d.nnz, "strata": int(d.stratum.max()) + 1,
+            "prior": "laplace(0.05)", "convergence": "gradient, tol 1e-6", "precision": "fp64",
+            "step": "one converged findMode from a cold start",
+            "l2": "flushed between timed steps (512 MiB device write)",
+        }
     return {
         "workload": "poisson_offset" + ("_small" if small else ""),
         "model": "poisson",
@@ -84,6 +100,17 @@ def config_of(d, small: bool) -> dict:
         "step": "one converged findMode from a cold start",
         "l2": "flushed between timed steps (512 MiB device write)",
     }
+
+
+def column_slice(d, n_cols: int):
+    """The first n_cols columns of a problem (same rows, strata, times)."""
+    from ccd_b200.data import CyclopsData
+    n = min(n_cols, d.J)
+    cs = d.col_start[:n + 1].copy()
+    vs = d.val_start[:n + 1].copy()
+    return CyclopsData(d.model_type, d.y, cs, d.rows[:cs[-1]], vs, d.vals[:vs[-1]], d.fmt[:n],
+                       d.prior_type[:n], d.prior_var[:n], time=d.time, stratum=d.stratum,
+                       offset_col0=d.offset_col0)
 
 
 def cold_beta(d) -> np.ndarray:
@@ -215,6 +242,18 @@ def cpu_reference_sample(d, target_s: float = 15.0):
     from oracle import checker
     eng_cls = checker.best_engine()
     kind = "reference" if eng_cls is checker.ReferenceEngine else "port"
+    if WORKLOAD == "cox_breslow":
+        # O(#groups) per coordinate in the reference: time the first sweep over a
+        # 2,000-column slice of the same data (rows, strata, times unchanged)
+        ds = column_slice(d, 2000)
+        eng = eng_cls(ds)
+        t0 = time.perf_counter()
+        eng.fit(GRADIENT, 1e-6, max_iter=1)
+        t1 = time.perf_counter() - t0
+        eng.close()
+        return {"value": ds.J / t1, "unit": METRIC, "cores": 1, "kind": kind,
+                "sample": f"first sweep over the first {ds.J} columns of the same rows/strata "
+                          f"({ds.J} coordinate updates, {t1:.1f} s), single thread"}
     eng = eng_cls(d)
     t0 = time.perf_counter()
     eng.fit(GRADIENT, 1e-6, max_iter=1)
@@ -363,11 +402,11 @@ def run_ours(args, world, rank, local):
             "return_flag": last.return_flag,
             "e2e": {"value": tot_e2e / e2e_max, "unit": METRIC, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_source": peak_kind,
-                         "algorithmic_bytes_per_launch": per_launch_bytes,
-                         "kernel": "indep_sweep_kernel<POISSON> (one launch per findMode)",
-                         "traffic": traffic},
+            "roofline": ({"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                          "frac": achieved / peak, "peak_source": peak_kind,
+                          "algorithmic_bytes_per_launch": per_launch_bytes,
+                          "kernel": "indep_sweep_kernel<POISSON> (one launch per findMode)",
+                          "traffic": traffic} if WORKLOAD == "poisson_offset" else None),
             "gpu_launches": int(tot_launch),
             "clocks": clk,
         }
@@ -466,7 +505,9 @@ def run_cv(args, world, rank, local):
 
 
 def main():
+    global WORKLOAD
     args = parse()
+    WORKLOAD = args.workload
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
