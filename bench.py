@@ -60,6 +60,14 @@ def parse():
                          "variances = 200 logistic fits over one shared 5e5 x 2e4 matrix")
     ap.add_argument("--plain-sample", type=int, default=3,
                     help="cv_grid: instances also fitted one at a time by the plain solver")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed",
+                    help="cv_grid: the mixed-precision lockstep engine (default) or the FP64 one")
+    ap.add_argument("--group", type=int, default=0,
+                    help="cv_grid, mixed: instances per lockstep group (0: the engine's choice)")
+    ap.add_argument("--cv-columns", type=int, default=20_000,
+                    help="cv_grid: covariate columns (fewer for short profiling captures)")
+    ap.add_argument("--fp64-check", type=int, default=4,
+                    help="cv_grid, mixed: instances also fitted by the FP64 engine to report the error")
     ap.add_argument("--trace", default=None,
                     help="write a per-level timestamp trace of the last timed findMode's first "
                          "sweep to this file (summarise with python -m ccd_b200.trace)")
@@ -420,11 +428,11 @@ def run_ours(args, world, rank, local):
         tdist.destroy_process_group()
 
 
-def cv_workload(small: bool):
+def cv_workload(small: bool, columns: int = 20_000):
     if small:
-        d = synthetic.logistic_cv(seed=4, K=50_000, P=2_000)
+        d = synthetic.logistic_cv(seed=4, K=50_000, P=max(1, columns // 10))
     else:
-        d = synthetic.logistic_cv(seed=4)
+        d = synthetic.logistic_cv(seed=4, P=columns)
     fold = synthetic.cv_folds(d.K, n_folds=10, seed=7)
     hold, var = synthetic.cv_grid(n_folds=10, n_vars=20, lower=1e-4, upper=1.0)
     return d, fold, hold, var
@@ -444,26 +452,44 @@ def cv_bytes(d, res) -> float:
 def run_cv(args, world, rank, local):
     import torch
     from ccd_b200 import native
-    d, fold, hold, var = cv_workload(args.small)
+    d, fold, hold, var = cv_workload(args.small, args.cv_columns)
+    mixed = args.precision == "mixed"
+    prec = native.PRECISION_MIXED if mixed else native.PRECISION_FP64
     ctx = native.Context(local)
     m = native.Matrix(ctx, d)
-    f = native.Fit(ctx, m, d)
+    f = native.Fit(ctx, m, d, precision=prec)
     margs = native.ModeFindingArguments(convergence_type=GRADIENT, tolerance=1e-6,
                                         max_iterations=args.max_sweeps)
+    grid = lambda fit: fit.batch_find_mode(var, hold, fold, margs, group=args.group)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
     for _ in range(args.warmup):
-        f.batch_find_mode(var, hold, fold, margs)
+        grid(f)
     clocks = Clocks(local)
     clocks.start()
-    t, fits, res_all = 0.0, 0, None
+    t, fits, res_all, beta_all = 0.0, 0, None, None
     for _ in range(args.steps):
         flush.fill_(1)
         torch.cuda.synchronize()
-        beta, res, secs = f.batch_find_mode(var, hold, fold, margs)
+        beta, res, secs = grid(f)
         t += secs
         fits += len(var)
-        res_all = res
+        res_all, beta_all = res, beta
     clk = clocks.stop()
+    # end to end through the C ABI from host buffers: matrix upload, fit, coefficients back
+    e2e_t = 0.0
+    h2d = d.rows.nbytes + d.vals.nbytes + d.col_start.nbytes + d.val_start.nbytes + d.fmt.nbytes \
+        + d.y.nbytes + fold.astype(np.int32).nbytes + var.nbytes + hold.astype(np.int32).nbytes
+    d2h = len(var) * d.J * 8
+    for _ in range(args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        me = native.Matrix(ctx, d)
+        fe = native.Fit(ctx, me, d, precision=prec)
+        grid(fe)
+        e2e_t += time.perf_counter() - t0
+        fe.close()
+        me.close()
     # the plain solver on a sample of the same instances, one at a time
     plain_t, plain_n = 0.0, 0
     for i in np.linspace(0, len(var) - 1, args.plain_sample).astype(int):
@@ -475,33 +501,78 @@ def run_cv(args, world, rank, local):
         plain_t += r.device_seconds
         plain_n += 1
         fi.close()
+    # error of the mixed engine against the FP64 engine on a sample of instances
+    err = None
+    if mixed and args.fp64_check > 0:
+        idx = np.linspace(0, len(var) - 1, args.fp64_check).astype(int)
+        f64 = native.Fit(ctx, m, d)
+        b64, r64, _ = f64.batch_find_mode(var[idx], hold[idx], fold, margs)
+        f64.close()
+        ce = [float(np.max(np.abs(beta_all[i] - b64[q])) / max(np.max(np.abs(b64[q])), 1e-8))
+              for q, i in enumerate(idx)]
+        le = [abs(res_all[i]["loglik"] - r64[q]["loglik"]) / abs(r64[q]["loglik"]) for q, i in enumerate(idx)]
+        err = {"instances": [int(i) for i in idx], "max_rel_coef": max(ce), "max_rel_loglik": max(le),
+               "same_sweeps": int(sum(res_all[i]["iterations"] == r64[q]["iterations"] for q, i in enumerate(idx))),
+               "fp64_engine": "FP64 batched engine (parity-tested against the reference CPU engine)"}
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = cv_cpu_sample(d, fold, hold, var, res_all)
     peak, peak_kind = read_peaks()
     byts = cv_bytes(d, res_all)
     achieved = byts / (t / args.steps) / 1e9
     sweeps = [r["iterations"] for r in res_all]
+    kernel = "batch_mixed_kernel<LOGISTIC>" if mixed else "batch_sweep_kernel<LOGISTIC>"
     line = {
         "metric": "converged fits/s", "value": fits / t, "unit": "fits/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32/f64 (f32 exp, ratios, per-entry terms; f64 state, reductions, step)" if mixed else "f64",
         "data": "synthetic (seeded PCG64, workload shapes of the benchmark config)",
-        "config": {"workload": "cv_grid" + ("_small" if args.small else ""), "model": "logistic",
+        "config": {"workload": "cv_grid" + ("_small" if args.small else "")
+                   + ("" if args.cv_columns == 20_000 else f"_{args.cv_columns}cols"), "model": "logistic",
                    "rows": d.K, "columns": d.J, "nnz": d.nnz, "instances": len(var),
                    "folds": 10, "variances": "20 log-uniform in [1e-4, 1] (Laplace)",
                    "convergence": "gradient, tol 1e-6", "start": "cold (beta = 0) per instance",
+                   "precision": args.precision, "group": args.group or "engine's choice",
                    "step": "one grid of 200 fits to convergence",
                    "l2": "flushed between timed steps (512 MiB device write)"},
-        "plain_fits_per_s": plain_n / plain_t,
-        "batched_over_plain": (fits / t) / (plain_n / plain_t),
-        "plain_sample": f"{plain_n} instances fitted one at a time by ccdb_find_mode",
+        "e2e": {"value": fits / e2e_t, "unit": "fits/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "plain_fits_per_s": plain_n / plain_t if plain_n else None,
+        "batched_over_plain": (fits / t) / (plain_n / plain_t) if plain_n else None,
+        "plain_sample": f"{plain_n} instances fitted one at a time by ccdb_find_mode (FP64)",
         "sweeps_per_fit": {"min": int(min(sweeps)), "median": float(np.median(sweeps)), "max": int(max(sweeps))},
+        "error_vs_fp64": err,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
-                     "algorithmic_bytes_per_launch": byts, "kernel": "batch_sweep_kernel<LOGISTIC>",
+                     "algorithmic_bytes_per_launch": byts, "kernel": kernel,
                      "traffic": None},
+        "cpu_baseline": cpu,
         "gpu_launches": args.steps,
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
+
+
+def cv_cpu_sample(d, fold, hold, var, res):
+    """The reference CPU engine on a bounded sample of the grid: the first sweep of
+    the median-variance instance, single thread; fits/s = 1 / (that sweep time x the
+    mean sweeps per fit the grid needed)."""
+    from oracle import checker
+    eng_cls = checker.best_engine()
+    kind = "reference" if eng_cls is checker.ReferenceEngine else "port"
+    i = len(var) // 2
+    di = d.with_prior(1, float(var[i]))
+    e = eng_cls(di)
+    e.set_weights((fold != hold[i]).astype(float))
+    t0 = time.perf_counter()
+    e.fit(GRADIENT, 1e-6, 1)
+    t_sweep = time.perf_counter() - t0
+    e.close()
+    mean_sweeps = float(np.mean([r["iterations"] for r in res]))
+    return {"value": 1.0 / (t_sweep * mean_sweeps), "unit": "fits/s", "cores": 1, "kind": kind,
+            "sample": f"first sweep of instance {i} (variance {var[i]:.3g}), {t_sweep:.2f} s, "
+                      f"x {mean_sweeps:.1f} mean sweeps per fit of this grid, single thread"}
 
 
 def main():

@@ -820,7 +820,9 @@ int ccdb_fit_create(ccdb_context* ctx, const ccdb_matrix* m, const ccdb_fit_desc
             throw Error(CCDB_ERR_INVALID, "conditional models need stratum ids");
         if (d->model_type == M_COX && !d->time)
             throw Error(CCDB_ERR_INVALID, "Cox fits need survival times");
-        if (d->precision != CCDB_PRECISION_FP64)
+        if (d->precision != CCDB_PRECISION_FP64 &&
+            !(d->precision == CCDB_PRECISION_MIXED &&
+              (d->model_type == M_LOGISTIC || d->model_type == M_POISSON)))
             throw Error(CCDB_ERR_UNSUPPORTED, "precision not supported for this model");
         check_cuda(cudaSetDevice(ctx->device), "cudaSetDevice");
         std::unique_ptr<ccdb_fit> f(new ccdb_fit());
@@ -880,6 +882,13 @@ int ccdb_fit_destroy(ccdb_fit* f) {
     return guard([&] { delete f; });
 }
 
+// Mixed precision is implemented by the batched engine; the single-fit calls
+// compute in FP64 only and refuse a mixed fit rather than ignore its setting.
+static void require_fp64(const ccdb_fit* f) {
+    if (f->precision != CCDB_PRECISION_FP64)
+        throw Error(CCDB_ERR_UNSUPPORTED, "mixed precision serves batched fits (ccdb_batch_find_mode) only");
+}
+
 int ccdb_set_weights(ccdb_fit* f, const double* w) {
     return guard([&] {
         require(f != nullptr, "NULL fit");
@@ -908,6 +917,7 @@ int ccdb_set_beta(ccdb_fit* f, const double* beta) {
 int ccdb_compute_gradient_hessian(ccdb_fit* f, int32_t j, double* g, double* h) {
     return guard([&] {
         require(f && g && h, "NULL argument");
+        require_fp64(f);
         require(j >= 0 && j < f->J, "column out of range");
         f->gradient_hessian(j, g, h);
     });
@@ -916,6 +926,7 @@ int ccdb_compute_gradient_hessian(ccdb_fit* f, int32_t j, double* g, double* h) 
 int ccdb_update_xbeta(ccdb_fit* f, int32_t j, double delta) {
     return guard([&] {
         require(f != nullptr, "NULL fit");
+        require_fp64(f);
         require(j >= 0 && j < f->J, "column out of range");
         f->update_xbeta(j, delta);
     });
@@ -924,6 +935,7 @@ int ccdb_update_xbeta(ccdb_fit* f, int32_t j, double delta) {
 int ccdb_compute_remaining_statistics(ccdb_fit* f) {
     return guard([&] {
         require(f != nullptr, "NULL fit");
+        require_fp64(f);
         f->check_lazy();
         f->remaining_statistics();
         check_cuda(cudaStreamSynchronize(f->stream), "sync");
@@ -933,6 +945,7 @@ int ccdb_compute_remaining_statistics(ccdb_fit* f) {
 int ccdb_get_log_likelihood(ccdb_fit* f, double* ll) {
     return guard([&] {
         require(f && ll, "NULL argument");
+        require_fp64(f);
         *ll = f->log_likelihood();
     });
 }
@@ -940,6 +953,7 @@ int ccdb_get_log_likelihood(ccdb_fit* f, double* ll) {
 int ccdb_get_xbeta(ccdb_fit* f, double* out) {
     return guard([&] {
         require(f && out, "NULL argument");
+        require_fp64(f);
         f->check_lazy();
         const int stride = f->group_engine() ? 1 : 2;
         const double2* src = f->group_engine() ? f->cox.xbe : f->row;
@@ -954,6 +968,7 @@ int ccdb_get_xbeta(ccdb_fit* f, double* out) {
 int ccdb_get_gradient_objective(ccdb_fit* f, double* out) {
     return guard([&] {
         require(f && out, "NULL argument");
+        require_fp64(f);
         double t[4];
         f->objective_terms(t);
         *out = t[2];
@@ -970,6 +985,7 @@ int ccdb_get_beta(ccdb_fit* f, double* out) {
 int ccdb_find_mode(ccdb_fit* f, const ccdb_mode_args* args, double* beta_inout, ccdb_fit_result* res) {
     return guard([&] {
         require(f && args, "NULL argument");
+        require_fp64(f);
         check_cuda(cudaSetDevice(f->ctx->device), "cudaSetDevice");
         f->find_mode(*args, beta_inout, res);
     });
@@ -1006,6 +1022,19 @@ int ccdb_fit_model(ccdb_context* ctx, int64_t K, int32_t J, const int64_t* col_s
     if (m) ccdb_matrix_destroy(m);
     g_last_error = err;
     return rc;
+}
+
+// Lockstep group size of the mixed-precision batched engine.  G = 4 packs the
+// group's state for one row into one 32-byte sector (a quarter of the DRAM
+// sectors G = 1 moves per instance), but gives one CTA G times the per-column
+// arithmetic and leaves ceil(n / G) CTAs for the SMs.  Take the largest G that
+// still gives every third SM a CTA.
+static int batch_group_size(const Matrix* m, int n, int n_sm) {
+    (void)m;
+    const int want = std::max(1, n_sm / 3);
+    for (int G : {4, 2})
+        if ((n + G - 1) / G >= want) return G;
+    return 1;
 }
 
 int ccdb_batch_find_mode(ccdb_fit* f, const ccdb_batch_desc* b, const ccdb_mode_args* a, double* beta_out,
@@ -1066,37 +1095,93 @@ int ccdb_batch_find_mode(ccdb_fit* f, const ccdb_batch_desc* b, const ccdb_mode_
                         table.push_back(c >= 2 ? table.back() + -std::log((double)c) : 0.0);
                     }
                     const double t = yi >= 2 ? table[yi] : 0.0;
-                    const double w = (b->row_fold && b->row_fold[k] == hold[i]) ? 0.0 : 1.0;
+                    const double w = (b->row_fold && hold[i] >= 0 && b->row_fold[k] == hold[i]) ? 0.0 : 1.0;
                     acc += t * w;
                 }
                 fixed[i] = acc;
             }
             P.ll_fixed = (const double*)keep(upload(ctx, fixed.data(), (size_t)n, s));
         }
-        P.row = (double2*)keep(ctx->alloc(sizeof(double2) * 2 * (size_t)K * n));
-        P.beta = (double*)keep(ctx->alloc(sizeof(double) * (size_t)J * n));
-        P.hdelta = (double*)keep(ctx->alloc(sizeof(double) * (size_t)J * n));
-        P.xjy = (double*)keep(ctx->alloc(sizeof(double) * (size_t)J * n));
-        P.results = (BatchResult*)keep(ctx->alloc(sizeof(BatchResult) * n));
+        const bool mixed = f->precision == CCDB_PRECISION_MIXED;
         // weakest priors first: they need the most sweeps, so they start in the first wave
+        // (and, in mixed precision, instances of similar variance share a group)
         std::vector<int32_t> order(n);
         for (int i = 0; i < n; ++i) order[i] = i;
         std::stable_sort(order.begin(), order.end(),
                          [&](int32_t x, int32_t y) { return b->variance[x] > b->variance[y]; });
         P.order = (const int32_t*)keep(upload(ctx, order.data(), (size_t)n, s));
+        P.results = (BatchResult*)keep(ctx->alloc(sizeof(BatchResult) * n));
+        int G = 1, n_groups = n;
+        if (mixed) {
+            G = b->group ? b->group : batch_group_size(m, n, ctx->n_sm);
+            if (G != 1 && G != 2 && G != 4) throw Error(CCDB_ERR_INVALID, "batch group must be 1, 2 or 4");
+            n_groups = (n + G - 1) / G;
+            P.group = G;
+            // the mixed engine reads each entry's fold with its row id (row | fold << 24)
+            if (K > kKeyRowMask)
+                throw Error(CCDB_ERR_UNSUPPORTED, "mixed batched fits: at most 16,777,215 rows");
+            for (int i = 0; i < n; ++i)
+                if (hold[i] >= kKeyNoFold)
+                    throw Error(CCDB_ERR_UNSUPPORTED, "mixed batched fits: held-out fold ids below 127");
+            const int64_t nnz = m->col_start.back();
+            int32_t* keys = (int32_t*)keep(ctx->alloc(sizeof(int32_t) * (size_t)std::max<int64_t>(nnz, 1)));
+            check_cuda(launch_batch_keys(m->d_rows, nnz, P.row_fold, keys, s), "batch keys");
+            P.keys = keys;
+            const char* pf = std::getenv("CCDB_BATCH_PREFETCH");
+            P.prefetch = pf ? std::atoi(pf) : 1;
+            P.xg = (double*)keep(ctx->alloc(sizeof(double) * (size_t)K * G * n_groups));
+            P.beta_g = (double*)keep(ctx->alloc(sizeof(double) * (size_t)J * G * n_groups));
+            P.hd_g = (double*)keep(ctx->alloc(sizeof(double) * (size_t)J * G * n_groups));
+            P.xjy_g = (double*)keep(ctx->alloc(sizeof(double) * (size_t)J * G * n_groups));
+        } else {
+            P.row = (double2*)keep(ctx->alloc(sizeof(double2) * 2 * (size_t)K * n));
+            P.beta = (double*)keep(ctx->alloc(sizeof(double) * (size_t)J * n));
+            P.hdelta = (double*)keep(ctx->alloc(sizeof(double) * (size_t)J * n));
+            P.xjy = (double*)keep(ctx->alloc(sizeof(double) * (size_t)J * n));
+        }
+        // CCDB_BATCH_TRACE_FILE: per-column phase clocks of CTA 0 in one sweep
+        // (CCDB_BATCH_TRACE_SWEEP, default 1) of the mixed engine, written as int64 [J][6]
+        const char* trace_path = mixed ? std::getenv("CCDB_BATCH_TRACE_FILE") : nullptr;
+        if (trace_path) {
+            const char* sw = std::getenv("CCDB_BATCH_TRACE_SWEEP");
+            P.trace_sweep = sw ? std::atoi(sw) : 1;
+            P.trace = (long long*)keep(ctx->alloc(sizeof(long long) * 6 * (size_t)J));
+            check_cuda(cudaMemsetAsync(P.trace, 0, sizeof(long long) * 6 * (size_t)J, s), "trace");
+        }
         cudaEvent_t e0, e1;
         check_cuda(cudaEventCreate(&e0), "event");
         check_cuda(cudaEventCreate(&e1), "event");
         check_cuda(cudaEventRecord(e0, s), "event");
-        check_cuda(launch_batch_sweep(P, s), "batch sweep");
+        if (mixed) check_cuda(launch_batch_mixed(P, s), "batch sweep (mixed)");
+        else check_cuda(launch_batch_sweep(P, s), "batch sweep");
         check_cuda(cudaEventRecord(e1, s), "event");
         std::vector<BatchResult> res(n);
         check_cuda(cudaMemcpyAsync(res.data(), P.results, sizeof(BatchResult) * n, cudaMemcpyDeviceToHost, s),
                    "results");
-        if (beta_out)
+        std::vector<double> bg;
+        if (beta_out && mixed) {
+            bg.resize((size_t)J * G * n_groups);
+            check_cuda(cudaMemcpyAsync(bg.data(), P.beta_g, sizeof(double) * bg.size(), cudaMemcpyDeviceToHost, s),
+                       "beta");
+        } else if (beta_out) {
             check_cuda(cudaMemcpyAsync(beta_out, P.beta, sizeof(double) * (size_t)J * n, cudaMemcpyDeviceToHost, s),
                        "beta");
+        }
         check_cuda(cudaStreamSynchronize(s), "batch sync");
+        if (trace_path) {
+            std::vector<long long> tr(6 * (size_t)J);
+            check_cuda(cudaMemcpy(tr.data(), P.trace, sizeof(long long) * tr.size(), cudaMemcpyDeviceToHost),
+                       "trace copy");
+            if (FILE* fh = std::fopen(trace_path, "wb")) {
+                std::fwrite(tr.data(), sizeof(long long), tr.size(), fh);
+                std::fclose(fh);
+            }
+        }
+        if (beta_out && mixed)  // [group][J][G] -> [instance][J]
+            for (int q = 0; q < n; ++q) {
+                const int grp = q / G, gi = q % G, inst = order[q];
+                for (int j = 0; j < J; ++j) beta_out[(size_t)inst * J + j] = bg[((size_t)grp * J + j) * G + gi];
+            }
         float ms = 0.f;
         check_cuda(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
         cudaEventDestroy(e0);

@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(kBT, 1) batch_sweep_kernel(BatchParams P) {
     for (int64_t k = threadIdx.x; k < P.K; k += kBT) {
         const double xb = P.offset_vals ? 0.0 + 1.0 * P.offset_vals[k] : 0.0;
         const double e = exp(xb);
-        const double w = (P.row_fold && P.row_fold[k] == hold) ? 0.0 : 1.0;
+        const double w = (P.row_fold && hold >= 0 && P.row_fold[k] == hold) ? 0.0 : 1.0;
         row[2 * k] = make_double2(xb, e);
         row[2 * k + 1] = make_double2(null_denom + e, w);
     }

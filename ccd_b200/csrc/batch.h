@@ -48,8 +48,33 @@ struct BatchParams {
     double* xjy;               // n_inst x J
     BatchResult* results;      // n_inst
     const int32_t* order;      // launch order of the instances (CTA b runs order[b]), or NULL
+    // mixed precision (batch_mixed.cu): CTA b runs instances order[b*group .. b*group+group-1]
+    // in lockstep; their state is interleaved instance-minor so that one row's
+    // state for the whole group is one 32-byte sector at group 4.
+    int32_t group;             // instances per CTA: 1, 2 or 4
+    int32_t pad1;
+    double* xg;                // n_groups x K x group: xBeta
+    double* beta_g;            // n_groups x J x group
+    double* hd_g;              // n_groups x J x group
+    double* xjy_g;             // n_groups x J x group
+    // optional phase trace of CTA 0, sweep `trace_sweep`: per column six SM clock
+    // stamps (start, issued, terms, reduced, updated, end); NULL: off
+    long long* trace;
+    int32_t trace_sweep;
+    int32_t prefetch;          // mixed: prefetch the rows of a later column into L2 (0/1)
+    // mixed: per entry of the row-indexed columns, row id | fold code << 24
+    // (fold code: the row's fold id, or 127 for rows in no fold)
+    const int32_t* keys;
 };
 
+constexpr int kKeyRowBits = 24;
+constexpr int32_t kKeyRowMask = (1 << kKeyRowBits) - 1;
+constexpr int kKeyNoFold = 127;
+
 cudaError_t launch_batch_sweep(const BatchParams& P, cudaStream_t stream);
+cudaError_t launch_batch_mixed(const BatchParams& P, cudaStream_t stream);
+// keys[e] = rows[e] | code(fold[rows[e]]) << 24 for e < nnz
+cudaError_t launch_batch_keys(const int32_t* rows, int64_t nnz, const int32_t* fold, int32_t* keys,
+                              cudaStream_t stream);
 
 }  // namespace ccdb

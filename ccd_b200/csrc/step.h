@@ -16,14 +16,15 @@ CCDB_HD int sgn_d(double x) { return x == 0 ? 0 : (x < 0 ? -1 : 1); }
 
 // ccdUpdateBeta's clamp + JointPrior::getDelta (CyclicCoordinateDescent.cpp:1394-1413;
 // priors/CovariatePrior.h:186-188 NoPrior, :240-273 Laplace, :410-415 Normal).
-CCDB_HD double newton_prior_delta(double g, double h, double beta, int ptype,
-                                                     double var) {
+// `lambda` is sqrt(2 / var) of a Laplace prior (CovariatePrior.h:282-292),
+// passed in by callers that take many steps under one variance.
+CCDB_HD double newton_prior_delta_l(double g, double h, double beta, int ptype, double var,
+                                    double lambda) {
     if (h < 0.0) {
         g = 0.0;
         h = 0.0;
     }
     if (ptype == 1) {
-        const double lambda = sqrt(2.0 / var);
         const double neg = -(g - lambda) / h;
         const double pos = -(g + lambda) / h;
         const int s = sgn_d(beta);
@@ -41,6 +42,10 @@ CCDB_HD double newton_prior_delta(double g, double h, double beta, int ptype,
         return -(g + (beta / var)) / (h + (1.0 / var));
     }
     return -(g / h);
+}
+
+CCDB_HD double newton_prior_delta(double g, double h, double beta, int ptype, double var) {
+    return newton_prior_delta_l(g, h, beta, ptype, var, ptype == 1 ? sqrt(2.0 / var) : 0.0);
 }
 
 // applyBounds (CyclicCoordinateDescent.cpp:1503-1520), std::max semantics.

@@ -9,6 +9,7 @@ library is missing or no GPU is present, constructing a ``Context`` raises.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 import os
 from dataclasses import dataclass
 from typing import Optional
@@ -47,7 +48,7 @@ class _ModeArgs(C.Structure):
 
 class _BatchDesc(C.Structure):
     _fields_ = [("n_instances", C.c_int32), ("row_fold", C.c_void_p), ("holdout", C.c_void_p),
-                ("variance", C.c_void_p)]
+                ("variance", C.c_void_p), ("group", C.c_int32)]
 
 
 class _BatchResult(C.Structure):
@@ -149,6 +150,9 @@ class Context:
         _check(lib().ccdb_context_create(device, hbm_budget, C.byref(h)))
         self.h = h
         self.device = device
+        # matrices and fits made on this context: closed before it, whatever
+        # order the interpreter releases the Python objects in
+        self._children = weakref.WeakSet()
 
     def memory_in_use(self) -> int:
         v = C.c_size_t()
@@ -157,6 +161,9 @@ class Context:
 
     def close(self):
         if getattr(self, "h", None):
+            kids = list(getattr(self, "_children", ()))
+            for c in sorted(kids, key=lambda c: isinstance(c, Matrix)):  # fits, then matrices
+                c.close()
             lib().ccdb_context_destroy(self.h)
             self.h = None
 
@@ -178,6 +185,7 @@ class Matrix:
         h = _P()
         _check(lib().ccdb_matrix_create(ctx.h, d.K, d.J, *[_p(a) for a in arrs], C.byref(h)))
         self.h = h
+        ctx._children.add(self)
 
     def close(self):
         if getattr(self, "h", None):
@@ -219,6 +227,7 @@ class Fit:
         h = _P()
         _check(lib().ccdb_fit_create(ctx.h, matrix.h, C.byref(desc), C.byref(h)))
         self.h = h
+        ctx._children.add(self)
 
     def close(self):
         if getattr(self, "h", None):
@@ -273,8 +282,9 @@ class Fit:
 
     # --- the cross-validation grid: many instances in one launch
     def batch_find_mode(self, variance, holdout=None, row_fold=None,
-                        args: Optional[ModeFindingArguments] = None):
+                        args: Optional[ModeFindingArguments] = None, group: int = 0):
         """Fit len(variance) instances (fold held out, prior variance) together.
+        ``group``: lockstep group size of a mixed-precision fit (0: the engine's choice).
         Returns (beta[n, J], list of per-instance dicts, device seconds)."""
         args = args or ModeFindingArguments()
         keep = []
@@ -283,7 +293,7 @@ class Fit:
         n = var.shape[0]
         hold = None if holdout is None else _c(holdout, np.int32)
         fold = None if row_fold is None else _c(row_fold, np.int32)
-        bd = _BatchDesc(n, _p(fold), _p(hold), _p(var))
+        bd = _BatchDesc(n, _p(fold), _p(hold), _p(var), int(group))
         beta = np.zeros((n, self.d.J))
         res = (_BatchResult * n)()
         secs = C.c_double()

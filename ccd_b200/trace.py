@@ -6,6 +6,11 @@ global timer at: wait start, level open, end of the CTA-wide phase, end of
 the warp phase, arrival.  ``python -m ccd_b200.trace <path>`` prints where the
 time of a sweep goes: level-to-level detection, per-level span, and the phase
 breakdown by segment kind.
+
+``CCDB_BATCH_TRACE_FILE=<path>`` does the same for the mixed-precision batched
+engine: CTA 0's SM clock at six points of every column of one sweep
+(``CCDB_BATCH_TRACE_SWEEP``, default 1).  ``python -m ccd_b200.trace --batch
+<path> [sm_mhz]`` prints the per-phase breakdown.
 """
 from __future__ import annotations
 
@@ -67,5 +72,27 @@ def summarise(path: str) -> str:
     return "\n".join(out)
 
 
+BATCH_PHASES = ("issue (stage, prefetch, metadata)", "gather + FP32 terms", "group reduction",
+                "step + update", "cp.async wait + barrier")
+
+
+def summarise_batch(path: str, sm_mhz: float = 1965.0) -> str:
+    tr = np.fromfile(path, np.int64).reshape(-1, 6)
+    cols = np.nonzero(tr[:, 0])[0]
+    t = tr[cols]
+    per = np.diff(t, axis=1)  # five phases
+    span = np.diff(t[:, 0])
+    us = 1.0 / sm_mhz
+    out = [f"columns traced: {len(cols)}; sweep span {(t[-1, 5] - t[0, 0]) * us / 1e3:.2f} ms; "
+           f"median column {np.median(span) * us:.2f} us (mean {span.mean() * us:.2f} us)"]
+    for name, col in zip(BATCH_PHASES, per.T):
+        out.append(f"  {name:34s} median {np.median(col) * us:7.3f} us  mean {col.mean() * us:7.3f} us  "
+                   f"share {col.sum() / per.sum():6.1%}")
+    return "\n".join(out)
+
+
 if __name__ == "__main__":
-    print(summarise(sys.argv[1]))
+    if sys.argv[1] == "--batch":
+        print(summarise_batch(sys.argv[2], *(float(a) for a in sys.argv[3:4])))
+    else:
+        print(summarise(sys.argv[1]))

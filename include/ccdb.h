@@ -40,7 +40,9 @@ extern "C" {
 #define CCDB_ERR_TIMEOUT (-5)     /* a bounded device-side wait ran out */
 
 #define CCDB_PRECISION_FP64 0  /* all arithmetic in double, as the reference's RealType=double */
-#define CCDB_PRECISION_MIXED 1 /* FP32 row state and gathers, compensated sums, FP64 step */
+#define CCDB_PRECISION_MIXED 1 /* batched fits only: FP64 xBeta and step; exp, ratios and
+                                  per-entry gradient/Hessian terms in FP32 with compensated
+                                  sums; FP64 cross-thread reductions and log-likelihoods */
 
 typedef struct ccdb_context ccdb_context;
 typedef struct ccdb_matrix ccdb_matrix;
@@ -162,6 +164,8 @@ typedef struct {
     const int32_t* row_fold; /* K fold id per row, or NULL (no row held out) */
     const int32_t* holdout;  /* n_instances: fold held out by each instance (-1: none) */
     const double* variance;  /* n_instances: prior variance of the regularised columns */
+    int32_t group;           /* CCDB_PRECISION_MIXED fits: instances stepped in lockstep per CTA
+                                (1, 2 or 4); 0 lets the engine choose.  Ignored for FP64 fits. */
 } ccdb_batch_desc;
 
 typedef struct {
@@ -182,7 +186,10 @@ typedef struct {
  * CrossValidationSelector::getWeights gives, drivers/CrossValidationSelector.cpp:72-130),
  * uses args->prior_type per column with variance[i], and starts from beta = 0.
  * Each instance runs the sequential sweep of a standalone fit; instances do not
- * interact.  Logistic and Poisson models.  beta_out: n_instances x J. */
+ * interact.  Logistic and Poisson models.  beta_out: n_instances x J.
+ * A CCDB_PRECISION_MIXED fit runs the mixed-precision engine, whose instances
+ * step through the columns in lockstep groups of batch->group (at most
+ * 16,777,215 rows; held-out fold ids below 127). */
 int ccdb_batch_find_mode(ccdb_fit* f, const ccdb_batch_desc* batch, const ccdb_mode_args* args,
                          double* beta_out, ccdb_batch_result* results, double* device_seconds);
 
