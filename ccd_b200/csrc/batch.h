@@ -73,6 +73,7 @@ constexpr int kKeyNoFold = 127;
 
 cudaError_t launch_batch_sweep(const BatchParams& P, cudaStream_t stream);
 cudaError_t launch_batch_mixed(const BatchParams& P, cudaStream_t stream);
+
 // keys[e] = rows[e] | code(fold[rows[e]]) << 24 for e < nnz
 cudaError_t launch_batch_keys(const int32_t* rows, int64_t nnz, const int32_t* fold, int32_t* keys,
                               cudaStream_t stream);

@@ -82,3 +82,4 @@ def test_mixed_rejected_by_single_fit_calls(gpu_ctx):
     f = native.Fit(gpu_ctx, m, d, precision=native.PRECISION_MIXED)
     with pytest.raises(native.CcdbError, match="batched fits"):
         f.find_mode()
+
