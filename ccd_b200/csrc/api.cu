@@ -1037,6 +1037,36 @@ static int batch_group_size(const Matrix* m, int n, int n_sm) {
     return 1;
 }
 
+// Longest slice of a row-indexed column when C CTAs split the rows evenly.
+static int64_t batch_max_slice(const Matrix* m, int64_t K, int C) {
+    int64_t mx = 0;
+    for (int j = 0; j < m->J; ++j) {
+        if (m->fmt[j] != F_SPARSE && m->fmt[j] != F_INDICATOR) continue;
+        const int32_t* r0 = m->rows_h.data() + m->col_start[j];
+        const int32_t* r1 = m->rows_h.data() + m->col_start[j + 1];
+        const int32_t* lo = r0;
+        for (int r = 1; r <= C; ++r) {
+            const int32_t* hi = (r == C) ? r1 : std::lower_bound(lo, r1, K * r / C);
+            mx = std::max<int64_t>(mx, hi - lo);
+            lo = hi;
+        }
+    }
+    return mx;
+}
+
+// CTAs per group of the mixed engine.  The per-column critical path shrinks
+// when a column's rows are split over more SMs (each gathers and updates only
+// its slice), and the kernel's registers suffice without spills for the small
+// stage (1024 entries per slice).  Take the smallest power of two that both
+// fits every slice in the small stage and puts a CTA on every SM; at most 8.
+static int batch_cluster_size(const Matrix* m, int64_t K, int n_groups, int n_sm) {
+    for (int C = 1; C <= 8; C *= 2)
+        if ((int64_t)n_groups * C >= n_sm && batch_max_slice(m, K, C) <= 1024) return C;
+    for (int C = 1; C <= 8; C *= 2)
+        if (batch_max_slice(m, K, C) <= 1024) return C;
+    return 8;
+}
+
 int ccdb_batch_find_mode(ccdb_fit* f, const ccdb_batch_desc* b, const ccdb_mode_args* a, double* beta_out,
                          ccdb_batch_result* results, double* device_seconds) {
     return guard([&] {
@@ -1129,6 +1159,30 @@ int ccdb_batch_find_mode(ccdb_fit* f, const ccdb_batch_desc* b, const ccdb_mode_
             P.keys = keys;
             const char* pf = std::getenv("CCDB_BATCH_PREFETCH");
             P.prefetch = pf ? std::atoi(pf) : 1;
+            // CTAs per group (a cluster splits each column's rows among its CTAs);
+            // CCDB_BATCH_CLUSTER overrides
+            int C = batch_cluster_size(m, K, n_groups, ctx->n_sm);
+            if (const char* cs = std::getenv("CCDB_BATCH_CLUSTER")) C = std::atoi(cs);
+            if (C < 1 || C > 16) throw Error(CCDB_ERR_INVALID, "batch cluster size must be 1..16");
+            P.cluster = C;
+            // per row-indexed column, where its rows cross the CTAs' row boundaries;
+            // the stage capacity is the small variant when every slice fits it
+            std::vector<int32_t> split((size_t)J * (C + 1), 0);
+            int64_t max_slice = 0;
+            for (int j = 0; j < J; ++j) {
+                const int64_t cb = m->col_start[j], ce = m->col_start[j + 1];
+                const int32_t* r0 = m->rows_h.data() + cb;
+                const int32_t* r1 = m->rows_h.data() + ce;
+                int32_t* sp = split.data() + (size_t)j * (C + 1);
+                for (int r = 0; r <= C; ++r)
+                    sp[r] = (r == C) ? (int32_t)(ce - cb) : (int32_t)(std::lower_bound(r0, r1, K * r / C) - r0);
+                if (m->fmt[j] == F_SPARSE || m->fmt[j] == F_INDICATOR)
+                    for (int r = 0; r < C; ++r) max_slice = std::max<int64_t>(max_slice, sp[r + 1] - sp[r]);
+            }
+            if (C > 1) P.split = (const int32_t*)keep(upload(ctx, split.data(), split.size(), s));
+            P.stage_cap = max_slice <= 1024 ? 1024 : 3072;
+            P.min_blocks = 1;
+            if (const char* mb = std::getenv("CCDB_BATCH_MINB")) P.min_blocks = std::atoi(mb) == 2 ? 2 : 1;
             P.xg = (double*)keep(ctx->alloc(sizeof(double) * (size_t)K * G * n_groups));
             P.beta_g = (double*)keep(ctx->alloc(sizeof(double) * (size_t)J * G * n_groups));
             P.hd_g = (double*)keep(ctx->alloc(sizeof(double) * (size_t)J * G * n_groups));
@@ -1187,6 +1241,9 @@ int ccdb_batch_find_mode(ccdb_fit* f, const ccdb_batch_desc* b, const ccdb_mode_
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         if (device_seconds) *device_seconds = ms * 1e-3;
+        for (int i = 0; i < n; ++i)
+            if (res[i].flag == kBatchTimeoutFlag)
+                throw Error(CCDB_ERR_CUDA, "batched fits: a bounded device wait between cluster CTAs ran out");
         if (results)
             for (int i = 0; i < n; ++i) {
                 results[i].return_flag = res[i].flag;

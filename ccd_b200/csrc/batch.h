@@ -65,6 +65,14 @@ struct BatchParams {
     // mixed: per entry of the row-indexed columns, row id | fold code << 24
     // (fold code: the row's fold id, or 127 for rows in no fold)
     const int32_t* keys;
+    // mixed: CTAs per group (a thread-block cluster; CTA r owns rows
+    // [K r / C, K (r + 1) / C)) and, when above 1, per row-indexed column the
+    // C + 1 entry offsets where its rows cross those boundaries (J x (C + 1))
+    int32_t cluster;
+    int32_t stage_cap;         // mixed: staged entries per slice (1024 or 3072)
+    int32_t min_blocks;        // mixed, stage_cap 1024: CTAs per SM the kernel is built for (1 or 2)
+    int32_t pad4;
+    const int32_t* split;
 };
 
 constexpr int kKeyRowBits = 24;
@@ -73,6 +81,7 @@ constexpr int kKeyNoFold = 127;
 
 cudaError_t launch_batch_sweep(const BatchParams& P, cudaStream_t stream);
 cudaError_t launch_batch_mixed(const BatchParams& P, cudaStream_t stream);
+constexpr int32_t kBatchTimeoutFlag = -100;  // result flag: a bounded device wait ran out
 
 // keys[e] = rows[e] | code(fold[rows[e]]) << 24 for e < nnz
 cudaError_t launch_batch_keys(const int32_t* rows, int64_t nnz, const int32_t* fold, int32_t* keys,

@@ -45,34 +45,40 @@ constexpr int kRing = 8;           // column metadata ring: columns j .. j + kAh
 
 using namespace bm;
 
-template <int MODEL, int G>
-__global__ void __launch_bounds__(kMT, 1) batch_mixed_kernel(BatchParams P) {
+template <int MODEL, int G, int SN, int MINB>
+__global__ void __launch_bounds__(kMT, MINB) batch_mixed_kernel(BatchParams P) {
     constexpr int S = Inst<G>::S;    // threads per instance
-    constexpr int kE = kStageN / S;  // staged entries per thread
+    constexpr int kE = SN / S;       // staged entries per thread
     __shared__ double s_red2[2][kMW][4][2];
     __shared__ double s_red4[2][kMW][4][4];
+    __shared__ double s_xch2[2][4][2];  // cluster exchange of per-CTA sums
+    __shared__ double s_xch4[2][4][4];
     __shared__ MMeta s_meta[kRing];
+    __shared__ ColXch s_xch;  // per-column exchange of (g, h) between the CTAs of a cluster
     extern __shared__ __align__(16) unsigned char s_dyn[];
-    MStage* st = reinterpret_cast<MStage*>(s_dyn);
+    MStage<SN>* st = reinterpret_cast<MStage<SN>*>(s_dyn);
 
-    const Inst<G> I(P);
+    const Inst<G> I(P, P.cluster);
     const int g = I.g, sl = I.sl, hold = I.hold, J = I.J;
     double* X = I.X;
-    int rb2 = 0, rb4 = 0;
-    inst_setup<G>(P, I, s_red2, rb2);
+    int rb2 = 0, rb4 = 0, xb2 = 0, xb4 = 0;
+    unsigned xph = 0;  // parity bits of the exchange slots
+    if (threadIdx.x == 0 && I.C > 1) xch_init(s_xch);
+    inst_setup<G>(P, I, s_red2, rb2, s_xch2, xb2);  // ends with a cluster barrier
+    bool late = false;
 
     const int j0 = P.offset_vals ? 1 : 0;
     const bool need_ll = P.conv != C_GRADIENT;
     bool active = I.exists;
     double ll = 0.0;
-    double last = inst_objective<MODEL, G>(P, I, active, need_ll, ll, s_red4, rb4);
+    double last = inst_objective<MODEL, G>(P, I, active, need_ll, ll, s_red4, rb4, s_xch4, xb4);
     int iteration = 0, flag = R_FAIL;
     InstCounters cnt;
 
     auto stage = [&](int col) {
         const MMeta m = s_meta[col & (kRing - 1)];
-        if (!stageable(m)) return;
-        MStage& b = st[col % kNBuf];
+        if (!stageable<SN>(m)) return;
+        MStage<SN>& b = st[col % kNBuf];
         for (int p = threadIdx.x; p < m.n; p += kMT) {
             cp_async4(&b.k[p], P.keys + m.cb + p);
             if (m.fmt == F_SPARSE) cp_async8(&b.x[p], P.vals + m.vb + p);
@@ -80,8 +86,8 @@ __global__ void __launch_bounds__(kMT, 1) batch_mixed_kernel(BatchParams P) {
     };
     auto prefetch = [&](int col) {
         const MMeta m1 = s_meta[col & (kRing - 1)];
-        if (!stageable(m1)) return;
-        const MStage& b = st[col % kNBuf];
+        if (!stageable<SN>(m1)) return;
+        const MStage<SN>& b = st[col % kNBuf];
         for (int p = threadIdx.x; p < m1.n; p += kMT)
             asm volatile("prefetch.global.L2 [%0];" ::"l"(X + (int64_t)(b.k[p] & kKeyRowMask) * G));
     };
@@ -89,7 +95,7 @@ __global__ void __launch_bounds__(kMT, 1) batch_mixed_kernel(BatchParams P) {
     while (__syncthreads_or(active)) {
         // sweep prologue: metadata of the first kAhead + 1 columns, stage the first kAhead
         if (threadIdx.x <= kAhead && j0 + (int)threadIdx.x < J)
-            s_meta[(j0 + threadIdx.x) & (kRing - 1)] = load_meta(P, j0 + threadIdx.x);
+            s_meta[(j0 + threadIdx.x) & (kRing - 1)] = I.meta(P, j0 + threadIdx.x);
         __syncthreads();
         for (int q = 0; q < kAhead; ++q)
             if (j0 + q < J) stage(j0 + q);
@@ -118,7 +124,7 @@ __global__ void __launch_bounds__(kMT, 1) batch_mixed_kernel(BatchParams P) {
             const MMeta m = s_meta[j & (kRing - 1)];
             const int n = m.n;
             const bool ind = (m.fmt == F_INDICATOR || m.fmt == F_INTERCEPT);
-            const bool staged = stageable(m);
+            const bool staged = stageable<SN>(m);
             const double b0 = nb0, hd0 = nhd0, xjy0 = nxjy0;
             const int pt = npt;
             if (j + 1 < J) {
@@ -129,8 +135,8 @@ __global__ void __launch_bounds__(kMT, 1) batch_mixed_kernel(BatchParams P) {
                 }
                 npt = P.ptype[j + 1];
             }
-            MMeta nm{};
-            if (threadIdx.x == 0 && j + kAhead + 1 < J) nm = load_meta(P, j + kAhead + 1);
+            RawMeta nm{};
+            if (threadIdx.x == 0 && j + kAhead + 1 < J) nm = I.raw(P, j + kAhead + 1);
             if (j + kAhead < J) stage(j + kAhead);
             cp_async_commit();
             if (P.prefetch && j + kPf < J) prefetch(j + kPf);
@@ -139,7 +145,7 @@ __global__ void __launch_bounds__(kMT, 1) batch_mixed_kernel(BatchParams P) {
             // gather and FP32 terms with compensated sums
             float gs = 0.f, gc = 0.f, hs = 0.f, hc = 0.f;
             double xr[kE];
-            const MStage& c = st[j % kNBuf];
+            const MStage<SN>& c = st[j % kNBuf];
             if (staged) {
                 if (active) {
                     // loads only: every gather of the column is in flight at once
@@ -164,7 +170,7 @@ __global__ void __launch_bounds__(kMT, 1) batch_mixed_kernel(BatchParams P) {
                 const bool has_rows = (m.fmt == F_SPARSE || m.fmt == F_INDICATOR);
                 const bool has_vals = (m.fmt == F_SPARSE || m.fmt == F_DENSE);
                 for (int64_t p = sl; p < n; p += S) {
-                    const int64_t k = has_rows ? (int64_t)__ldg(P.rows + m.cb + p) : p;
+                    const int64_t k = has_rows ? (int64_t)__ldg(P.rows + m.cb + p) : m.cb + p;
                     if (I.held(k)) continue;
                     const float x = has_vals ? (float)__ldg(P.vals + m.vb + p) : 1.0f;
                     float gt, ht;
@@ -176,10 +182,11 @@ __global__ void __launch_bounds__(kMT, 1) batch_mixed_kernel(BatchParams P) {
             double gh[2] = {(double)gs + (double)gc, (double)hs + (double)hc};
             if (tr) tr[6 * j + 2] = clock64();
             group_sum<G, 2>(gh, s_red2, rb2);
+            if (I.C > 1 && !xch_sum<G>(I, gh, s_xch, j, xph)) late = true;
             if (tr) tr[6 * j + 3] = clock64();
 
             // the step, computed identically by every thread of the instance
-            const double d = active ? inst_step<G>(I, j, n, gh[0], gh[1], b0, hd0, xjy0, pt, cnt) : 0.0;
+            const double d = active ? inst_step<G>(I, j, m.ntot, gh[0], gh[1], b0, hd0, xjy0, pt, cnt) : 0.0;
             // update xBeta (FP64) from the gathered registers
             if (d != 0.0) {
                 if (staged) {
@@ -195,25 +202,37 @@ __global__ void __launch_bounds__(kMT, 1) batch_mixed_kernel(BatchParams P) {
                     const bool has_rows = (m.fmt == F_SPARSE || m.fmt == F_INDICATOR);
                     const bool has_vals = (m.fmt == F_SPARSE || m.fmt == F_DENSE);
                     for (int64_t p = sl; p < n; p += S) {
-                        const int64_t k = has_rows ? (int64_t)__ldg(P.rows + m.cb + p) : p;
+                        const int64_t k = has_rows ? (int64_t)__ldg(P.rows + m.cb + p) : m.cb + p;
                         const double x = has_vals ? __ldg(P.vals + m.vb + p) : 1.0;
                         X[k * G + g] += d * x;
                     }
                 }
             }
-            if (threadIdx.x == 0 && j + kAhead + 1 < J) s_meta[(j + kAhead + 1) & (kRing - 1)] = nm;
+            if (threadIdx.x == 0 && j + kAhead + 1 < J) s_meta[(j + kAhead + 1) & (kRing - 1)] = I.cook(nm);
             if (tr) tr[6 * j + 4] = clock64();
             cp_async_wait_but_last();
-            __syncthreads();
+            if (__syncthreads_or(late)) {
+                late = true;
+                break;
+            }
             if (tr) tr[6 * j + 5] = clock64();
         }
         cp_async_wait_all();
+        if (late) break;
 
         if (active) ++iteration;
-        const double cur = inst_objective<MODEL, G>(P, I, active, need_ll, ll, s_red4, rb4);
+        const double cur = inst_objective<MODEL, G>(P, I, active, need_ll, ll, s_red4, rb4, s_xch4, xb4);
         if (active) inst_converge(P, cur, last, iteration, flag, active);
     }
-    inst_finish<MODEL, G>(P, I, flag, iteration, last, cnt, s_red4, rb4);
+    if (late) {  // a wait for the other CTAs' sums ran out: report, no more cluster barriers
+        if (I.exists && I.sl == 0 && I.rank == 0) {
+            BatchResult r{};
+            r.flag = kBatchTimeoutFlag;
+            P.results[I.inst] = r;
+        }
+        return;
+    }
+    inst_finish<MODEL, G>(P, I, flag, iteration, last, cnt, s_red4, rb4, s_xch4, xb4);
 }
 
 __global__ void batch_keys_kernel(const int32_t* rows, int64_t nnz, const int32_t* fold, int32_t* keys) {
@@ -226,23 +245,46 @@ __global__ void batch_keys_kernel(const int32_t* rows, int64_t nnz, const int32_
     }
 }
 
-template <int MODEL, int G>
+template <int MODEL, int G, int SN, int MINB>
 cudaError_t launch_g(const BatchParams& P, cudaStream_t stream) {
-    const size_t smem = sizeof(MStage) * kNBuf;
-    cudaError_t e = cudaFuncSetAttribute(batch_mixed_kernel<MODEL, G>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t smem = sizeof(MStage<SN>) * kNBuf;
+    void (*fn)(BatchParams) = batch_mixed_kernel<MODEL, G, SN, MINB>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    const int C = P.cluster > 0 ? P.cluster : 1;
+    if (C > 8) {
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return e;
+    }
     const int n_groups = (P.n_inst + G - 1) / G;
-    batch_mixed_kernel<MODEL, G><<<n_groups, kMT, smem, stream>>>(P);
-    return cudaGetLastError();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(n_groups * C);
+    cfg.blockDim = dim3(kMT);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, fn, P);
+}
+
+template <int MODEL, int G>
+cudaError_t launch_sn(const BatchParams& P, cudaStream_t stream) {
+    if (P.stage_cap <= 1024)
+        return P.min_blocks == 2 ? launch_g<MODEL, G, 1024, 2>(P, stream) : launch_g<MODEL, G, 1024, 1>(P, stream);
+    return launch_g<MODEL, G, 3072, 1>(P, stream);
 }
 
 template <int MODEL>
 cudaError_t launch_m(const BatchParams& P, cudaStream_t stream) {
     switch (P.group) {
-    case 1: return launch_g<MODEL, 1>(P, stream);
-    case 2: return launch_g<MODEL, 2>(P, stream);
-    case 4: return launch_g<MODEL, 4>(P, stream);
+    case 1: return launch_sn<MODEL, 1>(P, stream);
+    case 2: return launch_sn<MODEL, 2>(P, stream);
+    case 4: return launch_sn<MODEL, 4>(P, stream);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -29,13 +29,16 @@ def _rel(b, want):
     return np.max(np.abs(b - want)) / max(np.max(np.abs(want)), 1e-8)
 
 
+@pytest.mark.parametrize("cluster", [1, 3])
 @pytest.mark.parametrize("group", [1, 2, 4])
 @pytest.mark.parametrize("model,kw,conv", [
     (MODEL_LOGISTIC, dict(seed=70, K=800, P=30), GRADIENT),
     (MODEL_LOGISTIC, dict(seed=71, K=600, P=20, formats=("sparse", "dense", "indicator")), MITTAL),
     (MODEL_POISSON, dict(seed=72, K=600, P=20, offset=True, prior=PRIOR_NORMAL), MITTAL),
 ])
-def test_mixed_batch_matches_fp64_oracle(gpu_ctx, oracle_engine, model, kw, conv, group):
+def test_mixed_batch_matches_fp64_oracle(gpu_ctx, oracle_engine, monkeypatch, model, kw, conv, group, cluster):
+    """cluster: CTAs per group, each owning a row range of every column."""
+    monkeypatch.setenv("CCDB_BATCH_CLUSTER", str(cluster))
     d = synthetic.small(model, **kw)
     fold = synthetic.cv_folds(d.K, n_folds=5, seed=4)
     hold, var = synthetic.cv_grid(n_folds=5, n_vars=3, lower=0.01, upper=10.0)
@@ -57,12 +60,14 @@ def test_mixed_batch_matches_fp64_oracle(gpu_ctx, oracle_engine, model, kw, conv
         assert abs(res[i]["loglik"] - want["loglik"]) <= LL_TOL * abs(want["loglik"]), i
         pred = e.predictive_loglik(1.0 - w)
         assert abs(res[i]["pred_loglik"] - pred) <= PRED_TOL * max(1.0, abs(pred)), i
-    print(f"mixed group={group}: max relative coefficient error {worst:.2e}")
+    print(f"mixed group={group} cluster={cluster}: max relative coefficient error {worst:.2e}")
 
 
-def test_mixed_instance_alone_equals_in_group(gpu_ctx):
+@pytest.mark.parametrize("cluster", [1, 4])
+def test_mixed_instance_alone_equals_in_group(gpu_ctx, monkeypatch, cluster):
     """An instance's arithmetic does not depend on its group mates: alone (its
     group padded) it gives bit-identical coefficients."""
+    monkeypatch.setenv("CCDB_BATCH_CLUSTER", str(cluster))
     d = synthetic.small(MODEL_LOGISTIC, seed=73, K=700, P=25)
     fold = synthetic.cv_folds(d.K, n_folds=4, seed=2)
     hold, var = synthetic.cv_grid(n_folds=4, n_vars=3, lower=0.05, upper=5.0)
