@@ -1157,8 +1157,10 @@ int ccdb_batch_find_mode(ccdb_fit* f, const ccdb_batch_desc* b, const ccdb_mode_
             int32_t* keys = (int32_t*)keep(ctx->alloc(sizeof(int32_t) * (size_t)std::max<int64_t>(nnz, 1)));
             check_cuda(launch_batch_keys(m->d_rows, nnz, P.row_fold, keys, s), "batch keys");
             P.keys = keys;
+            // L2 prefetch of a later column's rows: off by default (it spends the SM's
+            // load-issue slots, which bound the column, and measured no gain)
             const char* pf = std::getenv("CCDB_BATCH_PREFETCH");
-            P.prefetch = pf ? std::atoi(pf) : 1;
+            P.prefetch = pf ? std::atoi(pf) : 0;
             // CTAs per group (a cluster splits each column's rows among its CTAs);
             // CCDB_BATCH_CLUSTER overrides
             int C = batch_cluster_size(m, K, n_groups, ctx->n_sm);
@@ -1181,6 +1183,8 @@ int ccdb_batch_find_mode(ccdb_fit* f, const ccdb_batch_desc* b, const ccdb_mode_
             }
             if (C > 1) P.split = (const int32_t*)keep(upload(ctx, split.data(), split.size(), s));
             P.stage_cap = max_slice <= 1024 ? 1024 : 3072;
+            P.queue = (int32_t*)keep(ctx->alloc(sizeof(int32_t)));
+            check_cuda(cudaMemsetAsync(P.queue, 0, sizeof(int32_t), s), "batch queue");
             P.min_blocks = 1;
             if (const char* mb = std::getenv("CCDB_BATCH_MINB")) P.min_blocks = std::atoi(mb) == 2 ? 2 : 1;
             P.xg = (double*)keep(ctx->alloc(sizeof(double) * (size_t)K * G * n_groups));

@@ -73,6 +73,7 @@ struct BatchParams {
     int32_t min_blocks;        // mixed, stage_cap 1024: CTAs per SM the kernel is built for (1 or 2)
     int32_t pad4;
     const int32_t* split;
+    int32_t* queue;            // mixed: next group to fit (zeroed before the launch)
 };
 
 constexpr int kKeyRowBits = 24;

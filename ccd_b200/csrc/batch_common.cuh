@@ -187,10 +187,10 @@ struct Inst {
     double var, lambda;
     const int32_t* fold;  // NULL when the instance holds nothing out
 
-    __device__ Inst(const BatchParams& P, int cluster) {
+    __device__ Inst(const BatchParams& P, int cluster, int group, int cta_rank) {
         C = cluster;
-        grp = blockIdx.x / C;
-        rank = blockIdx.x % C;
+        grp = group;
+        rank = cta_rank;
         g = threadIdx.x % G;
         sl = threadIdx.x / G;
         const int pos = grp * G + g;
@@ -382,8 +382,8 @@ __device__ double inst_objective(const BatchParams& P, const Inst<G>& I, bool ac
     return ll_out + acc[3];
 }
 
-struct InstCounters {
-    long long steps = 0, updates = 0, upd_entries = 0, gh_entries = 0;
+struct InstCounters {  // kept in shared memory, updated by one thread per instance
+    long long steps, updates, upd_entries, gh_entries;
 };
 
 // The coordinate step of one instance (ccdUpdateBeta + applyBounds), computed

@@ -30,6 +30,7 @@
 //   * the coefficient, bound and XjY of column j+1 are loaded into registers;
 //   * column j's state is gathered into registers, reduced, stepped, and the
 //     updated xBeta written back from the same registers.
+#include <algorithm>
 #include <cstdint>
 
 #include "batch_common.cuh"
@@ -58,181 +59,205 @@ __global__ void __launch_bounds__(kMT, MINB) batch_mixed_kernel(BatchParams P) {
     extern __shared__ __align__(16) unsigned char s_dyn[];
     MStage<SN>* st = reinterpret_cast<MStage<SN>*>(s_dyn);
 
-    const Inst<G> I(P, P.cluster);
-    const int g = I.g, sl = I.sl, hold = I.hold, J = I.J;
-    double* X = I.X;
+    const int C = P.cluster > 0 ? P.cluster : 1;
+    const int rank = (int)(blockIdx.x % C);
+    const int n_groups = (P.n_inst + G - 1) / G;
+    __shared__ int s_grp;
+    __shared__ InstCounters s_cnt[4];
     int rb2 = 0, rb4 = 0, xb2 = 0, xb4 = 0;
     unsigned xph = 0;  // parity bits of the exchange slots
-    if (threadIdx.x == 0 && I.C > 1) xch_init(s_xch);
-    inst_setup<G>(P, I, s_red2, rb2, s_xch2, xb2);  // ends with a cluster barrier
-    bool late = false;
+    if (threadIdx.x == 0 && C > 1) xch_init(s_xch);
 
-    const int j0 = P.offset_vals ? 1 : 0;
-    const bool need_ll = P.conv != C_GRADIENT;
-    bool active = I.exists;
-    double ll = 0.0;
-    double last = inst_objective<MODEL, G>(P, I, active, need_ll, ll, s_red4, rb4, s_xch4, xb4);
-    int iteration = 0, flag = R_FAIL;
-    InstCounters cnt;
-
-    auto stage = [&](int col) {
-        const MMeta m = s_meta[col & (kRing - 1)];
-        if (!stageable<SN>(m)) return;
-        MStage<SN>& b = st[col % kNBuf];
-        for (int p = threadIdx.x; p < m.n; p += kMT) {
-            cp_async4(&b.k[p], P.keys + m.cb + p);
-            if (m.fmt == F_SPARSE) cp_async8(&b.x[p], P.vals + m.vb + p);
+    // Groups come from a queue in launch order (weakest priors first), so the
+    // longest fits start first whatever order the clusters are scheduled in.
+    for (;;) {
+        if (rank == 0 && threadIdx.x == 0) s_grp = atomicAdd(P.queue, 1);
+        int grp;
+        if (C > 1) {
+            cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+            cl.sync();
+            grp = *cl.map_shared_rank(&s_grp, 0);
+            cl.sync();  // every CTA has read rank 0's slot before any of them leaves or refills it
+        } else {
+            __syncthreads();
+            grp = s_grp;
         }
-    };
-    auto prefetch = [&](int col) {
-        const MMeta m1 = s_meta[col & (kRing - 1)];
-        if (!stageable<SN>(m1)) return;
-        const MStage<SN>& b = st[col % kNBuf];
-        for (int p = threadIdx.x; p < m1.n; p += kMT)
-            asm volatile("prefetch.global.L2 [%0];" ::"l"(X + (int64_t)(b.k[p] & kKeyRowMask) * G));
-    };
+        if (grp >= n_groups) break;
+        const Inst<G> I(P, C, grp, rank);
+        const int g = I.g, sl = I.sl, hold = I.hold, J = I.J;
+        double* X = I.X;
+        inst_setup<G>(P, I, s_red2, rb2, s_xch2, xb2);  // ends with a cluster barrier
+        bool late = false;
 
-    while (__syncthreads_or(active)) {
-        // sweep prologue: metadata of the first kAhead + 1 columns, stage the first kAhead
-        if (threadIdx.x <= kAhead && j0 + (int)threadIdx.x < J)
-            s_meta[(j0 + threadIdx.x) & (kRing - 1)] = I.meta(P, j0 + threadIdx.x);
-        __syncthreads();
-        for (int q = 0; q < kAhead; ++q)
-            if (j0 + q < J) stage(j0 + q);
-        cp_async_commit();
-        cp_async_wait_all();
-        __syncthreads();
-        if (P.prefetch)
-            for (int q = 0; q < kPf; ++q)
-                if (j0 + q < J) prefetch(j0 + q);
-        // coefficient, bound, XjY and prior of the next column, one column ahead
-        double nb0 = 0.0, nhd0 = 0.0, nxjy0 = 0.0;
-        int npt = 0;
-        if (j0 < J) {
-            if (active) {
-                nb0 = I.Bt[(size_t)j0 * G + g];
-                nhd0 = I.Hd[(size_t)j0 * G + g];
-                nxjy0 = I.Xy[(size_t)j0 * G + g];
-            }
-            npt = P.ptype[j0];
-        }
-        long long* tr = (P.trace && blockIdx.x == 0 && threadIdx.x == 0 && iteration == P.trace_sweep)
-                            ? P.trace : nullptr;
+        const int j0 = P.offset_vals ? 1 : 0;
+        const bool need_ll = P.conv != C_GRADIENT;
+        bool active = I.exists;
+        double ll = 0.0;
+        double last = inst_objective<MODEL, G>(P, I, active, need_ll, ll, s_red4, rb4, s_xch4, xb4);
+        int iteration = 0, flag = R_FAIL;
+        if (threadIdx.x < 4) s_cnt[threadIdx.x] = InstCounters{0, 0, 0, 0};
+        InstCounters& cnt = s_cnt[g];
 
-        for (int j = j0; j < J; ++j) {
-            if (tr) tr[6 * j] = clock64();
-            const MMeta m = s_meta[j & (kRing - 1)];
-            const int n = m.n;
-            const bool ind = (m.fmt == F_INDICATOR || m.fmt == F_INTERCEPT);
-            const bool staged = stageable<SN>(m);
-            const double b0 = nb0, hd0 = nhd0, xjy0 = nxjy0;
-            const int pt = npt;
-            if (j + 1 < J) {
-                if (active) {
-                    nb0 = I.Bt[(size_t)(j + 1) * G + g];
-                    nhd0 = I.Hd[(size_t)(j + 1) * G + g];
-                    nxjy0 = I.Xy[(size_t)(j + 1) * G + g];
-                }
-                npt = P.ptype[j + 1];
+        auto stage = [&](int col) {
+            const MMeta m = s_meta[col & (kRing - 1)];
+            if (!stageable<SN>(m)) return;
+            MStage<SN>& b = st[col % kNBuf];
+            for (int p = threadIdx.x; p < m.n; p += kMT) {
+                cp_async4(&b.k[p], P.keys + m.cb + p);
+                if (m.fmt == F_SPARSE) cp_async8(&b.x[p], P.vals + m.vb + p);
             }
-            RawMeta nm{};
-            if (threadIdx.x == 0 && j + kAhead + 1 < J) nm = I.raw(P, j + kAhead + 1);
-            if (j + kAhead < J) stage(j + kAhead);
+        };
+        auto prefetch = [&](int col) {
+            const MMeta m1 = s_meta[col & (kRing - 1)];
+            if (!stageable<SN>(m1)) return;
+            const MStage<SN>& b = st[col % kNBuf];
+            for (int p = threadIdx.x; p < m1.n; p += kMT)
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(X + (int64_t)(b.k[p] & kKeyRowMask) * G));
+        };
+
+        while (__syncthreads_or(active)) {
+            // sweep prologue: metadata of the first kAhead + 1 columns, stage the first kAhead
+            if (threadIdx.x <= kAhead && j0 + (int)threadIdx.x < J)
+                s_meta[(j0 + threadIdx.x) & (kRing - 1)] = I.meta(P, j0 + threadIdx.x);
+            __syncthreads();
+            for (int q = 0; q < kAhead; ++q)
+                if (j0 + q < J) stage(j0 + q);
             cp_async_commit();
-            if (P.prefetch && j + kPf < J) prefetch(j + kPf);
-            if (tr) tr[6 * j + 1] = clock64();
-
-            // gather and FP32 terms with compensated sums
-            float gs = 0.f, gc = 0.f, hs = 0.f, hc = 0.f;
-            double xr[kE];
-            const MStage<SN>& c = st[j % kNBuf];
-            if (staged) {
+            cp_async_wait_all();
+            __syncthreads();
+            if (P.prefetch)
+                for (int q = 0; q < kPf; ++q)
+                    if (j0 + q < J) prefetch(j0 + q);
+            // coefficient, bound, XjY and prior of the next column, one column ahead
+            double nb0 = 0.0, nhd0 = 0.0, nxjy0 = 0.0;
+            int npt = 0;
+            if (j0 < J) {
                 if (active) {
-                    // loads only: every gather of the column is in flight at once
-#pragma unroll
-                    for (int i = 0; i < kE; ++i) {
-                        const int p = sl + i * S;
-                        if (p < n) xr[i] = X[(int64_t)(c.k[p] & kKeyRowMask) * G + g];
-                    }
-#pragma unroll
-                    for (int i = 0; i < kE; ++i) {
-                        const int p = sl + i * S;
-                        if (p < n && (c.k[p] >> kKeyRowBits) != hold) {
-                            const float x = (m.fmt == F_SPARSE) ? (float)c.x[p] : 1.0f;
-                            float gt, ht;
-                            entry_terms<MODEL>(xr[i], x, ind, gt, ht);
-                            two_sum(gs, gc, gt);
-                            two_sum(hs, hc, ht);
-                        }
-                    }
+                    nb0 = I.Bt[(size_t)j0 * G + g];
+                    nhd0 = I.Hd[(size_t)j0 * G + g];
+                    nxjy0 = I.Xy[(size_t)j0 * G + g];
                 }
-            } else if (active) {
-                const bool has_rows = (m.fmt == F_SPARSE || m.fmt == F_INDICATOR);
-                const bool has_vals = (m.fmt == F_SPARSE || m.fmt == F_DENSE);
-                for (int64_t p = sl; p < n; p += S) {
-                    const int64_t k = has_rows ? (int64_t)__ldg(P.rows + m.cb + p) : m.cb + p;
-                    if (I.held(k)) continue;
-                    const float x = has_vals ? (float)__ldg(P.vals + m.vb + p) : 1.0f;
-                    float gt, ht;
-                    entry_terms<MODEL>(X[k * G + g], x, ind, gt, ht);
-                    two_sum(gs, gc, gt);
-                    two_sum(hs, hc, ht);
-                }
+                npt = P.ptype[j0];
             }
-            double gh[2] = {(double)gs + (double)gc, (double)hs + (double)hc};
-            if (tr) tr[6 * j + 2] = clock64();
-            group_sum<G, 2>(gh, s_red2, rb2);
-            if (I.C > 1 && !xch_sum<G>(I, gh, s_xch, j, xph)) late = true;
-            if (tr) tr[6 * j + 3] = clock64();
+            long long* tr = (P.trace && blockIdx.x == 0 && threadIdx.x == 0 && iteration == P.trace_sweep)
+                                ? P.trace : nullptr;
 
-            // the step, computed identically by every thread of the instance
-            const double d = active ? inst_step<G>(I, j, m.ntot, gh[0], gh[1], b0, hd0, xjy0, pt, cnt) : 0.0;
-            // update xBeta (FP64) from the gathered registers
-            if (d != 0.0) {
+            for (int j = j0; j < J; ++j) {
+                if (tr) tr[6 * j] = clock64();
+                const MMeta m = s_meta[j & (kRing - 1)];
+                const int n = m.n;
+                const bool ind = (m.fmt == F_INDICATOR || m.fmt == F_INTERCEPT);
+                const bool staged = stageable<SN>(m);
+                const double b0 = nb0, hd0 = nhd0, xjy0 = nxjy0;
+                const int pt = npt;
+                if (j + 1 < J) {
+                    if (active) {
+                        nb0 = I.Bt[(size_t)(j + 1) * G + g];
+                        nhd0 = I.Hd[(size_t)(j + 1) * G + g];
+                        nxjy0 = I.Xy[(size_t)(j + 1) * G + g];
+                    }
+                    npt = P.ptype[j + 1];
+                }
+                RawMeta nm{};
+                if (threadIdx.x == 0 && j + kAhead + 1 < J) nm = I.raw(P, j + kAhead + 1);
+                if (j + kAhead < J) stage(j + kAhead);
+                cp_async_commit();
+                if (P.prefetch && j + kPf < J) prefetch(j + kPf);
+                if (tr) tr[6 * j + 1] = clock64();
+
+                // gather and FP32 terms with compensated sums
+                float gs = 0.f, gc = 0.f, hs = 0.f, hc = 0.f;
+                double xr[kE];
+                const MStage<SN>& c = st[j % kNBuf];
                 if (staged) {
-#pragma unroll
-                    for (int i = 0; i < kE; ++i) {
-                        const int p = sl + i * S;
-                        if (p < n) {
-                            const double x = (m.fmt == F_SPARSE) ? c.x[p] : 1.0;
-                            X[(int64_t)(c.k[p] & kKeyRowMask) * G + g] = xr[i] + d * x;
+                    if (active) {
+                        // loads only: every gather of the column is in flight at once
+    #pragma unroll
+                        for (int i = 0; i < kE; ++i) {
+                            const int p = sl + i * S;
+                            if (p < n) xr[i] = X[(int64_t)(c.k[p] & kKeyRowMask) * G + g];
+                        }
+    #pragma unroll
+                        for (int i = 0; i < kE; ++i) {
+                            const int p = sl + i * S;
+                            if (p < n && (c.k[p] >> kKeyRowBits) != hold) {
+                                const float x = (m.fmt == F_SPARSE) ? (float)c.x[p] : 1.0f;
+                                float gt, ht;
+                                entry_terms<MODEL>(xr[i], x, ind, gt, ht);
+                                two_sum(gs, gc, gt);
+                                two_sum(hs, hc, ht);
+                            }
                         }
                     }
-                } else {
+                } else if (active) {
                     const bool has_rows = (m.fmt == F_SPARSE || m.fmt == F_INDICATOR);
                     const bool has_vals = (m.fmt == F_SPARSE || m.fmt == F_DENSE);
                     for (int64_t p = sl; p < n; p += S) {
                         const int64_t k = has_rows ? (int64_t)__ldg(P.rows + m.cb + p) : m.cb + p;
-                        const double x = has_vals ? __ldg(P.vals + m.vb + p) : 1.0;
-                        X[k * G + g] += d * x;
+                        if (I.held(k)) continue;
+                        const float x = has_vals ? (float)__ldg(P.vals + m.vb + p) : 1.0f;
+                        float gt, ht;
+                        entry_terms<MODEL>(X[k * G + g], x, ind, gt, ht);
+                        two_sum(gs, gc, gt);
+                        two_sum(hs, hc, ht);
                     }
                 }
-            }
-            if (threadIdx.x == 0 && j + kAhead + 1 < J) s_meta[(j + kAhead + 1) & (kRing - 1)] = I.cook(nm);
-            if (tr) tr[6 * j + 4] = clock64();
-            cp_async_wait_but_last();
-            if (__syncthreads_or(late)) {
-                late = true;
-                break;
-            }
-            if (tr) tr[6 * j + 5] = clock64();
-        }
-        cp_async_wait_all();
-        if (late) break;
+                double gh[2] = {(double)gs + (double)gc, (double)hs + (double)hc};
+                if (tr) tr[6 * j + 2] = clock64();
+                group_sum<G, 2>(gh, s_red2, rb2);
+                if (I.C > 1 && !xch_sum<G>(I, gh, s_xch, j, xph)) late = true;
+                if (tr) tr[6 * j + 3] = clock64();
 
-        if (active) ++iteration;
-        const double cur = inst_objective<MODEL, G>(P, I, active, need_ll, ll, s_red4, rb4, s_xch4, xb4);
-        if (active) inst_converge(P, cur, last, iteration, flag, active);
-    }
-    if (late) {  // a wait for the other CTAs' sums ran out: report, no more cluster barriers
-        if (I.exists && I.sl == 0 && I.rank == 0) {
-            BatchResult r{};
-            r.flag = kBatchTimeoutFlag;
-            P.results[I.inst] = r;
+                // the step, computed identically by every thread of the instance
+                const double d = active ? inst_step<G>(I, j, m.ntot, gh[0], gh[1], b0, hd0, xjy0, pt, cnt) : 0.0;
+                // update xBeta (FP64) from the gathered registers
+                if (d != 0.0) {
+                    if (staged) {
+    #pragma unroll
+                        for (int i = 0; i < kE; ++i) {
+                            const int p = sl + i * S;
+                            if (p < n) {
+                                const double x = (m.fmt == F_SPARSE) ? c.x[p] : 1.0;
+                                X[(int64_t)(c.k[p] & kKeyRowMask) * G + g] = xr[i] + d * x;
+                            }
+                        }
+                    } else {
+                        const bool has_rows = (m.fmt == F_SPARSE || m.fmt == F_INDICATOR);
+                        const bool has_vals = (m.fmt == F_SPARSE || m.fmt == F_DENSE);
+                        for (int64_t p = sl; p < n; p += S) {
+                            const int64_t k = has_rows ? (int64_t)__ldg(P.rows + m.cb + p) : m.cb + p;
+                            const double x = has_vals ? __ldg(P.vals + m.vb + p) : 1.0;
+                            X[k * G + g] += d * x;
+                        }
+                    }
+                }
+                if (threadIdx.x == 0 && j + kAhead + 1 < J) s_meta[(j + kAhead + 1) & (kRing - 1)] = I.cook(nm);
+                if (tr) tr[6 * j + 4] = clock64();
+                cp_async_wait_but_last();
+                if (__syncthreads_or(late)) {
+                    late = true;
+                    break;
+                }
+                if (tr) tr[6 * j + 5] = clock64();
+            }
+            cp_async_wait_all();
+            if (late) break;
+
+            if (active) ++iteration;
+            const double cur = inst_objective<MODEL, G>(P, I, active, need_ll, ll, s_red4, rb4, s_xch4, xb4);
+            if (active) inst_converge(P, cur, last, iteration, flag, active);
         }
-        return;
-    }
-    inst_finish<MODEL, G>(P, I, flag, iteration, last, cnt, s_red4, rb4, s_xch4, xb4);
+        if (late) {  // a wait for the other CTAs' sums ran out: report, no more cluster barriers
+            if (I.exists && I.sl == 0 && I.rank == 0) {
+                BatchResult r{};
+                r.flag = kBatchTimeoutFlag;
+                P.results[I.inst] = r;
+            }
+            return;
+        }
+        inst_finish<MODEL, G>(P, I, flag, iteration, last, cnt, s_red4, rb4, s_xch4, xb4);
+        __syncthreads();
+    }  // next group
 }
 
 __global__ void batch_keys_kernel(const int32_t* rows, int64_t nnz, const int32_t* fold, int32_t* keys) {
@@ -269,6 +294,12 @@ cudaError_t launch_g(const BatchParams& P, cudaStream_t stream) {
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
+    // as many clusters as can be resident at once (they take groups from the queue)
+    int resident = 0;
+    e = cudaOccupancyMaxActiveClusters(&resident, fn, &cfg);
+    if (e != cudaSuccess) return e;
+    if (resident < 1) return cudaErrorInvalidConfiguration;
+    cfg.gridDim = dim3(std::min(n_groups, resident) * C);
     return cudaLaunchKernelEx(&cfg, fn, P);
 }
 
