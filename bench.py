@@ -173,8 +173,8 @@ def read_traffic(workload_name: str):
             for line in fh:
                 if line.strip().startswith("traffic_bytes_per_sweep:"):
                     return float(line.split(":", 1)[1].split()[0])
-    except OSError:
-        pass
+    except (OSError, ValueError, IndexError):
+        pass  # not captured yet: traffic is reported as null
     return None
 
 
