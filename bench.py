@@ -235,13 +235,21 @@ def dist_setup():
 
 
 def allreduce(vals, op, world):
+    """All-reduce a few floats over the ranks (NCCL on GPUs, gloo on CPU)."""
     if world == 1:
         return vals
     import torch
     import torch.distributed as dist
-    t = torch.tensor(vals, dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor(vals, dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=op)
     return t.tolist()
+
+
+def cv_shard(n: int, world: int, rank: int) -> np.ndarray:
+    """Instances of a cross-validation grid fitted by `rank`: round robin over the
+    grid, so that every rank gets a share of the weak priors (the longest fits)."""
+    return np.arange(rank, n, world)
 
 
 def cpu_reference_sample(d, target_s: float = 15.0):
@@ -451,8 +459,17 @@ def cv_bytes(d, res) -> float:
 
 def run_cv(args, world, rank, local):
     import torch
+    import torch.distributed as tdist
+    if world > 1:  # instances shard over the ranks; no data-path collective
+        import datetime
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     from ccd_b200 import native
     d, fold, hold, var = cv_workload(args.small, args.cv_columns)
+    n_grid = len(var)
+    if world > 1:
+        mine = cv_shard(n_grid, world, rank)
+        hold, var = hold[mine], var[mine]
     mixed = args.precision == "mixed"
     prec = native.PRECISION_MIXED if mixed else native.PRECISION_FP64
     ctx = native.Context(local)
@@ -465,6 +482,9 @@ def run_cv(args, world, rank, local):
     for _ in range(args.warmup):
         grid(f)
     clocks = Clocks(local)
+    if world > 1:
+        tdist.barrier()
+    torch.cuda.synchronize()
     clocks.start()
     t, fits, res_all, beta_all = 0.0, 0, None, None
     for _ in range(args.steps):
@@ -474,7 +494,16 @@ def run_cv(args, world, rank, local):
         t += secs
         fits += len(var)
         res_all, beta_all = res, beta
+    if world > 1:
+        tdist.barrier()
     clk = clocks.stop()
+    # whole job: every rank's fits over the slowest rank's device time
+    t = allreduce([t], tdist.ReduceOp.MAX if world > 1 else None, world)[0]
+    fits = int(allreduce([float(fits)], tdist.ReduceOp.SUM if world > 1 else None, world)[0])
+    if world > 1 and rank != 0:
+        tdist.barrier()
+        tdist.destroy_process_group()
+        return
     # end to end through the C ABI from host buffers: matrix upload, fit, coefficients back
     e2e_t = 0.0
     h2d = d.rows.nbytes + d.vals.nbytes + d.col_start.nbytes + d.val_start.nbytes + d.fmt.nbytes \
@@ -523,9 +552,9 @@ def run_cv(args, world, rank, local):
     sweeps = [r["iterations"] for r in res_all]
     kernel = "batch_mixed_kernel<LOGISTIC>" if mixed else "batch_sweep_kernel<LOGISTIC>"
     line = {
-        "metric": "converged fits/s", "value": fits / t, "unit": "fits/s", "n_gpus": 1,
+        "metric": "converged fits/s", "value": fits / t, "unit": "fits/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "higher_is_better": True, "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
         "dtype": "f32/f64 (f32 exp, ratios, per-entry terms; f64 state, reductions, step)" if mixed else "f64",
         "data": "synthetic (seeded PCG64, workload shapes of the benchmark config)",
         "config": {"workload": "cv_grid" + ("_small" if args.small else "")
@@ -534,9 +563,10 @@ def run_cv(args, world, rank, local):
                    "folds": 10, "variances": "20 log-uniform in [1e-4, 1] (Laplace)",
                    "convergence": "gradient, tol 1e-6", "start": "cold (beta = 0) per instance",
                    "precision": args.precision, "group": args.group or "engine's choice",
+                   "parallelism": f"instances round-robin over {world} GPUs" if world > 1 else "1 GPU",
                    "step": "one grid of 200 fits to convergence",
                    "l2": "flushed between timed steps (512 MiB device write)"},
-        "e2e": {"value": fits / e2e_t, "unit": "fits/s", "h2d_bytes_per_step": int(h2d),
+        "e2e": {"value": world * len(var) * args.steps / e2e_t, "unit": "fits/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "plain_fits_per_s": plain_n / plain_t if plain_n else None,
         "batched_over_plain": (fits / t) / (plain_n / plain_t) if plain_n else None,
@@ -552,6 +582,9 @@ def run_cv(args, world, rank, local):
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
+    if world > 1:
+        tdist.barrier()
+        tdist.destroy_process_group()
 
 
 def cv_cpu_sample(d, fold, hold, var, res):
