@@ -25,6 +25,7 @@ the same workload per step.
 from __future__ import annotations
 
 import argparse
+import collections
 import json
 import os
 import subprocess
@@ -54,7 +55,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--max-sweeps", type=int, default=1000,
                     help="cap on sweeps per findMode (profiling captures of one short launch)")
-    ap.add_argument("--workload", choices=["poisson_offset", "cv_grid", "cox_breslow"],
+    ap.add_argument("--serve-requests", type=int, default=200,
+                    help="serve: requests in the replayed stream")
+    ap.add_argument("--serve-slots", type=int, default=8, help="serve: concurrent fits")
+    ap.add_argument("--workload", choices=["poisson_offset", "cv_grid", "cox_breslow", "serve"],
                     default="poisson_offset",
                     help="poisson_offset: plain fits (default); cv_grid: 10 folds x 20 Laplace "
                          "variances = 200 logistic fits over one shared 5e5 x 2e4 matrix")
@@ -608,6 +612,96 @@ def cv_cpu_sample(d, fold, hold, var, res):
                       f"x {mean_sweeps:.1f} mean sweeps per fit of this grid, single thread"}
 
 
+SERVE_RANGES = dict(rate=50.0, K_range=(1e3, 1e5), J_range=(1e2, 1e4), density_range=(0.001, 0.02))
+
+
+def run_serve(args, world, rank, local):
+    """The served stream: Poisson(50/s) arrivals of independent logistic /
+    conditional logistic / Cox fits, replayed in real time into the server."""
+    import torch
+    from ccd_b200 import native, serve
+    if world > 1 and rank != 0:
+        return  # one server per GPU box; replicas add nothing to a latency figure
+    stream = synthetic.serving_stream(args.serve_requests, seed=11, **SERVE_RANGES)
+    warm = synthetic.serving_stream(max(4, args.serve_slots), seed=12, rate=1e3, K_range=(1e3, 3e3),
+                                    J_range=(50, 200))
+    srv = serve.Server(device=local, hbm_budget=150e9, slots=args.serve_slots)
+    try:
+        for _ in range(args.warmup):
+            srv.done.clear()
+            serve.replay(srv, warm)
+        clocks = Clocks(local)
+        torch.cuda.synchronize()
+        clocks.start()
+        summaries = []
+        for _ in range(args.steps):
+            srv.done.clear()
+            done = serve.replay(srv, stream)
+            summaries.append(serve.latency_summary(done))
+        clk = clocks.stop()
+        peak = srv.peak_running
+    finally:
+        srv.close()
+    s = summaries[-1]
+    kinds = collections.Counter(int(d.model_type) for _, d in stream)
+    h2d = sum(d.rows.nbytes + d.vals.nbytes + d.col_start.nbytes + d.val_start.nbytes + d.y.nbytes
+              + (d.time.nbytes if d.time is not None else 0) + (d.stratum.nbytes if d.stratum is not None else 0)
+              for _, d in stream)
+    d2h = sum(8 * d.J for _, d in stream)
+    cpu = None if args.no_cpu_baseline else serve_cpu_sample(stream)
+    line = {
+        "metric": "p50 fit latency", "value": s["p50_s"], "unit": "s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * s["makespan_s"], "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded PCG64 problems and arrival trace)",
+        "config": {"workload": "serve", "requests": len(stream), "arrivals": "Poisson, 50/s",
+                   "mix": {str(k): v for k, v in sorted(kinds.items())},
+                   "K": "log-uniform 1e3..1e5", "J": "log-uniform 1e2..1e4",
+                   "density": "uniform 0.001..0.02", "prior": "Laplace, variance 0.1",
+                   "slots": args.serve_slots, "hbm_budget_bytes": 150e9,
+                   "step": "replay of the whole stream; latency = completion - arrival",
+                   "strategy": "speculative batches (ordinary launches, fits interleave on streams)"},
+        "p99_s": s["p99_s"], "mean_s": s["mean_s"], "fits_per_s": s["fits_per_s"],
+        "failed": s["failed"], "peak_concurrent_fits": peak,
+        "e2e": {"value": s["p50_s"], "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "roofline": None, "cpu_baseline": cpu, "gpu_launches": None, "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def serve_cpu_sample(stream, n: int = 40):
+    """The reference CPU engine serving the first n requests of the same trace:
+    FIFO over a pool of all host cores, each fit single-threaded, replayed at
+    the trace's arrival times."""
+    import concurrent.futures as cf
+    from oracle import checker
+    eng_cls = checker.best_engine()
+    kind = "reference" if eng_cls is checker.ReferenceEngine else "port"
+    sub = stream[:n]
+    cores = os.cpu_count() or 1
+
+    def one(d):
+        e = eng_cls(d)
+        try:
+            e.fit(GRADIENT, 1e-6, 1000)
+        finally:
+            e.close()
+        return time.perf_counter()
+
+    t0 = time.perf_counter()
+    futs = []
+    with cf.ThreadPoolExecutor(max_workers=cores) as ex:
+        for t_arr, d in sub:
+            delay = t0 + t_arr - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            futs.append((t0 + t_arr, ex.submit(one, d)))
+        lat = np.array([f.result() - a for a, f in futs])
+    return {"value": float(np.percentile(lat, 50)), "unit": "s", "cores": cores, "kind": kind,
+            "p99_s": float(np.percentile(lat, 99)),
+            "sample": f"first {len(sub)} requests of the same trace, FIFO over {cores} host threads"}
+
+
 def main():
     global WORKLOAD
     args = parse()
@@ -617,6 +711,8 @@ def main():
         run_reference(args, world, rank)
     elif args.workload == "cv_grid":
         run_cv(args, world, rank, local)
+    elif args.workload == "serve":
+        run_serve(args, world, rank, local)
     else:
         run_ours(args, world, rank, local)
 

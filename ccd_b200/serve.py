@@ -1,0 +1,188 @@
+"""Serving: a request loop over independent fits with continuous batching.
+
+Requests (a problem and its mode-finding arguments) arrive over time.  A
+fixed set of slots -- host threads, each with its own engine context and so
+its own CUDA stream -- takes requests in arrival order as soon as a slot is
+free and the request's device-memory estimate fits the HBM budget next to the
+fits already running; a request that arrives while others are on the GPU is
+admitted the moment a slot and memory free up, and its kernels overlap theirs
+on the device.  A fit runs exactly as it would alone (same engine, same
+kernels, same arithmetic: its result does not depend on its neighbours); the
+server only decides when it starts.
+
+Fits run with the speculative-batch sweep strategy: its kernels are ordinary
+launches, so fits on different streams interleave freely (the dependency-level
+strategy's persistent kernel would hold every SM for the length of a sweep).
+
+The reference has no serving layer; this loop drives the same C ABI entry
+point a single fit uses (ccdb_fit_model: upload, findMode, coefficients back).
+"""
+from __future__ import annotations
+
+import collections
+import threading
+import time
+from dataclasses import dataclass
+from typing import Callable, List, Optional
+
+import numpy as np
+
+from .data import CyclopsData
+
+
+@dataclass
+class Request:
+    rid: int
+    data: CyclopsData
+    args: object = None          # native.ModeFindingArguments (None: defaults, speculative sweeps)
+    bytes: int = 0               # device-memory estimate used for admission
+    arrival: float = 0.0         # time.perf_counter() at submission
+
+
+@dataclass
+class Completed:
+    rid: int
+    beta: np.ndarray
+    flag: int
+    iterations: int
+    loglik: float
+    arrival: float
+    start: float
+    end: float
+    slot: int
+    error: Optional[str] = None
+
+    @property
+    def latency(self) -> float:
+        return self.end - self.arrival
+
+
+def estimate_bytes(d: CyclopsData) -> int:
+    """Upper estimate of a fit's device memory: the matrix (CSC and the CSR copy
+    a warm start may build), the per-row state, per-column state and, for Cox,
+    the risk-set tables; twice that for allocator slack and a fixed 64 MiB."""
+    nnz, nv = int(d.nnz), int(d.vals.size)
+    core = 12 * nnz + 8 * nv + 16 * (d.J + 1) + 96 * d.K + 96 * d.J
+    if d.time is not None:
+        core += 120 * d.K
+    return 2 * core + (64 << 20)
+
+
+class Server:
+    """`slots` concurrent fits under an HBM budget of `hbm_budget` bytes.
+
+    ``fit_fn(slot, request, slot_state) -> (beta, flag, iterations, loglik)``
+    runs one fit (`slot_state` is the slot thread's own attribute holder); the
+    default runs it on the GPU through the slot's own context.  Tests of the
+    admission logic pass a stand-in that needs no GPU.
+    """
+
+    def __init__(self, device: int = 0, hbm_budget: float = 150e9, slots: int = 8,
+                 fit_fn: Optional[Callable] = None):
+        self.device = device
+        self.budget = int(hbm_budget)
+        self.n_slots = slots
+        self._fit_fn = fit_fn or self._gpu_fit
+        self._cv = threading.Condition()
+        self._pending: collections.deque = collections.deque()
+        self._reserved = 0
+        self._running = 0
+        self._stop = False
+        self.peak_reserved = 0
+        self.peak_running = 0
+        self.done: List[Completed] = []
+        self._threads = [threading.Thread(target=self._worker, args=(i,), daemon=True) for i in range(slots)]
+        for t in self._threads:
+            t.start()
+
+    # -- submission and shutdown
+    def submit(self, req: Request) -> None:
+        if not req.bytes:
+            req.bytes = estimate_bytes(req.data)
+        if req.bytes > self.budget:
+            raise ValueError(f"request {req.rid} needs ~{req.bytes} bytes, above the HBM budget {self.budget}")
+        req.arrival = time.perf_counter()
+        with self._cv:
+            self._pending.append(req)
+            self._cv.notify_all()
+
+    def drain(self, n_expected: int, timeout: float = 3600.0) -> List[Completed]:
+        """Wait until n_expected requests have completed."""
+        t_end = time.perf_counter() + timeout
+        with self._cv:
+            while len(self.done) < n_expected:
+                left = t_end - time.perf_counter()
+                if left <= 0:
+                    raise TimeoutError(f"{len(self.done)} of {n_expected} requests completed")
+                self._cv.wait(min(left, 1.0))
+            return list(self.done)
+
+    def close(self) -> None:
+        with self._cv:
+            self._stop = True
+            self._cv.notify_all()
+        for t in self._threads:
+            t.join()
+
+    # -- the slots
+    def _worker(self, slot: int) -> None:
+        local = threading.local()
+        while True:
+            with self._cv:
+                while True:
+                    if self._pending and self._reserved + self._pending[0].bytes <= self.budget:
+                        break  # the oldest request fits: admit it (arrival order, no overtaking)
+                    if self._stop and not self._pending:
+                        ctx = getattr(local, "ctx", None)
+                        if ctx is not None:
+                            ctx.close()
+                        return
+                    self._cv.wait()
+                req = self._pending.popleft()
+                self._reserved += req.bytes
+                self._running += 1
+                self.peak_reserved = max(self.peak_reserved, self._reserved)
+                self.peak_running = max(self.peak_running, self._running)
+            start = time.perf_counter()
+            beta, flag, iters, ll, err = None, -1, 0, float("nan"), None
+            try:
+                beta, flag, iters, ll = self._fit_fn(slot, req, local)
+            except Exception as e:  # the request fails, the server keeps serving
+                err = f"{type(e).__name__}: {e}"
+            end = time.perf_counter()
+            with self._cv:
+                self._reserved -= req.bytes
+                self._running -= 1
+                self.done.append(Completed(req.rid, beta, flag, iters, ll, req.arrival, start, end, slot, err))
+                self._cv.notify_all()
+
+    def _gpu_fit(self, slot: int, req: Request, local):
+        from . import native
+        if not hasattr(local, "ctx"):
+            local.ctx = native.Context(self.device)
+        args = req.args or native.ModeFindingArguments(strategy=native.SWEEP_SPECULATIVE)
+        r = native.fit_model(local.ctx, req.data, args)
+        return r.beta, r.return_flag, r.iterations, r.log_likelihood
+
+
+def replay(server: Server, stream, args=None, time_scale: float = 1.0) -> List[Completed]:
+    """Submit [(arrival seconds, CyclopsData)] at their arrival times and wait for
+    every result.  Returns the completions in request order."""
+    t0 = time.perf_counter()
+    for i, (t_arr, d) in enumerate(stream):
+        delay = t0 + t_arr * time_scale - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        server.submit(Request(i, d, args))
+    done = server.drain(len(stream))
+    return sorted(done, key=lambda c: c.rid)
+
+
+def latency_summary(done: List[Completed]) -> dict:
+    lat = np.array([c.latency for c in done])
+    first = min(c.arrival for c in done)
+    last = max(c.end for c in done)
+    return {"requests": len(done), "failed": sum(c.error is not None for c in done),
+            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "mean_s": float(lat.mean()), "fits_per_s": len(done) / (last - first),
+            "makespan_s": last - first}

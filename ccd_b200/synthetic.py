@@ -340,3 +340,35 @@ def cv_grid(n_folds: int = 10, n_vars: int = 20, lower: float = 1e-4, upper: flo
     hold = np.repeat(np.arange(n_folds, dtype=np.int32), n_vars)
     var = np.tile(grid, n_folds)
     return hold, var
+
+
+def serving_stream(n_requests: int = 200, seed: int = 11, rate: float = 50.0,
+                   K_range=(1e3, 1e5), J_range=(1e2, 1e4), density_range=(0.001, 0.02),
+                   variance: float = 0.1):
+    """A served stream of independent fits: Poisson(rate) arrivals; each request
+    an independently seeded problem, 50 % logistic, 30 % conditional logistic
+    (one case : 1-10 controls per matched set), 20 % Breslow Cox; K and J
+    log-uniform over the given ranges, indicator density uniform, 10-200 true
+    coefficients, Laplace prior of the given variance on every covariate.
+    Returns [(arrival seconds, CyclopsData)] in arrival order."""
+    rng = _rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=n_requests))
+    out = []
+    for i in range(n_requests):
+        u = rng.random()
+        K = int(round(np.exp(rng.uniform(np.log(K_range[0]), np.log(K_range[1])))))
+        J = int(round(np.exp(rng.uniform(np.log(J_range[0]), np.log(J_range[1])))))
+        dens = float(rng.uniform(*density_range))
+        n_true = int(rng.integers(10, 201))
+        s = int(rng.integers(1, 2 ** 31 - 1))
+        if u < 0.5:
+            d = logistic_l1(seed=s, K=K, P=J, density=dens, n_true=n_true, intercept=-2.0, variance=variance)
+        elif u < 0.8:
+            d = conditional_logistic(seed=s, n_sets=max(1, int(round(K / 6.5))), P=J, density=dens,
+                                     n_true=n_true, variance=variance)
+        else:
+            d = cox_breslow(seed=s, K=K, n_strata=max(1, K // 1000), P=J, density=dens, n_true=n_true,
+                            variance=variance)
+        d.meta = dict(d.meta, request=i)
+        out.append((float(t[i]), d))
+    return out

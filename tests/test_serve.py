@@ -1,0 +1,97 @@
+"""Host logic of the serving loop (admission under the HBM budget, arrival
+order, failures), with a stand-in fit that needs no GPU."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from ccd_b200 import serve, synthetic
+from ccd_b200.data import MODEL_LOGISTIC
+
+
+def _stub(duration=0.02, fail_on=()):
+    lock = threading.Lock()
+    live = {"now": 0, "peak": 0}
+
+    def fit(slot, req, local):
+        with lock:
+            live["now"] += 1
+            live["peak"] = max(live["peak"], live["now"])
+        time.sleep(duration)
+        with lock:
+            live["now"] -= 1
+        if req.rid in fail_on:
+            raise RuntimeError("planted failure")
+        return np.full(3, float(req.rid)), 0, 1, -1.0
+    return fit, live
+
+
+def _req(i, nbytes):
+    d = synthetic.small(MODEL_LOGISTIC, seed=i, K=50, P=3)
+    return serve.Request(i, d, bytes=nbytes)
+
+
+def test_budget_bounds_concurrency_and_order_is_kept():
+    fit, live = _stub()
+    srv = serve.Server(hbm_budget=300, slots=8, fit_fn=fit)
+    try:
+        for i in range(12):
+            srv.submit(_req(i, 100))  # three fit in the budget at a time
+        done = srv.drain(12, timeout=30)
+    finally:
+        srv.close()
+    assert len(done) == 12 and all(c.error is None for c in done)
+    assert srv.peak_reserved <= 300 and live["peak"] <= 3 and srv.peak_running <= 3
+    starts = [c.start for c in sorted(done, key=lambda c: c.rid)]
+    assert starts == sorted(starts)  # admitted in arrival order
+    assert all(np.array_equal(c.beta, np.full(3, float(c.rid))) for c in done)
+
+
+def test_slots_bound_concurrency():
+    fit, live = _stub()
+    srv = serve.Server(hbm_budget=1 << 40, slots=2, fit_fn=fit)
+    try:
+        for i in range(6):
+            srv.submit(_req(i, 10))
+        srv.drain(6, timeout=30)
+    finally:
+        srv.close()
+    assert live["peak"] <= 2
+
+
+def test_failed_fit_is_reported_and_serving_continues():
+    fit, _ = _stub(fail_on={1})
+    srv = serve.Server(hbm_budget=1 << 40, slots=2, fit_fn=fit)
+    try:
+        for i in range(4):
+            srv.submit(_req(i, 10))
+        done = {c.rid: c for c in srv.drain(4, timeout=30)}
+    finally:
+        srv.close()
+    assert "planted failure" in done[1].error
+    assert all(done[i].error is None for i in (0, 2, 3))
+
+
+def test_request_above_budget_is_refused():
+    fit, _ = _stub()
+    srv = serve.Server(hbm_budget=100, slots=1, fit_fn=fit)
+    try:
+        with pytest.raises(ValueError):
+            srv.submit(_req(0, 101))
+    finally:
+        srv.close()
+
+
+def test_latency_summary_and_stream_shape():
+    stream = synthetic.serving_stream(12, seed=4, K_range=(1e3, 2e3), J_range=(20, 50))
+    arrivals = [t for t, _ in stream]
+    assert arrivals == sorted(arrivals)
+    fit, _ = _stub(0.001)
+    srv = serve.Server(hbm_budget=1 << 40, slots=3, fit_fn=fit)
+    try:
+        done = serve.replay(srv, stream, time_scale=0.01)
+    finally:
+        srv.close()
+    s = serve.latency_summary(done)
+    assert s["requests"] == 12 and s["failed"] == 0 and s["p99_s"] >= s["p50_s"] > 0
