@@ -638,6 +638,14 @@ def run_serve(args, world, rank, local):
             srv.done.clear()
             done = serve.replay(srv, stream)
             summaries.append(serve.latency_summary(done))
+        # service time (start to end) per model type: where the GPU time goes
+        svc = collections.defaultdict(list)
+        for c in done:
+            svc[int(stream[c.rid][1].model_type)].append(c.end - c.start)
+        service = {str(k): {"n": len(v), "median_s": float(np.median(v)), "max_s": float(np.max(v))}
+                   for k, v in sorted(svc.items())}
+        errors = collections.Counter(
+            f"model {int(stream[c.rid][1].model_type)}: {c.error[:160]}" for c in done if c.error)
         clk = clocks.stop()
         peak = srv.peak_running
     finally:
@@ -662,7 +670,8 @@ def run_serve(args, world, rank, local):
                    "step": "replay of the whole stream; latency = completion - arrival",
                    "strategy": "speculative batches (ordinary launches, fits interleave on streams)"},
         "p99_s": s["p99_s"], "mean_s": s["mean_s"], "fits_per_s": s["fits_per_s"],
-        "failed": s["failed"], "peak_concurrent_fits": peak,
+        "failed": s["failed"], "errors": dict(errors.most_common(5)), "peak_concurrent_fits": peak,
+        "service_by_model": service,
         "e2e": {"value": s["p50_s"], "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "roofline": None, "cpu_baseline": cpu, "gpu_launches": None, "clocks": clk,
     }

@@ -45,12 +45,15 @@ void* Context::alloc(size_t bytes) {
                                              " bytes exceeds the HBM budget");
         in_use += bytes;
     }
+    // stream-ordered: allocation and release are ordered with the context's own
+    // work and do not synchronize the device, so fits of other contexts (other
+    // streams) keep running through them
     void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, bytes);
+    cudaError_t e = cudaMallocAsync(&p, bytes, stream);
     if (e != cudaSuccess) {
         std::lock_guard<std::mutex> g(mu);
         in_use -= bytes;
-        check_cuda(e, "cudaMalloc");
+        check_cuda(e, "cudaMallocAsync");
     }
     std::lock_guard<std::mutex> g(mu);
     sizes[p] = bytes;
@@ -59,7 +62,7 @@ void* Context::alloc(size_t bytes) {
 
 void Context::release(void* p) {
     if (!p) return;
-    cudaFree(p);
+    cudaFreeAsync(p, stream);
     std::lock_guard<std::mutex> g(mu);
     auto it = sizes.find(p);
     if (it != sizes.end()) {
