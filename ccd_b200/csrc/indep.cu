@@ -408,15 +408,15 @@ __global__ void __launch_bounds__(kThreads, 1) indep_sweep_kernel(IndepParams P)
 
             // ---- wait for the previous level
             if (P.trace && it == 0 && tid == 0) P.trace[3 * si] = global_ns();
-            if (sg.level > 0) {
-                if (tid == 0) {
-                    const unsigned target = (unsigned)(it + 1) * (unsigned)P.level_need[sg.level - 1];
-                    s_fail = wait_geq(P.level_done + sg.level - 1, target, P.wait_limit_ns, P.st,
-                                      E_WAIT_LEVEL, sg.level) ? 0 : 1;
-                }
-                __syncthreads();
-                if (s_fail) return;
+            if (sg.level > 0 && tid == 0) {
+                const unsigned target = (unsigned)(it + 1) * (unsigned)P.level_need[sg.level - 1];
+                s_fail = wait_geq(P.level_done + sg.level - 1, target, P.wait_limit_ns, P.st,
+                                  E_WAIT_LEVEL, sg.level) ? 0 : 1;
             }
+            // every segment, level 0 included: the metadata staged above by thread 0
+            // (s_meta) and by each warp's lane 0 is read by all threads below
+            __syncthreads();
+            if (sg.level > 0 && s_fail) return;
 
             if (P.trace && it == 0 && tid == 0) P.trace[3 * si + 1] = global_ns();
             // ---- phase 1: CTA-level tasks (split-column partials are published, not awaited)

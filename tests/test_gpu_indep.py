@@ -100,3 +100,22 @@ def test_fused_is_deterministic(gpu_ctx):
     r2 = native.fit_model(gpu_ctx, d)
     assert np.array_equal(r1.beta, r2.beta)
     assert r1.log_likelihood == r2.log_likelihood
+
+
+@pytest.mark.parametrize("model,kw", [
+    (MODEL_POISSON, dict(offset=True, prior=PRIOR_NORMAL)),
+    (MODEL_LOGISTIC, dict()),
+])
+def test_split_columns_beyond_the_stage(gpu_ctx, oracle_engine, model, kw):
+    """700,000 rows: the intercept splits over every CTA in chunks longer than a
+    CTA stages, so its gradient takes the streaming path -- on the first
+    dependency level, where the staged column metadata must be published to all
+    threads before the level starts."""
+    d = synthetic.small(model, seed=5, K=700_000, P=3, density=0.001, formats=("indicator",), **kw)
+    m = native.Matrix(gpu_ctx, d)
+    f = native.Fit(gpu_ctx, m, d)
+    r = f.find_mode(native.ModeFindingArguments(convergence_type=GRADIENT, strategy=native.SWEEP_LEVELS))
+    want = oracle_engine(d).fit(GRADIENT, 1e-6)
+    assert r.return_flag == want["flag"] and r.iterations == want["iterations"]
+    assert rel_beta(r.beta, want["beta"]) <= BETA_TOL
+    assert abs(r.log_likelihood - want["loglik"]) <= LL_TOL * abs(want["loglik"])
