@@ -668,7 +668,8 @@ def run_serve(args, world, rank, local):
                    "density": "uniform 0.001..0.02", "prior": "Laplace, variance 0.1",
                    "slots": args.serve_slots, "hbm_budget_bytes": 150e9,
                    "step": "replay of the whole stream; latency = completion - arrival",
-                   "strategy": "speculative batches (ordinary launches, fits interleave on streams)"},
+                   "strategy": "logistic: dependency-level sweeps on the slot's share of the SMs; "
+                               "grouped models: their engines"},
         "p99_s": s["p99_s"], "mean_s": s["mean_s"], "fits_per_s": s["fits_per_s"],
         "failed": s["failed"], "errors": dict(errors.most_common(5)), "peak_concurrent_fits": peak,
         "service_by_model": service,

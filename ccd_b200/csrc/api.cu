@@ -286,6 +286,7 @@ void Fit::ensure_schedule() {
     if (bps < 1) throw Error(CCDB_ERR_CUDA, "sweep kernel does not fit on an SM");
     ScheduleParams sp;
     sp.n_cta = ctx->n_sm * std::min(bps, 1);
+    if (ctx->max_ctas > 0) sp.n_cta = std::min(sp.n_cta, ctx->max_ctas);
     sp.warps_per_cta = indep_threads() / 32;
     std::vector<int64_t> entries(J);
     for (int j = 0; j < J; ++j) entries[j] = m->entries(j);
@@ -751,6 +752,21 @@ int ccdb_context_destroy(ccdb_context* ctx) {
         cudaEventDestroy(ctx->ev_b);
         cudaStreamDestroy(ctx->stream);
         delete ctx;
+    });
+}
+
+int ccdb_context_sm_count(const ccdb_context* ctx, int32_t* n_sm) {
+    return guard([&] {
+        require(ctx && n_sm, "NULL argument");
+        *n_sm = ctx->n_sm;
+    });
+}
+
+int ccdb_context_set_max_ctas(ccdb_context* ctx, int32_t max_ctas) {
+    return guard([&] {
+        require(ctx != nullptr, "NULL context");
+        require(max_ctas >= 0, "max_ctas must be >= 0");
+        ctx->max_ctas = max_ctas;
     });
 }
 

@@ -24,6 +24,7 @@ void check_cuda(cudaError_t e, const char* what);
 struct Context {
     int device = 0;
     int n_sm = 0;
+    int max_ctas = 0;  // persistent sweep grids: at most this many CTAs (0: n_sm)
     size_t budget = 0;
     size_t in_use = 0;
     cudaStream_t stream = nullptr;

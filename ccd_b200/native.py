@@ -105,6 +105,8 @@ def lib() -> C.CDLL:
         L.ccdb_context_create.argtypes = [C.c_int, C.c_size_t, C.POINTER(_P)]
         L.ccdb_context_destroy.argtypes = [_P]
         L.ccdb_context_memory.argtypes = [_P, C.POINTER(C.c_size_t)]
+        L.ccdb_context_sm_count.argtypes = [_P, C.POINTER(C.c_int32)]
+        L.ccdb_context_set_max_ctas.argtypes = [_P, C.c_int32]
         L.ccdb_matrix_create.argtypes = [_P, C.c_int64, C.c_int32, _P, _P, _P, _P, _P, C.POINTER(_P)]
         L.ccdb_matrix_destroy.argtypes = [_P]
         L.ccdb_fit_create.argtypes = [_P, _P, C.POINTER(_FitDesc), C.POINTER(_P)]
@@ -153,6 +155,16 @@ class Context:
         # matrices and fits made on this context: closed before it, whatever
         # order the interpreter releases the Python objects in
         self._children = weakref.WeakSet()
+
+    @property
+    def sm_count(self) -> int:
+        v = C.c_int32()
+        _check(lib().ccdb_context_sm_count(self.h, C.byref(v)))
+        return v.value
+
+    def set_max_ctas(self, max_ctas: int) -> None:
+        """Persistent sweep grids of this context's fits use at most max_ctas CTAs."""
+        _check(lib().ccdb_context_set_max_ctas(self.h, int(max_ctas)))
 
     def memory_in_use(self) -> int:
         v = C.c_size_t()

@@ -10,9 +10,11 @@ on the device.  A fit runs exactly as it would alone (same engine, same
 kernels, same arithmetic: its result does not depend on its neighbours); the
 server only decides when it starts.
 
-Fits run with the speculative-batch sweep strategy: its kernels are ordinary
-launches, so fits on different streams interleave freely (the dependency-level
-strategy's persistent kernel would hold every SM for the length of a sweep).
+Each slot's context limits its persistent sweep grids to its share of the SMs
+(SM count / slots), so the slots' sweep kernels can all be resident at once
+and run side by side; logistic and Poisson fits use the dependency-level sweep
+(one persistent launch per findMode), grouped models (conditional logistic,
+Cox) their own engines.
 
 The reference has no serving layer; this loop drives the same C ABI entry
 point a single fit uses (ccdb_fit_model: upload, findMode, coefficients back).
@@ -160,7 +162,8 @@ class Server:
         from . import native
         if not hasattr(local, "ctx"):
             local.ctx = native.Context(self.device)
-        args = req.args or native.ModeFindingArguments(strategy=native.SWEEP_SPECULATIVE)
+            local.ctx.set_max_ctas(max(1, local.ctx.sm_count // self.n_slots))
+        args = req.args or native.ModeFindingArguments(strategy=native.SWEEP_LEVELS)
         r = native.fit_model(local.ctx, req.data, args)
         return r.beta, r.return_flag, r.iterations, r.log_likelihood
 

@@ -57,6 +57,16 @@ int ccdb_context_destroy(ccdb_context* ctx);
 /* Bytes of device memory currently held by matrices and fits of ctx. */
 int ccdb_context_memory(const ccdb_context* ctx, size_t* bytes_in_use);
 
+/* Streaming multiprocessors of the context's GPU.  No reference counterpart. */
+int ccdb_context_sm_count(const ccdb_context* ctx, int32_t* n_sm);
+
+/* Persistent sweep kernels launched by this context's fits use at most
+ * max_ctas CTAs (0: one per SM, the default).  Contexts that run fits at the
+ * same time on one GPU (the serving loop's slots) split the SMs between them
+ * so that every persistent grid can be resident at once.  No reference
+ * counterpart (the reference runs one fit per thread on the CPU). */
+int ccdb_context_set_max_ctas(ccdb_context* ctx, int32_t max_ctas);
+
 /* Upload a column-major CompressedDataMatrix (CompressedDataMatrix.h:40-452).
  * col_start[J+1] offsets into rows[] (SPARSE/INDICATOR entries, row ids ascending);
  * val_start[J+1] offsets into vals[] (SPARSE: one per entry; DENSE: K values);

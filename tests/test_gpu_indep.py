@@ -119,3 +119,26 @@ def test_split_columns_beyond_the_stage(gpu_ctx, oracle_engine, model, kw):
     assert r.return_flag == want["flag"] and r.iterations == want["iterations"]
     assert rel_beta(r.beta, want["beta"]) <= BETA_TOL
     assert abs(r.log_likelihood - want["loglik"]) <= LL_TOL * abs(want["loglik"])
+
+
+@pytest.mark.parametrize("max_ctas", [3, 18])
+def test_find_mode_on_a_share_of_the_sms(oracle_engine, max_ctas):
+    """A context limited to a few CTAs (the serving loop's slots) builds its
+    sweep schedule for that grid: longer chunks, more split columns per CTA."""
+    ctx = native.Context(0)
+    try:
+        ctx.set_max_ctas(max_ctas)
+        for d in (synthetic.small(MODEL_POISSON, seed=6, K=120_000, P=8, density=0.01, offset=True,
+                                  prior=PRIOR_NORMAL, formats=("indicator", "sparse")),
+                  synthetic.logistic_l1(seed=7, K=20_000, P=400)):
+            m = native.Matrix(ctx, d)
+            f = native.Fit(ctx, m, d)
+            r = f.find_mode(native.ModeFindingArguments(strategy=native.SWEEP_LEVELS))
+            want = oracle_engine(d).fit(GRADIENT, 1e-6)
+            assert r.return_flag == want["flag"] and r.iterations == want["iterations"]
+            assert rel_beta(r.beta, want["beta"]) <= BETA_TOL
+            assert abs(r.log_likelihood - want["loglik"]) <= LL_TOL * abs(want["loglik"])
+            f.close()
+            m.close()
+    finally:
+        ctx.close()

@@ -17,10 +17,13 @@ def test_served_results_equal_alone(gpu_ctx):
         srv.close()
     assert all(c.error is None for c in done), [c.error for c in done if c.error]
     assert srv.peak_running >= 2  # requests were admitted while others ran
-    args = native.ModeFindingArguments(strategy=native.SWEEP_SPECULATIVE)
+    args = native.ModeFindingArguments(strategy=native.SWEEP_LEVELS)
+    alone_ctx = native.Context(0)
+    alone_ctx.set_max_ctas(max(1, alone_ctx.sm_count // 4))  # the slots' grid size
     for c, (_, d) in zip(done, stream):
-        alone = native.fit_model(gpu_ctx, d, args)
+        alone = native.fit_model(alone_ctx, d, args)
         assert c.flag == alone.return_flag and c.iterations == alone.iterations, c.rid
         assert np.array_equal(c.beta, alone.beta), c.rid
+    alone_ctx.close()
     s = serve.latency_summary(done)
     assert s["failed"] == 0 and s["p99_s"] >= s["p50_s"] > 0
