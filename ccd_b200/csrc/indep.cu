@@ -312,6 +312,70 @@ __device__ __forceinline__ void staged_update(const IndepParams& P, const Staged
     }
 }
 
+// The same gather, gradient/Hessian and update with the gathered row state
+// held in shared memory instead of registers: each thread copies its entries'
+// two 16-byte state words with cp.async (L2, like the register path's loads)
+// into its own slots, waits for its own copies, and computes from there; the
+// update reads the same slots.  Slot (i, tid) is g[2 * (i * kThreads + tid)].
+__device__ __forceinline__ void cp_async16_cg(void* dst, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+
+template <int MODEL, int N>
+__device__ __forceinline__ void staged_gh_smem(const IndepParams& P, bool ind, const Staged<N>& s,
+                                               double2* gbuf, int tid, double& g, double& h) {
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+        if (s.k[i] >= 0) {
+            double2* slot = gbuf + 2 * (i * kThreads + tid);
+            cp_async16_cg(slot, P.row + 2 * (int64_t)s.k[i]);
+            cp_async16_cg(slot + 1, P.row + 2 * (int64_t)s.k[i] + 1);
+        }
+    asm volatile("cp.async.commit_group;\ncp.async.wait_all;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        if (s.k[i] < 0) continue;
+        const double2 a = gbuf[2 * (i * kThreads + tid)];
+        const double2 b = gbuf[2 * (i * kThreads + tid) + 1];
+        const double x = s.x[i];
+        const double n1 = a.y * x;
+        if (MODEL == M_LOGISTIC) {
+            const double gg = n1 / b.x;
+            g += b.y * gg;
+            if (ind) h += b.y * gg * (1.0 - gg);
+            else h += b.y * ((n1 * x) / b.x - gg * gg);
+        } else {
+            if (ind) {
+                const double v = b.y * n1;
+                g += v;
+                h += v;
+            } else {
+                g += b.y * n1;
+                h += b.y * (n1 * x);
+            }
+        }
+    }
+}
+
+template <int N>
+__device__ __forceinline__ void staged_update_smem(const IndepParams& P, const Staged<N>& s,
+                                                   const double2* gbuf, int tid, double delta) {
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        if (s.k[i] < 0) continue;
+        const double2 a = gbuf[2 * (i * kThreads + tid)];
+        const double dn0 = gbuf[2 * (i * kThreads + tid) + 1].x;
+        const double xb = a.x + delta * s.x[i];
+        const double en = exp(xb);
+        const double dn = dn0 + (en - a.y);
+        __stcg(P.row + 2 * (int64_t)s.k[i], make_double2(xb, en));
+        __stcg(reinterpret_cast<double*>(P.row + 2 * (int64_t)s.k[i] + 1), dn);
+    }
+}
+
+constexpr size_t kGatherSmem = sizeof(double2) * 2 * kThreads * kE;  // 128 KiB
+
 __device__ __forceinline__ double meta_step(const ColMeta& m, int64_t entries, double gsum,
                                             double hsum, double& hd_out) {
     double g = 0.0, h = 0.0;
@@ -344,6 +408,7 @@ __global__ void __launch_bounds__(kThreads, 1) indep_sweep_kernel(IndepParams P)
     // and each lane's entries of its warp task
     __shared__ ColMeta s_meta[kWarps + 1];
     __shared__ Staged<kEw> s_wstage[kThreads];
+    extern __shared__ __align__(16) double2 s_gath[];  // gathered row state, kGatherSmem bytes
 
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     unsigned epoch = 0;
@@ -427,11 +492,9 @@ __global__ void __launch_bounds__(kThreads, 1) indep_sweep_kernel(IndepParams P)
                 const bool staged = (q == 0) && c_staged;
                 double g = 0.0, h = 0.0;
                 Staged<kE> sc;
-                double2 A[kE];
-                double Dn[kE];
                 if (staged) {
                     stage_entries(P, t, tid, blockDim.x, sc);  // L1 hits after the prefetch
-                    staged_gh<MODEL>(P, ind, sc, A, Dn, g, h);
+                    staged_gh_smem<MODEL>(P, ind, sc, s_gath, tid, g, h);
                 } else {
                     gh_dispatch<MODEL>(P, t.col, f, t.p0, t.p1, tid, blockDim.x, g, h);
                 }
@@ -454,7 +517,7 @@ __global__ void __launch_bounds__(kThreads, 1) indep_sweep_kernel(IndepParams P)
                     __syncthreads();
                     const double d = s_delta;
                     if (d != 0.0) {
-                        if (staged) staged_update(P, sc, A, Dn, d);
+                        if (staged) staged_update_smem(P, sc, s_gath, tid, d);
                         else update_dispatch(P, t.col, f, t.p0, t.p1, tid, blockDim.x, d);
                     }
                     __syncthreads();
@@ -471,12 +534,10 @@ __global__ void __launch_bounds__(kThreads, 1) indep_sweep_kernel(IndepParams P)
                     const bool ind = (f == F_INDICATOR || f == F_INTERCEPT);
                     const bool staged = (q == qw_first) && w_staged;
                     double g = 0.0, h = 0.0;
-                    double2 A[kEw];
-                    double Dn[kEw];
                     Staged<kEw> sw;
                     if (staged) {
                         sw = s_wstage[tid];
-                        staged_gh<MODEL>(P, ind, sw, A, Dn, g, h);
+                        staged_gh_smem<MODEL>(P, ind, sw, s_gath, tid, g, h);
                     } else {
                         gh_dispatch<MODEL>(P, t.col, f, t.p0, t.p1, lane, 32, g, h);
                     }
@@ -490,7 +551,7 @@ __global__ void __launch_bounds__(kThreads, 1) indep_sweep_kernel(IndepParams P)
                     }
                     d = __shfl_sync(0xffffffffu, d, 0);
                     if (d != 0.0) {
-                        if (staged) staged_update(P, sw, A, Dn, d);
+                        if (staged) staged_update_smem(P, sw, s_gath, tid, d);
                         else update_dispatch(P, t.col, f, t.p0, t.p1, lane, 32, d);
                     }
                 }
@@ -531,11 +592,9 @@ __global__ void __launch_bounds__(kThreads, 1) indep_sweep_kernel(IndepParams P)
                         // registers alive across phase 2 would spill
                         Staged<kE> s2;
                         stage_entries(P, t, tid, blockDim.x, s2);
-                        double2 A[kE];
-                        double Dn[kE];
                         double g = 0.0, h = 0.0;
-                        staged_gh<MODEL>(P, true, s2, A, Dn, g, h);
-                        staged_update(P, s2, A, Dn, d);
+                        staged_gh_smem<MODEL>(P, true, s2, s_gath, tid, g, h);
+                        staged_update_smem(P, s2, s_gath, tid, d);
                     } else {
                         update_dispatch(P, t.col, P.fmt[t.col], t.p0, t.p1, tid, blockDim.x, d);
                     }
@@ -731,20 +790,32 @@ cudaError_t launch_xbeta_dense(const double* vals, double b, int64_t K, double* 
 int indep_threads() { return kThreads; }
 int indep_max_split() { return kMaxSplit; }
 
+static cudaError_t indep_sweep_smem_attr() {
+    cudaError_t e = cudaFuncSetAttribute(indep_sweep_kernel<M_LOGISTIC>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGatherSmem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(indep_sweep_kernel<M_POISSON>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kGatherSmem);
+}
+
 cudaError_t indep_sweep_occupancy(int model, int* blocks_per_sm) {
+    cudaError_t e = indep_sweep_smem_attr();
+    if (e != cudaSuccess) return e;
     if (model == M_LOGISTIC)
         return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm,
                                                              indep_sweep_kernel<M_LOGISTIC>,
-                                                             kThreads, 0);
+                                                             kThreads, kGatherSmem);
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm,
-                                                         indep_sweep_kernel<M_POISSON>, kThreads, 0);
+                                                         indep_sweep_kernel<M_POISSON>, kThreads, kGatherSmem);
 }
 
 cudaError_t launch_indep_sweep(const IndepParams& P, int n_cta, cudaStream_t stream) {
     void* args[] = {(void*)&P};
     const void* fn = (P.model == M_LOGISTIC) ? (const void*)indep_sweep_kernel<M_LOGISTIC>
                                              : (const void*)indep_sweep_kernel<M_POISSON>;
-    return cudaLaunchCooperativeKernel(fn, dim3(n_cta), dim3(kThreads), args, 0, stream);
+    cudaError_t e = indep_sweep_smem_attr();
+    if (e != cudaSuccess) return e;
+    return cudaLaunchCooperativeKernel(fn, dim3(n_cta), dim3(kThreads), args, kGatherSmem, stream);
 }
 
 cudaError_t launch_indep_gh(const IndepParams& P, int j, int64_t entries, double2* parts,
