@@ -408,7 +408,9 @@ def run_ours(args, world, rank, local):
         per_launch_bytes = (sweep_bytes(d) * sweeps + objective_bytes(d) * (sweeps + args.steps)) / args.steps
         achieved = (sweep_bytes(d) * sweeps + objective_bytes(d) * (sweeps + args.steps)) / ker_t / 1e9
         wl = config_of(d, args.small)["workload"]
-        traffic = read_traffic(wl)
+        traffic = read_traffic(wl)  # DRAM bytes of one sweep (ncu), scaled to the launch's sweeps
+        if traffic is not None:
+            traffic = traffic * sweeps / args.steps
         line = {
             "metric": METRIC, "value": tot_updates / dev_max, "unit": METRIC, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dev_max / args.steps,
