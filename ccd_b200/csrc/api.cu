@@ -287,6 +287,11 @@ void Fit::ensure_schedule() {
     ScheduleParams sp;
     sp.n_cta = ctx->n_sm * std::min(bps, 1);
     if (ctx->max_ctas > 0) sp.n_cta = std::min(sp.n_cta, ctx->max_ctas);
+    // columns up to cta_max entries run on one CTA; longer ones split over CTAs
+    // (CCDB_CTA_MAX overrides, a tuning knob)
+    if (const char* cm = std::getenv("CCDB_CTA_MAX")) sp.cta_max = std::max<int64_t>(1024, std::atoll(cm));
+    if (const char* ck = std::getenv("CCDB_CHUNK")) sp.chunk = std::max<int64_t>(1024, std::atoll(ck));
+    if (const char* wm = std::getenv("CCDB_WARP_MAX")) sp.warp_max = std::max<int64_t>(32, std::atoll(wm));
     sp.warps_per_cta = indep_threads() / 32;
     std::vector<int64_t> entries(J);
     for (int j = 0; j < J; ++j) entries[j] = m->entries(j);
