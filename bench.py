@@ -453,7 +453,7 @@ def cv_workload(small: bool, columns: int = 20_000):
 
 
 def cv_bytes(d, res) -> float:
-    """Algorithmic bytes of a grid (batched form): column indices once for
+    """Algorithmic bytes of a grid (the batched form of the per-coordinate count): column indices once for
     all instances (the most any instance gathered), per instance one 8-byte state word
     per gathered entry, 4-byte weight per entry, read+write per updated entry, and the
     convergence checks (y and xBeta per row per sweep)."""
