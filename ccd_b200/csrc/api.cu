@@ -1209,8 +1209,6 @@ int ccdb_batch_find_mode(ccdb_fit* f, const ccdb_batch_desc* b, const ccdb_mode_
             P.stage_cap = max_slice <= 1024 ? 1024 : 3072;
             P.queue = (int32_t*)keep(ctx->alloc(sizeof(int32_t)));
             check_cuda(cudaMemsetAsync(P.queue, 0, sizeof(int32_t), s), "batch queue");
-            P.min_blocks = 1;
-            if (const char* mb = std::getenv("CCDB_BATCH_MINB")) P.min_blocks = std::atoi(mb) == 2 ? 2 : 1;
             P.xg = (double*)keep(ctx->alloc(sizeof(double) * (size_t)K * G * n_groups));
             P.beta_g = (double*)keep(ctx->alloc(sizeof(double) * (size_t)J * G * n_groups));
             P.hd_g = (double*)keep(ctx->alloc(sizeof(double) * (size_t)J * G * n_groups));

@@ -70,7 +70,7 @@ struct BatchParams {
     // C + 1 entry offsets where its rows cross those boundaries (J x (C + 1))
     int32_t cluster;
     int32_t stage_cap;         // mixed: staged entries per slice (1024 or 3072)
-    int32_t min_blocks;        // mixed, stage_cap 1024: CTAs per SM the kernel is built for (1 or 2)
+    int32_t pad5;
     int32_t pad4;
     const int32_t* split;
     int32_t* queue;            // mixed: next group to fit (zeroed before the launch)

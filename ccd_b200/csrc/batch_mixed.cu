@@ -46,8 +46,8 @@ constexpr int kRing = 8;           // column metadata ring: columns j .. j + kAh
 
 using namespace bm;
 
-template <int MODEL, int G, int SN, int MINB>
-__global__ void __launch_bounds__(kMT, MINB) batch_mixed_kernel(BatchParams P) {
+template <int MODEL, int G, int SN>
+__global__ void __launch_bounds__(kMT, 1) batch_mixed_kernel(BatchParams P) {
     constexpr int S = Inst<G>::S;    // threads per instance
     constexpr int kE = SN / S;       // staged entries per thread
     __shared__ double s_red2[2][kMW][4][2];
@@ -270,10 +270,10 @@ __global__ void batch_keys_kernel(const int32_t* rows, int64_t nnz, const int32_
     }
 }
 
-template <int MODEL, int G, int SN, int MINB>
+template <int MODEL, int G, int SN>
 cudaError_t launch_g(const BatchParams& P, cudaStream_t stream) {
     const size_t smem = sizeof(MStage<SN>) * kNBuf;
-    void (*fn)(BatchParams) = batch_mixed_kernel<MODEL, G, SN, MINB>;
+    void (*fn)(BatchParams) = batch_mixed_kernel<MODEL, G, SN>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int C = P.cluster > 0 ? P.cluster : 1;
@@ -306,8 +306,8 @@ cudaError_t launch_g(const BatchParams& P, cudaStream_t stream) {
 template <int MODEL, int G>
 cudaError_t launch_sn(const BatchParams& P, cudaStream_t stream) {
     if (P.stage_cap <= 1024)
-        return P.min_blocks == 2 ? launch_g<MODEL, G, 1024, 2>(P, stream) : launch_g<MODEL, G, 1024, 1>(P, stream);
-    return launch_g<MODEL, G, 3072, 1>(P, stream);
+        return launch_g<MODEL, G, 1024>(P, stream);
+    return launch_g<MODEL, G, 3072>(P, stream);
 }
 
 template <int MODEL>
