@@ -999,6 +999,38 @@ int ccdb_get_gradient_objective(ccdb_fit* f, double* out) {
     });
 }
 
+int ccdb_fisher_information(ccdb_fit* f, const int32_t* indices, int32_t n, double* out) {
+    return guard([&] {
+        require(f != nullptr, "NULL fit");
+        require(n >= 0, "negative column count");
+        require(n == 0 || (indices && out), "NULL argument");
+        require_fp64(f);
+        for (int32_t i = 0; i < n; ++i) require(indices[i] >= 0 && indices[i] < f->J, "column out of range");
+        if (f->weighted)
+            throw Error(CCDB_ERR_UNSUPPORTED, "Weights are not yet implemented in Fisher Information calculations");
+        f->fisher_information(indices, n, out);
+    });
+}
+
+int ccdb_get_predictive_log_likelihood(ccdb_fit* f, const double* weights, double* out) {
+    return guard([&] {
+        require(f && weights && out, "NULL argument");
+        require_fp64(f);
+        *out = f->predictive_log_likelihood(weights);
+    });
+}
+
+int ccdb_get_predictive_estimates(ccdb_fit* f, const double* weights, double* y) {
+    return guard([&] {
+        require(f && y, "NULL argument");
+        require_fp64(f);
+        std::vector<double> p(f->K);
+        f->predictive_estimates(p.data());
+        for (int64_t k = 0; k < f->K; ++k)
+            if (!weights || weights[k] != 0.0) y[k] = p[k];
+    });
+}
+
 int ccdb_get_beta(ccdb_fit* f, double* out) {
     return guard([&] {
         require(f && out, "NULL argument");

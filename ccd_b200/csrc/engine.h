@@ -176,6 +176,11 @@ struct Fit {
     void cox_objective_terms(double* out4);
     void cox_gh_batch(const int32_t* cols, int n, double2* out);
     void cox_update(int j, double delta);
+    // post-fit calls (postfit_host.cu)
+    void fisher_information(const int32_t* idx, int n, double* out);
+    double predictive_log_likelihood(const double* weights);
+    double predictive_sum(const double* weights);
+    void predictive_estimates(double* out);
 };
 
 }  // namespace ccdb

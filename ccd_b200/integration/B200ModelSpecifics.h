@@ -151,14 +151,26 @@ public:
                                      bool) override {
         unsupported("computeMMGradientAndHessian");
     }
-    void computeFisherInformation(int, int, double*, bool) override {
-        unsupported("computeFisherInformation");
+    // ModelSpecifics::computeFisherInformation (ModelSpecifics.hpp:1203-1225): the
+    // reference refuses weighted fits with a logic_error; so does this engine.
+    void computeFisherInformation(int indexOne, int indexTwo, double* oinfo, bool useWeights) override {
+        if (useWeights) throw std::logic_error("Weights are not yet implemented in Fisher Information calculations");
+        sync_beta();
+        const int32_t idx[2] = {indexOne, indexTwo};
+        double out[4];
+        check(ccdb_fisher_information(fit_, idx, 2, out), "computeFisherInformation");
+        *oinfo = out[1];
     }
-    double getPredictiveLogLikelihood(double*) override {
-        unsupported("getPredictiveLogLikelihood");
-        return 0.0;
+    double getPredictiveLogLikelihood(double* weights) override {
+        sync_beta();
+        double ll = 0.0;
+        check(ccdb_get_predictive_log_likelihood(fit_, weights, &ll), "getPredictiveLogLikelihood");
+        return ll;
     }
-    void getPredictiveEstimates(double*, double*) override { unsupported("getPredictiveEstimates"); }
+    void getPredictiveEstimates(double* y, double* weights) override {
+        sync_beta();
+        check(ccdb_get_predictive_estimates(fit_, weights, y), "getPredictiveEstimates");
+    }
     void printTiming() override {}
 
     AbstractModelSpecifics* clone() const override {

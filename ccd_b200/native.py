@@ -127,6 +127,9 @@ def lib() -> C.CDLL:
         L.ccdb_column_gradient_hessian_noalloc.argtypes = [C.c_int32, C.c_int32, C.c_int64, _P, _P, _P,
                                                            C.c_double, _P, _P]
         L.ccdb_sweep_levels.argtypes = [C.c_int64, C.c_int32, _P, _P, _P, _P, _P, _P]
+        L.ccdb_fisher_information.argtypes = [_P, _P, C.c_int32, _P]
+        L.ccdb_get_predictive_log_likelihood.argtypes = [_P, _P, _P]
+        L.ccdb_get_predictive_estimates.argtypes = [_P, _P, _P]
         _lib = L
     return _lib
 
@@ -290,6 +293,34 @@ class Fit:
     def get_beta(self) -> np.ndarray:
         out = np.zeros(self.d.J)
         _check(lib().ccdb_get_beta(self.h, _p(out)))
+        return out
+
+    # --- calls on a fitted state
+    def compute_fisher_information(self, indices) -> np.ndarray:
+        """CyclicCoordinateDescent::computeFisherInformation(indices)
+        (CyclicCoordinateDescent.cpp:1288-1299): the n x n Fisher information
+        over the columns `indices` on the current state.  Weighted fits raise
+        CcdbError(ERR_UNSUPPORTED), as the reference refuses them."""
+        idx = np.ascontiguousarray(indices, dtype=np.int32).reshape(-1)
+        out = np.zeros((len(idx), len(idx)))
+        _check(lib().ccdb_fisher_information(self.h, _p(idx), len(idx), _p(out)))
+        return out
+
+    def get_predictive_log_likelihood(self, weights: np.ndarray) -> float:
+        """getNewPredictiveLogLikelihood (CyclicCoordinateDescent.cpp:319-355)
+        of the current beta on held-out row weights."""
+        w = _c(weights, np.float64)
+        v = C.c_double()
+        _check(lib().ccdb_get_predictive_log_likelihood(self.h, _p(w), C.byref(v)))
+        return v.value
+
+    def get_predictive_estimates(self, weights: Optional[np.ndarray] = None,
+                                 y: Optional[np.ndarray] = None) -> np.ndarray:
+        """getPredictiveEstimates (ModelSpecifics.hpp:692-705): the model's
+        prediction of every row; with weights, rows of weight zero keep y."""
+        out = np.zeros(self.d.K) if y is None else np.array(y, dtype=np.float64)
+        w = _c(weights, np.float64)
+        _check(lib().ccdb_get_predictive_estimates(self.h, _p(w), _p(out)))
         return out
 
     # --- the cross-validation grid: many instances in one launch

@@ -117,6 +117,31 @@ int ccdb_get_beta(ccdb_fit* f, double* out);
 /* getGradientObjective (ModelSpecifics.hpp:103-120): sum of y * xBeta (* weight). */
 int ccdb_get_gradient_objective(ccdb_fit* f, double* out);
 
+/* --- calls on a fitted state ------------------------------------------------ */
+
+/* Fisher information over the columns indices[0..n) on the current state:
+ * out[i * n + j] for the pair (indices[i], indices[j]), symmetric, n x n.
+ * Replaces CyclicCoordinateDescent::computeFisherInformation(indices)
+ * (CyclicCoordinateDescent.cpp:1288-1299) and, with n = 2, the per-pair
+ * ModelSpecifics::computeFisherInformation (ModelSpecifics.hpp:1203-1337,
+ * AbstractModelSpecifics.h:68).  A weighted fit (ccdb_set_weights with
+ * weights) is refused with CCDB_ERR_UNSUPPORTED, as the reference throws for
+ * it (ModelSpecifics.hpp:1207-1208).  The strata cross terms of the grouped
+ * and Cox models come from the current state on every call. */
+int ccdb_fisher_information(ccdb_fit* f, const int32_t* indices, int32_t n, double* out);
+/* Predictive log-likelihood of the current beta on held-out row weights
+ * weights[K] (CyclicCoordinateDescent::getNewPredictiveLogLikelihood,
+ * CyclicCoordinateDescent.cpp:319-355, over ModelSpecifics::
+ * getPredictiveLogLikelihood, ModelSpecifics.hpp:652-690,
+ * AbstractModelSpecifics.h:106).  The Cox model takes its risk sets under the
+ * held-out weights and then returns to the fit's own weights. */
+int ccdb_get_predictive_log_likelihood(ccdb_fit* f, const double* weights, double* out);
+/* predictEstimate of each row's xBeta into y[K]: LR exp(xb)/(exp(xb)+1),
+ * Poisson exp(xb), conditional and Cox models xb (getPredictiveEstimates,
+ * ModelSpecifics.hpp:692-705, AbstractModelSpecifics.h:108).  With weights
+ * non-NULL only rows whose weight is nonzero are written. */
+int ccdb_get_predictive_estimates(ccdb_fit* f, const double* weights, double* y);
+
 /* --- mode finding (CyclicCoordinateDescent::update) ------------------------ */
 
 typedef struct {

@@ -838,6 +838,133 @@ int orc_predictive_loglik(void* hp, const double* w, double* out) {
     return 0;
 }
 
+/* incrementFisherInformation of the model (weight = hKWeight = 1: the unweighted
+ * fits computeFisherInformation accepts, MS.hpp:434-440):
+ *   Logistic MS.h:521-535   weight * (p/d - (p/d)^2) * x1x2
+ *   Poisson  MS.h:1497-1506 weight * p * x1x2
+ *   Survival MS.h:485-498   weight * p / d * x1x2   (CLR, CPR, Breslow Cox)
+ * d is denomPid of the row's group (its own slot for independent rows). */
+static double fisher_increment(const Orc* o, int64_t k, double x12) {
+    const double weight = 1.0, p = o->e[k];
+    switch (o->model) {
+    case MT_LOGISTIC: {
+        const double d = o->denom[k];
+        const double g = p / d;
+        return weight * (p / d - g * g) * x12;
+    }
+    case MT_POISSON:
+        return weight * p * x12;
+    default:
+        return weight * p / o->denom[o->hpid[k]] * x12;
+    }
+}
+
+/* getSubjectSpecificHessianIterator, MS.hpp:1245-1266: walk the column in row
+ * order, one (hPid, sum of e*x) pair per run of rows sharing hPid. */
+static int fisher_cross_terms(const Orc* o, int j, int32_t* gid, double* val) {
+    const int64_t len = col_len(o, j);
+    int n = 0;
+    int64_t p = 0;
+    while (p < len) {
+        double v = 0.0;
+        const int g = o->hpid[col_row(o, j, p)];
+        do {
+            const int64_t k = col_row(o, j, p);
+            v += o->e[k] * col_val(o, j, p); /* gradientNumeratorContrib, MS.h:437-441 */
+            ++p;
+        } while (p < len && o->hpid[col_row(o, j, p)] == g);
+        gid[n] = g;
+        val[n] = v;
+        ++n;
+    }
+    return n;
+}
+
+/* computeFisherInformationImpl, MS.hpp:1268-1337: the pair-product walk over
+ * the rows both columns hold (PairProductIterator, Iterators.h:627-680), minus
+ * the strata cross terms for GroupedData / OrderedWithTiesData models. */
+static double fisher_pair(const Orc* o, int i, int j, int32_t* g1, double* v1, int32_t* g2, double* v2) {
+    double information = 0.0;
+    const int64_t n1 = col_len(o, i), n2 = col_len(o, j);
+    int64_t p = 0, q = 0;
+    while (p < n1 && q < n2) {
+        const int64_t a = col_row(o, i, p), b = col_row(o, j, q);
+        if (a < b) {
+            ++p;
+        } else if (b < a) {
+            ++q;
+        } else {
+            information += fisher_increment(o, a, col_val(o, i, p) * col_val(o, j, q));
+            ++p;
+            ++q;
+        }
+    }
+    if (!is_indep(o)) { /* hasStrataCrossTerms */
+        const int m1 = fisher_cross_terms(o, i, g1, v1), m2 = fisher_cross_terms(o, j, g2, v2);
+        double cross = 0.0;
+        int r = 0, s = 0;
+        while (r < m1 && s < m2) {
+            if (g1[r] < g2[s]) {
+                ++r;
+            } else if (g2[s] < g1[r]) {
+                ++s;
+            } else {
+                const double d = o->denom[g1[r]];
+                cross += v1[r] * v2[s] / (d * d);
+                ++r;
+                ++s;
+            }
+        }
+        information -= cross;
+    }
+    return information;
+}
+
+/* CyclicCoordinateDescent::computeFisherInformation(indices), CCD.cpp:1288-1299
+ * -> ModelSpecifics::computeFisherInformation, MS.hpp:1203-1225.  `out` is
+ * n x n, row-major, symmetric.  Weighted (cross-validation) fits are refused
+ * as the reference refuses them (MS.hpp:1207-1208): returns -2. */
+int orc_fisher_information(void* hp, const int32_t* idx, int n, double* out) {
+    Orc* o = (Orc*)hp;
+    if (o->w) return -2;
+    check_lazy(o);
+    const size_t cap = (size_t)o->K + 1;
+    int32_t *g1 = (int32_t*)malloc(sizeof(int32_t) * cap), *g2 = (int32_t*)malloc(sizeof(int32_t) * cap);
+    double *v1 = (double*)malloc(sizeof(double) * cap), *v2 = (double*)malloc(sizeof(double) * cap);
+    for (int ii = 0; ii < n; ++ii)
+        for (int jj = ii; jj < n; ++jj) {
+            const double e = fisher_pair(o, idx[ii], idx[jj], g1, v1, g2, v2);
+            out[(size_t)ii * n + jj] = e;
+            out[(size_t)jj * n + ii] = e;
+        }
+    free(g1);
+    free(g2);
+    free(v1);
+    free(v2);
+    return 0;
+}
+
+/* getPredictiveEstimates, MS.hpp:692-705, with predictEstimate of the model:
+ * LR exp(xb)/(exp(xb)+1) (MS.h:1011-1014), Poisson exp(xb) (MS.h:1592-1594),
+ * the conditional and Cox models xb.  Rows with a zero weight keep y. */
+int orc_predictive_estimates(void* hp, const double* w, double* y) {
+    Orc* o = (Orc*)hp;
+    check_lazy(o);
+    for (int64_t k = 0; k < o->K; ++k) {
+        if (w && !w[k]) continue;
+        const double xb = o->xb[k];
+        if (o->model == MT_LOGISTIC) {
+            const double t = exp(xb);
+            y[k] = t / (t + 1.0);
+        } else if (o->model == MT_POISSON) {
+            y[k] = exp(xb);
+        } else {
+            y[k] = xb;
+        }
+    }
+    return 0;
+}
+
 int orc_num_patients(void* hp) { return ((Orc*)hp)->Npatients; }
 
 int orc_cox_groups(void* hp, int32_t* group_out, int32_t* acc_reset_out, int* n_reset_out) {

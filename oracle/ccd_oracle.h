@@ -35,6 +35,11 @@ int orc_get_beta(void* h, double* out);
 int orc_get_xbeta(void* h, double* out);
 int orc_predictive_loglik(void* h, const double* w, double* out);
 int orc_num_patients(void* h);
+/* Fisher information of the current state over columns idx[0..n) (n x n,
+ * row-major); -2 for a weighted fit, which the reference refuses. */
+int orc_fisher_information(void* h, const int32_t* idx, int n, double* out);
+/* predictEstimate per row; rows whose weight is zero keep y (w may be NULL). */
+int orc_predictive_estimates(void* h, const double* w, double* y);
 /* Cox grouping as setPidForAccumulation computes it: group id per row (N for
  * dropped rows), the stratum-start list accReset, returns N. */
 int orc_cox_groups(void* h, int32_t* group_out, int32_t* acc_reset_out, int* n_reset_out);

@@ -70,6 +70,12 @@ class _Engine:
                 getattr(lib, p + name).argtypes = [_P, _P]
             getattr(lib, p + "predictive_loglik").argtypes = [_P, _P, _P]
             getattr(lib, p + "num_patients").argtypes = [_P]
+            if p == "ref_":
+                lib.ref_fisher_information.argtypes = [_P, _P, C.c_int, _P, C.c_char_p, C.c_int]
+                lib.ref_asymptotic_variance.argtypes = [_P, C.c_int, C.c_int, _P, C.c_char_p, C.c_int]
+            else:
+                lib.orc_fisher_information.argtypes = [_P, _P, C.c_int, _P]
+            getattr(lib, p + "predictive_estimates").argtypes = [_P, _P, _P]
             _Engine._lib_cache[cls.libpath] = lib
         return _Engine._lib_cache[cls.libpath]
 
@@ -168,12 +174,51 @@ class _Engine:
         return v.value
 
 
+    def fisher_information(self, indices) -> np.ndarray:
+        """Fisher information over the columns `indices` (n x n).  Raises
+        FisherRefused where the engine refuses (weighted fits)."""
+        idx = np.ascontiguousarray(indices, np.int32)
+        out = np.zeros((len(idx), len(idx)))
+        if self.prefix == "ref_":
+            err = C.create_string_buffer(512)
+            rc = self._f("fisher_information")(self.h, _ptr(idx), len(idx), _ptr(out), err, 512)
+            msg = err.value.decode()
+        else:
+            rc = self._f("fisher_information")(self.h, _ptr(idx), len(idx), _ptr(out))
+            msg = "Weights are not yet implemented in Fisher Information calculations"
+        if rc == -2:
+            raise FisherRefused(msg)
+        if rc != 0:
+            raise RuntimeError(msg)
+        return out
+
+    def predictive_estimates(self, w: Optional[np.ndarray] = None, y: Optional[np.ndarray] = None):
+        y = np.zeros(self.d.K) if y is None else np.array(y, dtype=np.float64)
+        if w is not None:
+            w = np.ascontiguousarray(w, np.float64)
+        self._f("predictive_estimates")(self.h, _ptr(w), _ptr(y))
+        return y
+
+
+class FisherRefused(RuntimeError):
+    """The engine refuses a Fisher information request (a weighted fit)."""
+
+
 class ReferenceEngine(_Engine):
     prefix = "ref_"
     libpath = REF_LIB
 
 
-class ReferenceOnB200Engine(_Engine):
+    def asymptotic_variance(self, i: int, j: int) -> float:
+        v = C.c_double()
+        err = C.create_string_buffer(512)
+        rc = self._f("asymptotic_variance")(self.h, i, j, C.byref(v), err, 512)
+        if rc != 0:
+            raise (FisherRefused if rc == -2 else RuntimeError)(err.value.decode())
+        return v.value
+
+
+class ReferenceOnB200Engine(ReferenceEngine):
     """The reference's own CyclicCoordinateDescent driving the B200 engine
     through ccd_b200/integration/B200ModelSpecifics.h (the drop-in)."""
     prefix = "ref_"

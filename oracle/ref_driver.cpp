@@ -316,4 +316,60 @@ int ref_num_patients(void* hp) {
     return static_cast<int>(h->data->getNumberOfPatients());
 }
 
+// CyclicCoordinateDescent::computeFisherInformation(indices) (.cpp:1288-1299),
+// the call behind the R binding's getFisherInformation, after the lazy state is
+// brought current (that call itself does not check it).  out: n x n, row-major.
+// Returns -2 when the engine refuses (weighted fits: ModelSpecifics.hpp:1207-1208
+// throws a std::logic_error*, the B200 adapter a std::logic_error), -1 on any
+// other error.
+int ref_fisher_information(void* hp, const int32_t* idx, int n, double* out, char* err, int errlen) {
+    auto h = static_cast<RefHandle*>(hp);
+    try {
+        h->ccd->getLogLikelihood();
+        std::vector<IdType> indices(idx, idx + n);
+        const auto m = h->ccd->computeFisherInformation(indices);
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) out[(size_t)i * n + j] = m(i, j);
+        return 0;
+    } catch (std::logic_error* e) {
+        set_err(err, errlen, e->what());
+        delete e;
+        return -2;
+    } catch (const std::logic_error& e) {
+        set_err(err, errlen, e.what());
+        return -2;
+    } catch (const std::exception& e) {
+        set_err(err, errlen, e.what());
+        return -1;
+    }
+}
+
+// CyclicCoordinateDescent::getAsymptoticVariance(i, j) (.cpp:1249-1269): the
+// inverse of the Fisher information over the free, non-zero-Laplace columns
+// (computeAsymptoticPrecisionMatrix, .cpp:1301-1347); NaN for other columns.
+int ref_asymptotic_variance(void* hp, int i, int j, double* out, char* err, int errlen) {
+    auto h = static_cast<RefHandle*>(hp);
+    try {
+        *out = h->ccd->getAsymptoticVariance(i, j);
+        return 0;
+    } catch (std::logic_error* e) {
+        set_err(err, errlen, e->what());
+        delete e;
+        return -2;
+    } catch (const std::exception& e) {
+        set_err(err, errlen, e.what());
+        return -1;
+    }
+}
+
+// CyclicCoordinateDescent::getPredictiveEstimates (.cpp:357-359); w may be NULL.
+int ref_predictive_estimates(void* hp, const double* w, double* y) {
+    auto h = static_cast<RefHandle*>(hp);
+    h->ccd->getLogLikelihood();
+    std::vector<double> wb;
+    if (w) wb.assign(w, w + h->K);
+    h->ccd->getPredictiveEstimates(y, w ? wb.data() : nullptr);
+    return 0;
+}
+
 }  // extern "C"

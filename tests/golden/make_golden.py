@@ -6,8 +6,12 @@ Every case stores its inputs (the CompressedDataMatrix, outcomes, strata,
 times, priors, weights) and what the reference Cyclops engine
 (oracle/_ref/libccd_ref.so) returns for them: the gradient/Hessian of every
 coordinate at the starting state, and CyclicCoordinateDescent::update's
-coefficients, log-likelihood, iteration count and return flag.  Run only where
-the reference sources are present; the fixtures are committed.
+coefficients, log-likelihood, iteration count and return flag.  At that mode
+it also stores the calls on a fitted state: the Fisher information over every
+coefficient column (unweighted cases; the reference refuses weighted ones),
+the predictive estimates, and the predictive log-likelihood on a fixed
+held-out row set.  Run only where the reference sources are present; the
+fixtures are committed.
 """
 import hashlib
 import json
@@ -23,7 +27,7 @@ sys.path.insert(0, ROOT)
 from ccd_b200 import synthetic  # noqa: E402
 from ccd_b200.data import (GRADIENT, LANGE, MITTAL, MODEL_CONDITIONAL_LOGISTIC, MODEL_COX,  # noqa: E402
                            MODEL_LOGISTIC, MODEL_POISSON, PRIOR_LAPLACE, PRIOR_NORMAL)
-from oracle.checker import ReferenceEngine  # noqa: E402
+from oracle.checker import FisherRefused, ReferenceEngine  # noqa: E402
 
 CASES = [
     ("lr_mixed_laplace", MODEL_LOGISTIC, dict(seed=21), GRADIENT, None),
@@ -48,6 +52,11 @@ def weights_for(kind, K, seed):
     return (rng.random(K) > 0.25).astype(float)
 
 
+def heldout_for(K):
+    """A fixed held-out row set: every fifth row."""
+    return (np.arange(K) % 5 == 2).astype(float)
+
+
 def digest(arrs) -> str:
     h = hashlib.sha256()
     for a in arrs:
@@ -69,12 +78,24 @@ def main():
         if w is not None:
             e.set_weights(w)
         r = e.fit(conv, 1e-6)
+        cols = np.arange(1 if d.offset_col0 else 0, d.J, dtype=np.int32)
+        try:
+            fisher = e.fisher_information(cols)
+        except FisherRefused:
+            fisher = None
+        pred_est = e.predictive_estimates()
+        held = heldout_for(d.K)
+        pred_ll = e.predictive_loglik(held)
         e.close()
         arrays = dict(model_type=np.int32(d.model_type), y=d.y, col_start=d.col_start, rows=d.rows,
                       val_start=d.val_start, vals=d.vals, fmt=d.fmt, prior_type=d.prior_type,
                       prior_var=d.prior_var, offset_col0=np.int32(d.offset_col0),
                       conv=np.int32(conv), gh0=gh, beta=r["beta"], loglik=np.float64(r["loglik"]),
-                      iterations=np.int32(r["iterations"]), flag=np.int32(r["flag"]))
+                      iterations=np.int32(r["iterations"]), flag=np.int32(r["flag"]),
+                      pred_est=pred_est, heldout=held, pred_ll=np.float64(pred_ll))
+        if fisher is not None:
+            arrays["fisher_cols"] = cols
+            arrays["fisher"] = fisher
         if d.time is not None:
             arrays["time"] = d.time
         if d.stratum is not None:

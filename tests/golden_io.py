@@ -24,6 +24,12 @@ def load_case(name):
                     offset_col0=bool(int(z["offset_col0"])))
     want = {"conv": int(z["conv"]), "gh0": z["gh0"], "beta": z["beta"], "loglik": float(z["loglik"]),
             "iterations": int(z["iterations"]), "flag": int(z["flag"])}
+    # calls on the fitted state (absent from fixtures older than these fields)
+    for k in ("fisher", "fisher_cols", "pred_est", "heldout"):
+        if k in z:
+            want[k] = z[k]
+    if "pred_ll" in z:
+        want["pred_ll"] = float(z["pred_ll"])
     w = z["weights"] if "weights" in z else None
     return d, w, want
 
