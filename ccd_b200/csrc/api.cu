@@ -25,11 +25,6 @@ namespace ccdb {
 
 thread_local std::string g_last_error;
 
-struct Error : std::runtime_error {
-    int code;
-    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
-};
-
 void check_cuda(cudaError_t e, const char* what) {
     if (e != cudaSuccess)
         throw Error(CCDB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -401,6 +396,12 @@ void Fit::find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* 
     std::vector<double> hd(J, bound);  // resetBounds
     check_cuda(cudaMemcpyAsync(hdelta, hd.data(), sizeof(double) * J, cudaMemcpyHostToDevice, stream),
                "bounds");
+    if (a.algorithm == CCDB_ALGORITHM_MM) {
+        auto t0 = std::chrono::steady_clock::now();
+        find_mode_mm(a, flag, iters, obj);
+        *ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        return;
+    }
     if (a.per_coordinate) {
         // the reference's call pattern: one host round trip per coordinate
         double last = objective(a.convergence_type);
@@ -633,6 +634,16 @@ void Fit::find_mode(const ccdb_mode_args& a, double* beta_inout, ccdb_fit_result
     check_cuda(cudaMemcpyAsync(pvar, pvar_h.data(), sizeof(double) * J, cudaMemcpyHostToDevice, stream), "prior");
     if (a.convergence_type < C_GRADIENT || a.convergence_type > C_MITTAL)
         throw Error(CCDB_ERR_UNSUPPORTED, "convergence type");
+    if (a.algorithm != CCDB_ALGORITHM_CCD && a.algorithm != CCDB_ALGORITHM_MM)
+        throw Error(CCDB_ERR_UNSUPPORTED, "algorithm");
+    if (a.algorithm == CCDB_ALGORITHM_MM && !group_engine())
+        throw Error(CCDB_ERR_UNSUPPORTED,
+                    model == M_POISSON ? "Not model-specific" : "the MM algorithm needs stratified data");
+    if (a.fixed)  // setFixedBeta for every column; the offset stays fixed
+        for (int j = 0; j < J; ++j) fixed[j] = (a.fixed[j] != 0 || (offset_col0 && j == 0)) ? 1 : 0;
+    bool any_laplace = false;
+    for (int j = 0; j < J; ++j) any_laplace |= (ptype_h[j] == 1);
+    const bool swindle = a.use_kkt_swindle && any_laplace;
     if (beta_inout) {
         for (int j = 0; j < J; ++j) beta_h[j] = beta_inout[j];
         upload_beta();
@@ -649,7 +660,8 @@ void Fit::find_mode(const ccdb_mode_args& a, double* beta_inout, ccdb_fit_result
     int64_t updates = 0;
     for (;;) {
         float ms = 0.f;
-        find_mode_once(a, bound, &flag, &iters, &obj, &ms);
+        if (swindle) kkt_swindle(a, bound, &flag, &iters, &obj, &ms);
+        else find_mode_once(a, bound, &flag, &iters, &obj, &ms);
         secs += ms * 1e-3;
         updates += (int64_t)iters * active;
         ++count;
@@ -1009,6 +1021,22 @@ int ccdb_fisher_information(ccdb_fit* f, const int32_t* indices, int32_t n, doub
         if (f->weighted)
             throw Error(CCDB_ERR_UNSUPPORTED, "Weights are not yet implemented in Fisher Information calculations");
         f->fisher_information(indices, n, out);
+    });
+}
+
+int ccdb_compute_mm_gradient_hessian(ccdb_fit* f, const uint8_t* fixed, double* gradient, double* hessian) {
+    return guard([&] {
+        require(f && gradient && hessian, "NULL argument");
+        require_fp64(f);
+        if (!f->group_engine())
+            throw Error(CCDB_ERR_UNSUPPORTED, f->model == M_POISSON ? "Not model-specific"
+                                                                    : "the MM algorithm needs stratified data");
+        std::vector<double2> gh(f->J);
+        f->mm_gradient_hessian(fixed, gh.data());
+        for (int j = 0; j < f->J; ++j) {
+            gradient[j] = gh[j].x;
+            hessian[j] = gh[j].y;
+        }
     });
 }
 

@@ -7,6 +7,8 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <stdexcept>
+#include <string>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -18,6 +20,13 @@
 #include "step.h"
 
 namespace ccdb {
+
+// A failure with its C ABI status code (CCDB_ERR_*), raised by host code and
+// turned into the status at the ABI boundary.
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
 
 void check_cuda(cudaError_t e, const char* what);
 
@@ -176,6 +185,11 @@ struct Fit {
     void cox_objective_terms(double* out4);
     void cox_gh_batch(const int32_t* cols, int n, double2* out);
     void cox_update(int j, double delta);
+    // mode-finding variants (modes_host.cu): the MM cycle, the KKT swindle, and
+    // the MM all-coordinate (g, h) into out[J] (fixed may be nullptr)
+    void find_mode_mm(const ccdb_mode_args& a, int* flag, int* iters, double* obj);
+    void kkt_swindle(const ccdb_mode_args& a, double bound, int* flag, int* iters, double* obj, float* ms);
+    void mm_gradient_hessian(const uint8_t* fixed_flags, double2* out);
     // post-fit calls (postfit_host.cu)
     void fisher_information(const int32_t* idx, int n, double* out);
     double predictive_log_likelihood(const double* weights);

@@ -147,9 +147,15 @@ public:
     void saveXBeta() override { xbetaSave_ = getXBeta(); }
 
     // outside the coordinate-descent hot path
-    void computeMMGradientAndHessian(std::vector<GradientHessian>&, const std::vector<bool>&,
+    // ModelSpecifics::computeMMGradientAndHessian (ModelSpecifics.hpp:776-889).
+    void computeMMGradientAndHessian(std::vector<GradientHessian>& gh, const std::vector<bool>& fixBeta,
                                      bool) override {
-        unsupported("computeMMGradientAndHessian");
+        sync_beta();
+        std::vector<uint8_t> fixed(fixBeta.begin(), fixBeta.end());
+        std::vector<double> g(gh.size()), h(gh.size());
+        check(ccdb_compute_mm_gradient_hessian(fit_, fixed.data(), g.data(), h.data()),
+              "computeMMGradientAndHessian");
+        for (size_t j = 0; j < gh.size(); ++j) gh[j] = GradientHessian(g[j], h[j]);
     }
     // ModelSpecifics::computeFisherInformation (ModelSpecifics.hpp:1203-1225): the
     // reference refuses weighted fits with a logic_error; so does this engine.

@@ -23,6 +23,7 @@ LIB_PATH = os.path.join(HERE, "libccdb.so")
 
 OK = 0
 ERR_INVALID, ERR_CUDA, ERR_UNSUPPORTED, ERR_BUDGET, ERR_TIMEOUT = -1, -2, -3, -4, -5
+ALGORITHM_CCD, ALGORITHM_MM = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 SWEEP_AUTO, SWEEP_LEVELS, SWEEP_SPECULATIVE = 0, 1, 2
 
@@ -43,7 +44,8 @@ class _ModeArgs(C.Structure):
                 ("convergence_type", C.c_int32), ("tolerance", C.c_double),
                 ("max_iterations", C.c_int32), ("initial_bound", C.c_double),
                 ("max_bound_count", C.c_int32), ("per_coordinate", C.c_int32),
-                ("strategy", C.c_int32)]
+                ("strategy", C.c_int32), ("algorithm", C.c_int32), ("use_kkt_swindle", C.c_int32),
+                ("fixed", C.c_void_p)]
 
 
 class _BatchDesc(C.Structure):
@@ -75,6 +77,9 @@ class ModeFindingArguments:
     max_bound_count: int = 5
     per_coordinate: bool = False
     strategy: int = 0  # SWEEP_AUTO / SWEEP_LEVELS / SWEEP_SPECULATIVE
+    algorithm: int = 0  # ALGORITHM_CCD / ALGORITHM_MM (AlgorithmType)
+    kkt_swindle: bool = False  # ModeFindingArguments::useKktSwindle
+    fixed: Optional[np.ndarray] = None  # J flags (setFixedBeta), None keeps the fit's set
 
 
 @dataclass
@@ -130,6 +135,7 @@ def lib() -> C.CDLL:
         L.ccdb_fisher_information.argtypes = [_P, _P, C.c_int32, _P]
         L.ccdb_get_predictive_log_likelihood.argtypes = [_P, _P, _P]
         L.ccdb_get_predictive_estimates.argtypes = [_P, _P, _P]
+        L.ccdb_compute_mm_gradient_hessian.argtypes = [_P, _P, _P, _P]
         _lib = L
     return _lib
 
@@ -225,9 +231,11 @@ def _desc(d: CyclopsData, precision: int, keep: list) -> _FitDesc:
 def _mode_args(d: CyclopsData, a: ModeFindingArguments, keep: list) -> _ModeArgs:
     pt = _c(d.prior_type, np.int32)
     pv = _c(d.prior_var, np.float64)
-    keep += [pt, pv]
+    fx = None if a.fixed is None else np.ascontiguousarray(a.fixed, dtype=np.uint8)
+    keep += [pt, pv, fx]
     return _ModeArgs(_p(pt), _p(pv), a.convergence_type, a.tolerance, a.max_iterations,
-                     a.initial_bound, a.max_bound_count, int(a.per_coordinate), int(a.strategy))
+                     a.initial_bound, a.max_bound_count, int(a.per_coordinate), int(a.strategy),
+                     int(a.algorithm), int(a.kkt_swindle), _p(fx))
 
 
 class Fit:
@@ -305,6 +313,14 @@ class Fit:
         out = np.zeros((len(idx), len(idx)))
         _check(lib().ccdb_fisher_information(self.h, _p(idx), len(idx), _p(out)))
         return out
+
+    def compute_mm_gradient_and_hessian(self, fixed: Optional[np.ndarray] = None):
+        """ModelSpecifics::computeMMGradientAndHessian: the MM algorithm's
+        gradient and Hessian bound of every column on the current state."""
+        fx = _c(fixed, np.uint8)
+        g, h = np.zeros(self.d.J), np.zeros(self.d.J)
+        _check(lib().ccdb_compute_mm_gradient_hessian(self.h, _p(fx), _p(g), _p(h)))
+        return g, h
 
     def get_predictive_log_likelihood(self, weights: np.ndarray) -> float:
         """getNewPredictiveLogLikelihood (CyclicCoordinateDescent.cpp:319-355)

@@ -136,6 +136,15 @@ int ccdb_fisher_information(ccdb_fit* f, const int32_t* indices, int32_t n, doub
  * AbstractModelSpecifics.h:106).  The Cox model takes its risk sets under the
  * held-out weights and then returns to the fit's own weights. */
 int ccdb_get_predictive_log_likelihood(ccdb_fit* f, const double* weights, double* out);
+/* The MM algorithm's all-coordinate gradient and Hessian bound on the current
+ * state (ModelSpecifics::computeMMGradientAndHessian, ModelSpecifics.hpp:776-889,
+ * AbstractModelSpecifics.h:66): gradient[J], hessian[J]; columns with
+ * fixed[j] != 0 give (0, 0) (fixed may be NULL).  Conditional logistic,
+ * conditional Poisson and Cox fits; others return CCDB_ERR_UNSUPPORTED (the
+ * reference's Poisson increment throws, and its MM set-up reads stratum ids that
+ * unstratified data does not have). */
+int ccdb_compute_mm_gradient_hessian(ccdb_fit* f, const uint8_t* fixed, double* gradient,
+                                     double* hessian);
 /* predictEstimate of each row's xBeta into y[K]: LR exp(xb)/(exp(xb)+1),
  * Poisson exp(xb), conditional and Cox models xb (getPredictiveEstimates,
  * ModelSpecifics.hpp:692-705, AbstractModelSpecifics.h:108).  With weights
@@ -159,7 +168,19 @@ typedef struct {
                                   dependency levels) or _SPECULATIVE (batched gradients,
                                   restart after each nonzero step); other models always
                                   use speculative batches */
+    int32_t algorithm;         /* AlgorithmType (Types.h:149-153): CCDB_ALGORITHM_CCD (0,
+                                  default) or CCDB_ALGORITHM_MM (findMode's MM cycle,
+                                  CyclicCoordinateDescent.cpp:974-1001; conditional logistic,
+                                  conditional Poisson and Cox fits only) */
+    int32_t use_kkt_swindle;   /* ModeFindingArguments::useKktSwindle: 1 runs
+                                  CyclicCoordinateDescent::kktSwindle (.cpp:636-826) when
+                                  some column has a Laplace prior */
+    const uint8_t* fixed;      /* J flags or NULL: setFixedBeta for every column (the
+                                  offset column stays fixed); NULL keeps the fit's set */
 } ccdb_mode_args;
+
+#define CCDB_ALGORITHM_CCD 0
+#define CCDB_ALGORITHM_MM 1
 
 #define CCDB_SWEEP_AUTO 0
 #define CCDB_SWEEP_LEVELS 1

@@ -560,6 +560,240 @@ static void find_mode(Orc* o, int max_iter, int conv, double eps) {
     o->last_iter = iteration;
 }
 
+/* computeMMGradientAndHessianImpl, MS.hpp:848-889, with the model's
+ * incrementMMGradientAndHessian: Logistic MS.h:570-583 and Survival MS.h:499-516
+ * (the same expressions; weight = hNWeight and denominator = denomPid of the
+ * row's group).  PoissonRegression's throws (MS.h:1545-1552): returns -1. */
+static int mm_gradient_hessian(Orc* o, int j, double* og, double* oh) {
+    if (o->model == MT_POISSON) return -1;
+    double gradient = 0.0, hessian = 0.0;
+    const int ind = col_is_indicator(o, j);
+    const int64_t n = col_len(o, j);
+    for (int64_t p = 0; p < n; ++p) {
+        const int64_t k = col_row(o, j, p);
+        const int g = group_of(o, k);
+        const double weight = o->nw[g], e = o->e[k], d = o->denom[g];
+        if (ind) {
+            gradient += weight * e / d;
+            hessian += weight * e / d;
+        } else {
+            const double x = col_val(o, j, p);
+            gradient += weight * e * x / d;
+            hessian += weight * e * x * x / d;
+        }
+    }
+    gradient -= o->xjy[j]; /* precomputeGradient */
+    *og = gradient;
+    *oh = hessian;
+    return 0;
+}
+
+static void find_mode_prepare(Orc* o) {
+    if (!o->valid_weights || o->touched_y) {
+        set_weights_ms(o);
+        fixed_ll(o);
+        compute_xjy(o);
+        o->valid_weights = 1;
+        o->touched_y = 0;
+    }
+    if (!o->xb_known) {
+        compute_xbeta(o);
+        o->xb_known = 1;
+        o->suff_known = 0;
+    }
+    if (!o->suff_known) {
+        remaining_statistics(o);
+        o->suff_known = 1;
+    }
+    for (int j = 0; j < o->J; ++j) o->hdelta[j] = o->bound; /* resetBounds */
+}
+
+/* findMode with AlgorithmType::MM, CCD.cpp:957-1001 and the MM check
+ * :1032-1048: every free coordinate's step from one all-coordinate (g, h)
+ * (mmUpdateAllBeta, CCD.cpp:1354-1391; no applyBounds), then xBeta from beta
+ * (ModelSpecifics::computeXBeta, MS.hpp:313-361) and the remaining
+ * statistics.  A log posterior that decreases raises "Non-increasing!"
+ * (returned as -1 with the message). */
+static int find_mode_mm(Orc* o, int max_iter, int conv, double eps, const char** msg) {
+    if (o->model == MT_POISSON) {
+        *msg = "Not model-specific";
+        return -1;
+    }
+    if (is_indep(o)) {
+        /* initializeMM (MS.hpp:181-257) reduces each column by stratum through
+         * ModelData::binaryReductionByStratum (ModelData.h:606-660), which
+         * indexes the stratum ids that unstratified data does not have: the
+         * reference reads out of bounds there. */
+        *msg = "the MM algorithm needs stratified data";
+        return -1;
+    }
+    find_mode_prepare(o);
+    int iteration = 0, done = 0;
+    double last = objective(o, conv), last_lp = -10E10;
+    double* delta = (double*)malloc(sizeof(double) * o->J);
+    while (!done) {
+        for (int j = 0; j < o->J; ++j) {
+            delta[j] = 0.0;
+            if (o->fix[j]) continue;
+            double g, h;
+            if (mm_gradient_hessian(o, j, &g, &h) != 0) {
+                free(delta);
+                *msg = "Not model-specific";
+                return -1;
+            }
+            if (h < 0.0) {
+                g = 0.0;
+                h = 0.0;
+            }
+            delta[j] = prior_delta(o, j, g, h);
+        }
+        for (int j = 0; j < o->J; ++j)
+            if (!o->fix[j] && delta[j] != 0.0) o->beta[j] += delta[j];
+        compute_xbeta(o);
+        remaining_statistics(o);
+        iteration++;
+        const double lp = log_likelihood(o) + log_prior(o);
+        if (iteration > 1 && lp - last_lp < 0.0) {
+            free(delta);
+            *msg = "Non-increasing!";
+            return -1;
+        }
+        last_lp = lp;
+        double cur = objective(o, conv), c;
+        int ill = 0;
+        if (cur != cur) {
+            c = 0.0;
+            ill = 1;
+        } else {
+            c = fabs(cur - last) / (fabs(cur) + 1.0);
+        }
+        last = cur;
+        if (eps > 0 && c < eps) {
+            o->last_flag = ill ? R_ILLCONDITIONED : R_SUCCESS;
+            done = 1;
+        } else if (iteration == max_iter) {
+            o->last_flag = R_MAX_ITERATIONS;
+            done = 1;
+        }
+    }
+    o->last_iter = iteration;
+    free(delta);
+    return 0;
+}
+
+static int find_mode_alg(Orc* o, int max_iter, int conv, double eps, int algorithm, const char** msg) {
+    if (algorithm == 1) return find_mode_mm(o, max_iter, conv, eps, msg);
+    find_mode(o, max_iter, conv, eps);
+    return 0;
+}
+
+/* One KKT score: |gradient| of column idx at the current state, and whether
+ * the column is forced into the active set (computeKktConditions,
+ * CCD.cpp:809-826). */
+typedef struct {
+    int idx;
+    double score;
+    int force;
+} Score;
+
+/* std::list::sort with computeKktConditions' comparator (CCD.cpp:819-825):
+ * forced entries first, then decreasing score; a stable merge, as list::sort. */
+static void kkt_sort(Score* a, int n) {
+    for (int i = 1; i < n; ++i) { /* insertion sort: stable */
+        Score t = a[i];
+        int j = i - 1;
+        while (j >= 0) {
+            const int before = (t.force == a[j].force) ? (a[j].score < t.score) : t.force;
+            if (!before) break;
+            a[j + 1] = a[j];
+            --j;
+        }
+        a[j + 1] = t;
+    }
+}
+
+/* CyclicCoordinateDescent::kktSwindle, CCD.cpp:636-807: Laplace columns start
+ * inactive at beta = 0 (the intercept and non-Laplace columns are active);
+ * findMode over the active set; the inactive columns whose |gradient| exceeds
+ * their Laplace lambda (getKktBoundary, CP.h:235-238) move into the active
+ * set, largest first, until every inactive column satisfies the condition. */
+static int kkt_swindle(Orc* o, int max_iter, int conv, double eps, int algorithm, const char** msg) {
+    check_lazy(o);
+    const int J = o->J;
+    int has_intercept = 0;
+    for (int j = 0; j < J; ++j) has_intercept |= (o->fmt[j] == F_INTERCEPT);
+    const int intercept = has_intercept ? (o->offset_col0 ? 1 : 0) : -1;
+    const size_t cap = (size_t)(J > 0 ? J : 0) + 1;
+    uint8_t* exclude = (uint8_t*)malloc(cap);
+    Score* active = (Score*)malloc(sizeof(Score) * cap);
+    Score* inactive = (Score*)malloc(sizeof(Score) * cap);
+    int na = 0, ni = 0;
+    for (int j = 0; j < J; ++j) {
+        exclude[j] = o->fix[j];
+        if (o->fix[j]) continue;
+        Score s = {j, 0.0, 0};
+        if (j == intercept || o->prior_type[j] != 1) {
+            s.force = 1;
+            active[na++] = s;
+        } else {
+            inactive[ni++] = s;
+        }
+    }
+    int done = 0, count = 1, rc = 0;
+    while (!done) {
+        for (int q = 0; q < ni; ++q) { /* setBeta(i, 0.0): an incremental step of -beta */
+            const int i = inactive[q].idx;
+            if (o->beta[i] != 0.0) {
+                const double delta = 0.0 - o->beta[i];
+                o->beta[i] += delta;
+                update_xbeta_ms(o, i, delta);
+            }
+        }
+        o->last_flag = R_SUCCESS;
+        if (na > 0) { /* findMode(begin(activeSet), end(activeSet)), CCD.cpp:621-634 */
+            for (int j = 0; j < J; ++j) o->fix[j] = 1;
+            for (int q = 0; q < na; ++q) o->fix[active[q].idx] = 0;
+            rc = find_mode_alg(o, max_iter, conv, eps, algorithm, msg);
+            if (rc != 0) break;
+        }
+        if (ni == 0 || o->last_flag != R_SUCCESS) {
+            done = 1;
+        } else if (count == max_iter) {
+            o->last_flag = R_MAX_ITERATIONS;
+            done = 1;
+        } else {
+            for (int q = 0; q < ni; ++q) {
+                double g, h;
+                numerator_for_gradient(o, inactive[q].idx);
+                gradient_hessian(o, inactive[q].idx, &g, &h);
+                inactive[q].score = fabs(g);
+            }
+            kkt_sort(inactive, ni);
+            int satisfied = 1;
+            for (int q = 0; q < ni; ++q)
+                if (!(inactive[q].score <= sqrt(2.0 / o->prior_var[inactive[q].idx]))) satisfied = 0;
+            if (satisfied) {
+                done = 1;
+            } else {
+                int moved = 0;
+                while (moved < ni &&
+                       !(inactive[moved].score <= sqrt(2.0 / o->prior_var[inactive[moved].idx]))) {
+                    active[na++] = inactive[moved];
+                    ++moved;
+                }
+                memmove(inactive, inactive + moved, sizeof(Score) * (ni - moved));
+                ni -= moved;
+            }
+        }
+        ++count;
+    }
+    for (int j = 0; j < J; ++j) o->fix[j] = exclude[j]; /* restore fixBeta */
+    free(exclude);
+    free(active);
+    free(inactive);
+    return rc;
+}
+
 static void set_err(char* err, int errlen, const char* msg) {
     if (err && errlen > 0) {
         strncpy(err, msg, errlen - 1);
@@ -716,17 +950,28 @@ int orc_set_beta(void* hp, const double* beta) { /* CCD.cpp:700-708 */
 
 /* CyclicCoordinateDescent::update, CCD.cpp:586-615 (resetBeta :256-264) */
 int orc_fit(void* hp, int conv_type, double tol, int max_iter, double initial_bound,
-            int max_bound_count, double* beta_out, double* ll_out, int* iters_out, int* flag_out,
-            char* err, int errlen) {
+            int max_bound_count, int algorithm, int use_kkt, const uint8_t* fixed, double* beta_out,
+            double* ll_out, int* iters_out, int* flag_out, char* err, int errlen) {
     Orc* o = (Orc*)hp;
     if (conv_type < C_GRADIENT || conv_type > C_MITTAL) {
         set_err(err, errlen, "unsupported convergence type");
         return -1;
     }
+    if (fixed) /* setFixedBeta per column; the offset stays fixed (CCD.cpp:218-221) */
+        for (int j = 0; j < o->J; ++j) o->fix[j] = (fixed[j] != 0) || (o->offset_col0 && j == 0);
     o->bound = initial_bound;
     int count = 0;
     for (;;) {
-        find_mode(o, max_iter, conv_type, tol);
+        const char* msg = NULL;
+        /* update: kktSwindle when asked and a Laplace prior supports it (CCD.cpp:598-603) */
+        int any_laplace = 0;
+        for (int j = 0; j < o->J; ++j) any_laplace |= (o->prior_type[j] == 1);
+        const int rc = (use_kkt && any_laplace) ? kkt_swindle(o, max_iter, conv_type, tol, algorithm, &msg)
+                                                : find_mode_alg(o, max_iter, conv_type, tol, algorithm, &msg);
+        if (rc != 0) {
+            set_err(err, errlen, msg ? msg : "mode finding failed");
+            return -1;
+        }
         ++count;
         if (o->last_flag == R_ILLCONDITIONED && count < max_bound_count) {
             o->bound /= 10.0;

@@ -24,9 +24,11 @@ void* orc_create(int model_type, int fp32_unused, int64_t K, int J, const double
 void orc_destroy(void* h);
 int orc_set_weights(void* h, const double* w);
 int orc_set_beta(void* h, const double* beta);
+/* algorithm: 0 CCD, 1 MM (AlgorithmType, Types.h:149-153); use_kkt: the KKT
+ * swindle (ModeFindingArguments::useKktSwindle); fixed: J flags or NULL. */
 int orc_fit(void* h, int conv_type, double tol, int max_iter, double initial_bound,
-            int max_bound_count, double* beta_out, double* ll_out, int* iters_out, int* flag_out,
-            char* err, int errlen);
+            int max_bound_count, int algorithm, int use_kkt, const uint8_t* fixed, double* beta_out,
+            double* ll_out, int* iters_out, int* flag_out, char* err, int errlen);
 int orc_grad_hess(void* h, int j, double* g, double* hs);
 int orc_update_beta(void* h, int j, double delta);
 int orc_loglik(void* h, double* ll);

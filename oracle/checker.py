@@ -63,7 +63,7 @@ class _Engine:
                 C.c_int, _P, _P, C.c_char_p, C.c_int]
             getattr(lib, p + "destroy").argtypes = [_P]
             getattr(lib, p + "fit").argtypes = [_P, C.c_int, C.c_double, C.c_int, C.c_double, C.c_int,
-                                                _P, _P, _P, _P, C.c_char_p, C.c_int]
+                                                C.c_int, C.c_int, _P, _P, _P, _P, _P, C.c_char_p, C.c_int]
             getattr(lib, p + "grad_hess").argtypes = [_P, C.c_int, _P, _P]
             getattr(lib, p + "update_beta").argtypes = [_P, C.c_int, C.c_double]
             for name in ("set_weights", "set_beta", "loglik", "log_prior", "get_beta", "get_xbeta"):
@@ -127,14 +127,18 @@ class _Engine:
         self._f("set_beta")(self.h, _ptr(beta))
 
     def fit(self, conv_type: int = 0, tol: float = 1e-6, max_iter: int = 1000,
-            initial_bound: float = 2.0, max_bound_count: int = 5):
+            initial_bound: float = 2.0, max_bound_count: int = 5, algorithm: int = 0,
+            kkt_swindle: bool = False, fixed: Optional[np.ndarray] = None):
+        """CyclicCoordinateDescent::update; algorithm 0 = CCD, 1 = MM."""
         beta = np.zeros(self.d.J)
         ll = C.c_double()
         it = C.c_int()
         fl = C.c_int()
         err = C.create_string_buffer(512)
+        fx = None if fixed is None else np.ascontiguousarray(fixed, np.uint8)
         rc = self._f("fit")(self.h, conv_type, tol, max_iter, initial_bound, max_bound_count,
-                            _ptr(beta), C.byref(ll), C.byref(it), C.byref(fl), err, 512)
+                            algorithm, int(kkt_swindle), _ptr(fx), _ptr(beta), C.byref(ll), C.byref(it),
+                            C.byref(fl), err, 512)
         if rc != 0:
             raise RuntimeError(err.value.decode())
         return {"beta": beta, "loglik": ll.value, "iterations": it.value, "flag": fl.value}

@@ -234,10 +234,12 @@ int ref_set_beta(void* hp, const double* beta) {
     return 0;
 }
 
-// Full mode finding through CyclicCoordinateDescent::update.
+// Full mode finding through CyclicCoordinateDescent::update.  algorithm:
+// AlgorithmType (0 CCD, 1 MM); use_kkt: ModeFindingArguments::useKktSwindle;
+// fixed: J flags for setFixedBeta, or NULL (the offset stays fixed either way).
 int ref_fit(void* hp, int conv_type, double tol, int max_iter, double initial_bound,
-            int max_bound_count, double* beta_out, double* ll_out, int* iters_out, int* flag_out,
-            char* err, int errlen) {
+            int max_bound_count, int algorithm, int use_kkt, const uint8_t* fixed, double* beta_out,
+            double* ll_out, int* iters_out, int* flag_out, char* err, int errlen) {
     auto h = static_cast<RefHandle*>(hp);
     try {
         ModeFindingArguments a;
@@ -246,6 +248,12 @@ int ref_fit(void* hp, int conv_type, double tol, int max_iter, double initial_bo
         a.convergenceType = conv_type;
         a.initialBound = initial_bound;
         a.maxBoundCount = max_bound_count;
+        a.algorithmType = algorithm == 1 ? AlgorithmType::MM : AlgorithmType::CCD;
+        a.useKktSwindle = use_kkt != 0;
+        if (fixed) {
+            const bool offset = h->data->getHasOffsetCovariate();
+            for (int j = 0; j < h->J; ++j) h->ccd->setFixedBeta(j, fixed[j] != 0 || (offset && j == 0));
+        }
         h->ccd->update(a);
         for (int j = 0; j < h->J; ++j) beta_out[j] = h->ccd->getBeta(j);
         *ll_out = h->ccd->getLogLikelihood();
@@ -254,6 +262,10 @@ int ref_fit(void* hp, int conv_type, double tol, int max_iter, double initial_bo
         return 0;
     } catch (const std::exception& e) {
         set_err(err, errlen, e.what());
+        return -1;
+    } catch (std::logic_error* e) {  // the reference throws some errors by pointer
+        set_err(err, errlen, e->what());
+        delete e;
         return -1;
     }
 }
