@@ -58,10 +58,13 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=200,
                     help="serve: requests in the replayed stream")
     ap.add_argument("--serve-slots", type=int, default=8, help="serve: concurrent fits")
-    ap.add_argument("--workload", choices=["poisson_offset", "cv_grid", "cox_breslow", "serve"],
+    ap.add_argument("--workload", choices=["poisson_offset", "cv_grid", "cox_breslow", "serve",
+                                           "kkt_l1", "mm_clr", "fisher_l1"],
                     default="poisson_offset",
                     help="poisson_offset: plain fits (default); cv_grid: 10 folds x 20 Laplace "
-                         "variances = 200 logistic fits over one shared 5e5 x 2e4 matrix")
+                         "variances = 200 logistic fits over one shared 5e5 x 2e4 matrix; "
+                         "kkt_l1 / mm_clr / fisher_l1: the mode-finding variants and the Fisher "
+                         "information (see variant_problem)")
     ap.add_argument("--plain-sample", type=int, default=3,
                     help="cv_grid: instances also fitted one at a time by the plain solver")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed",
@@ -72,6 +75,8 @@ def parse():
                     help="cv_grid: covariate columns (fewer for short profiling captures)")
     ap.add_argument("--fp64-check", type=int, default=4,
                     help="cv_grid, mixed: instances also fitted by the FP64 engine to report the error")
+    ap.add_argument("--strategy", choices=["auto", "levels", "speculative"], default="auto",
+                    help="sweep strategy of the independent-row engine (CCDB_SWEEP_*)")
     ap.add_argument("--trace", default=None,
                     help="write a per-level timestamp trace of the last timed findMode's first "
                          "sweep to this file (summarise with python -m ccd_b200.trace)")
@@ -714,13 +719,289 @@ def serve_cpu_sample(stream, n: int = 40):
             "sample": f"first {len(sub)} requests of the same trace, FIFO over {cores} host threads"}
 
 
+# ------------------------------------------------------------------ variants
+VARIANTS = ("kkt_l1", "mm_clr", "fisher_l1")
+STRATEGIES = {"auto": 0, "levels": 1, "speculative": 2}
+
+
+def variant_problem(name: str):
+    """kkt_l1: L1 logistic regression on the cross-validation grid's shared
+    matrix (500,000 rows x 20,000 indicator covariates at density 0.005, ~5e7
+    nonzeros, intercept) with Laplace variance 0.01 -- a sparse fit, the case
+    the swindle is for; mm_clr: conditional logistic regression, 50,000 matched
+    sets of 2-11 rows (~325,000 rows), 5,000 indicator covariates at density
+    0.01, Laplace variance 0.1; fisher_l1: the 10,000 x 1,000 L1 logistic
+    problem (density 0.01, intercept, Laplace variance 0.1), information over
+    all 1,001 columns at its mode."""
+    if name == "mm_clr":
+        return synthetic.conditional_logistic(seed=5, n_sets=50_000, P=5_000)
+    if name == "kkt_l1":
+        d = synthetic.logistic_cv(seed=4)
+        d.prior_var[:] = 0.01
+        return d
+    return synthetic.logistic_l1(seed=1)
+
+
+def variant_fit_kw(name: str) -> dict:
+    """Oracle / reference fit() keywords and the matching C ABI mode arguments."""
+    if name == "kkt_l1":
+        return dict(kkt_swindle=True)
+    if name == "mm_clr":
+        return dict(algorithm=1)
+    return {}
+
+
+def variant_config(name: str, d) -> dict:
+    from ccd_b200.data import MITTAL  # noqa: F401 (documented below)
+    base = {"workload": name, "rows": d.K, "columns": d.J, "nnz": d.nnz, "precision": "fp64",
+            "prior": f"laplace({float(d.prior_var[-1]):g}), none on the intercept",
+            "convergence": "relative log-likelihood change (mittal), tol 1e-6",
+            "l2": "flushed between timed steps (512 MiB device write)"}
+    if name == "kkt_l1":
+        return {**base, "model": "logistic", "step": "one converged KKT-swindle fit from a cold start"}
+    if name == "mm_clr":
+        return {**base, "model": "conditional logistic", "strata": int(d.stratum.max()) + 1,
+                "step": "one converged MM fit from a cold start"}
+    return {**base, "model": "logistic", "step": "Fisher information over every coefficient column "
+                                                 "at the fitted mode (n = columns)"}
+
+
+def variant_unit(name: str) -> str:
+    return "Fisher entries/s" if name == "fisher_l1" else "fits/s"
+
+
+def fisher_cols(d) -> np.ndarray:
+    return np.arange(1 if d.offset_col0 else 0, d.J, dtype=np.int32)
+
+
+def fisher_bytes(d, cols) -> float:
+    """Algorithmic bytes of one Fisher call: per pass of 8 columns, the scatter
+    reads each of its columns' entries (row id 4 B where stored, value 8 B where
+    stored) and writes an 8-byte table slot; the gather reads, per entry of every
+    column at or after the pass, the row id / value, a 64-byte table row and
+    the 32-byte row state."""
+    n = len(cols)
+    ent = np.array([d.K if d.fmt[j] in (DENSE, INTERCEPT) else d.col_start[j + 1] - d.col_start[j]
+                    for j in cols], dtype=np.float64)
+    per = np.array([(4 if d.fmt[j] in (SPARSE, INDICATOR) else 0) + (8 if d.fmt[j] in (SPARSE, DENSE) else 0)
+                    for j in cols], dtype=np.float64)
+    suffix = np.cumsum((ent * (per + 64 + 32))[::-1])[::-1]
+    total = 0.0
+    for p0 in range(0, n, 8):
+        total += float(np.sum(ent[p0:p0 + 8] * (per[p0:p0 + 8] + 8))) + float(suffix[p0])
+    return total
+
+
+def mm_cycle_bytes(d) -> float:
+    """Algorithmic bytes of one MM cycle's bound kernel: per entry the row id
+    (4 B) and value (8 B where stored), {xBeta, e} (16 B), the group (4 B), the
+    group's events and denominator (16 B)."""
+    cnt = np.diff(d.col_start).astype(np.float64)
+    val = np.where((d.fmt == SPARSE) | (d.fmt == DENSE), 8.0, 0.0)
+    return float(np.sum(cnt * (4 + val + 16 + 4 + 16)))
+
+
+def variant_reference_time(eng, name: str, d, cols) -> float:
+    """Seconds of one step of the reference CPU engine (single thread)."""
+    from ccd_b200.data import MITTAL
+    if name == "fisher_l1":
+        t0 = time.perf_counter()
+        eng.fisher_information(cols)
+        return time.perf_counter() - t0
+    eng.set_beta(cold_beta(d))
+    t0 = time.perf_counter()
+    eng.fit(MITTAL, 1e-6, **variant_fit_kw(name))
+    return time.perf_counter() - t0
+
+
+def variant_reference_engine(name: str, d):
+    from ccd_b200.data import MITTAL
+    from oracle import checker
+    eng_cls = checker.best_engine()
+    kind = "reference" if eng_cls is checker.ReferenceEngine else "port"
+    eng = eng_cls(d)
+    if name == "fisher_l1":
+        eng.fit(MITTAL, 1e-6)  # the state the information is taken at
+    return eng, kind
+
+
+def variant_units_per_step(name: str, d) -> float:
+    if name == "fisher_l1":
+        n = len(fisher_cols(d))
+        return n * (n + 1) / 2.0
+    return 1.0
+
+
+def run_variant_reference(args, world, rank):
+    if rank != 0:
+        return
+    d = variant_problem(args.workload)
+    cols = fisher_cols(d)
+    eng, kind = variant_reference_engine(args.workload, d)
+    times = []
+    for i in range(args.warmup + args.steps):
+        dt = variant_reference_time(eng, args.workload, d, cols)
+        if i >= args.warmup:
+            times.append(dt)
+    eng.close()
+    total = float(np.sum(times))
+    unit = variant_unit(args.workload)
+    v = args.steps * variant_units_per_step(args.workload, d) / total
+    line = {
+        "impl": "reference", "metric": unit, "value": v, "unit": unit, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded PCG64)", "config": variant_config(args.workload, d),
+        "cpu_baseline": {"value": v, "unit": unit, "cores": 1, "kind": kind,
+                         "sample": "the whole step per step, single thread"},
+        "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_variant(args, world, rank, local):
+    """The KKT swindle, the MM algorithm or the Fisher information; each rank
+    runs its own replica (these fits do not shard)."""
+    import torch
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import torch.distributed as tdist
+    from ccd_b200 import native
+    from ccd_b200.data import MITTAL
+    name = args.workload
+    d = variant_problem(name)
+    cols = fisher_cols(d)
+    ctx = native.Context(local)
+    m = native.Matrix(ctx, d)
+    f = native.Fit(ctx, m, d)
+    kw = variant_fit_kw(name)
+    margs = native.ModeFindingArguments(convergence_type=MITTAL, tolerance=1e-6,
+                                        max_iterations=args.max_sweeps,
+                                        algorithm=kw.get("algorithm", 0),
+                                        kkt_swindle=kw.get("kkt_swindle", False),
+                                        strategy=STRATEGIES[args.strategy])
+    cold = cold_beta(d)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    units = variant_units_per_step(name, d)
+    if name == "fisher_l1":
+        f.set_beta(cold)
+        fitted = f.find_mode(margs)
+
+    def one_step():
+        """Device seconds, launches and cycles of one step."""
+        if name == "fisher_l1":
+            f.compute_fisher_information(cols)
+            return f.last_call_seconds(), 2 * ((len(cols) + 7) // 8), 1
+        f.set_beta(cold)
+        r = f.find_mode(margs)
+        return r.device_seconds, r.kernel_launches, r.iterations
+
+    for _ in range(args.warmup):
+        one_step()
+    clocks = Clocks(local)
+    if world > 1:
+        tdist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    dev_t, launches, cycles = 0.0, 0, 0
+    for _ in range(args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t, nl, it = one_step()
+        dev_t += t
+        launches += nl
+        cycles += it
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+
+    # end to end from host buffers: the one-call fit (upload, fit, beta back) or
+    # the Fisher call with its index upload and n x n copy back, host-timed
+    if name == "fisher_l1":
+        h2d, d2h = len(cols) * 4, len(cols) ** 2 * 8
+        e2e_t = 0.0
+        for _ in range(args.steps):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            f.compute_fisher_information(cols)
+            e2e_t += time.perf_counter() - t0
+    else:
+        def pinned(a):
+            return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+        from ccd_b200.data import CyclopsData
+        dp = CyclopsData(d.model_type, pinned(d.y), pinned(d.col_start), pinned(d.rows),
+                         pinned(d.val_start), pinned(d.vals), pinned(d.fmt), d.prior_type, d.prior_var,
+                         time=d.time, stratum=d.stratum, offset_col0=d.offset_col0)
+        h2d = sum(a.nbytes for a in (dp.y, dp.col_start, dp.rows, dp.val_start, dp.vals, dp.fmt))
+        d2h = d.J * 8
+        e2e_t = 0.0
+        for _ in range(args.steps):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            e2e_t += native.fit_model(ctx, dp, margs).device_seconds
+    mx = allreduce([dev_t, e2e_t], tdist.ReduceOp.MAX if world > 1 else None, world)
+    sm = allreduce([float(launches)], tdist.ReduceOp.SUM if world > 1 else None, world)
+    if rank == 0:
+        unit = variant_unit(name)
+        peak, peak_kind = read_peaks()
+        roofline = None
+        if name == "fisher_l1":
+            b = fisher_bytes(d, cols)
+            ach = b * args.steps / dev_t / 1e9
+            roofline = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                        "peak_source": peak_kind, "algorithmic_bytes_per_launch": b / (2 * ((len(cols) + 7) // 8)),
+                        "kernel": "fisher_scatter + fisher_gather passes (one call)", "traffic": None}
+        elif name == "mm_clr":
+            b = mm_cycle_bytes(d) * cycles
+            ach = b / dev_t / 1e9
+            roofline = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                        "peak_source": peak_kind, "algorithmic_bytes_per_launch": mm_cycle_bytes(d),
+                        "kernel": "mm_gh_kernel (bound of one cycle; timed over the whole fit)",
+                        "traffic": None}
+        line = {
+            "metric": unit, "value": world * args.steps * units / mx[0], "unit": unit, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * mx[0] / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded PCG64)",
+            "config": {**variant_config(name, d), "parallelism": f"replicas x{world}",
+                       "sweep_strategy": args.strategy},
+            "cycles_per_step": cycles / args.steps,
+            "e2e": {"value": world * args.steps * units / mx[1], "unit": unit,
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "roofline": roofline,
+            "gpu_launches": int(sm[0]),
+            "clocks": clk,
+        }
+        if name == "fisher_l1":
+            line["fitted"] = {"iterations": fitted.iterations, "return_flag": fitted.return_flag}
+        if world == 1 and not args.no_cpu_baseline:
+            eng, kind = variant_reference_engine(name, d)
+            t = variant_reference_time(eng, name, d, cols)
+            eng.close()
+            line["cpu_baseline"] = {"value": units / t, "unit": unit, "cores": 1, "kind": kind,
+                                    "sample": f"one whole step ({t:.2f} s), single thread"}
+        print(json.dumps(line), flush=True)
+    f.close()
+    m.close()
+    ctx.close()
+    if world > 1:
+        tdist.destroy_process_group()
+
+
 def main():
     global WORKLOAD
     args = parse()
     WORKLOAD = args.workload
     world, rank, local = dist_setup()
-    if args.impl == "reference":
+    if args.impl == "reference" and args.workload in VARIANTS:
+        run_variant_reference(args, world, rank)
+    elif args.impl == "reference":
         run_reference(args, world, rank)
+    elif args.workload in VARIANTS:
+        run_variant(args, world, rank, local)
     elif args.workload == "cv_grid":
         run_cv(args, world, rank, local)
     elif args.workload == "serve":

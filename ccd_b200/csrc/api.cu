@@ -1059,6 +1059,13 @@ int ccdb_get_predictive_estimates(ccdb_fit* f, const double* weights, double* y)
     });
 }
 
+int ccdb_get_last_call_seconds(const ccdb_fit* f, double* seconds) {
+    return guard([&] {
+        require(f && seconds, "NULL argument");
+        *seconds = f->last_call_seconds;
+    });
+}
+
 int ccdb_get_beta(ccdb_fit* f, double* out) {
     return guard([&] {
         require(f && out, "NULL argument");

@@ -130,6 +130,7 @@ struct Fit {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;    // around the sweep launches
     cudaEvent_t evc0 = nullptr, evc1 = nullptr;  // around a whole find_mode
     int64_t launches = 0;                        // engine kernels launched so far
+    double last_call_seconds = 0.0;              // device time of the last fisher_information passes
     std::unique_ptr<DevSchedule> sched;
     CoxDev cox;
 

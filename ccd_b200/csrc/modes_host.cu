@@ -172,6 +172,12 @@ void Fit::kkt_swindle(const ccdb_mode_args& a, double bound, int* flag, int* ite
         if (j == intercept || ptype_h[j] != 1) active.push_back({j, 0.0, true});
         else inactive.push_back({j, 0.0, false});
     }
+    // The active set's findMode runs the fused dependency-level sweep unless the
+    // caller chose a strategy: its columns are the ones that violated their KKT
+    // condition, so most of them move, and a fixed set that changes each pass
+    // costs one schedule build instead of a launch per nonzero step.
+    ccdb_mode_args inner = a;
+    if (inner.strategy == CCDB_SWEEP_AUTO) inner.strategy = CCDB_SWEEP_LEVELS;
     auto lambda = [&](int j) { return std::sqrt(2.0 / pvar_h[j]); };
     auto meets = [&](const Score& s) { return s.score <= lambda(s.idx); };
     try {
@@ -185,7 +191,7 @@ void Fit::kkt_swindle(const ccdb_mode_args& a, double bound, int* flag, int* ite
                 std::fill(fixed.begin(), fixed.end(), uint8_t(1));
                 for (const Score& s : active) fixed[s.idx] = 0;
                 float t = 0.f;
-                find_mode_once(a, bound, flag, iters, obj, &t);
+                find_mode_once(inner, bound, flag, iters, obj, &t);
                 *ms += t;
                 if (beta_dirty_host) {
                     download_beta();

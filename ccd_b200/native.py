@@ -136,6 +136,7 @@ def lib() -> C.CDLL:
         L.ccdb_get_predictive_log_likelihood.argtypes = [_P, _P, _P]
         L.ccdb_get_predictive_estimates.argtypes = [_P, _P, _P]
         L.ccdb_compute_mm_gradient_hessian.argtypes = [_P, _P, _P, _P]
+        L.ccdb_get_last_call_seconds.argtypes = [_P, _P]
         _lib = L
     return _lib
 
@@ -321,6 +322,12 @@ class Fit:
         g, h = np.zeros(self.d.J), np.zeros(self.d.J)
         _check(lib().ccdb_compute_mm_gradient_hessian(self.h, _p(fx), _p(g), _p(h)))
         return g, h
+
+    def last_call_seconds(self) -> float:
+        """Device time of the kernels of the last compute_fisher_information."""
+        v = C.c_double()
+        _check(lib().ccdb_get_last_call_seconds(self.h, C.byref(v)))
+        return v.value
 
     def get_predictive_log_likelihood(self, weights: np.ndarray) -> float:
         """getNewPredictiveLogLikelihood (CyclicCoordinateDescent.cpp:319-355)

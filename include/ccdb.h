@@ -281,6 +281,11 @@ int ccdb_column_gradient_hessian_noalloc(int32_t model_type, int32_t fmt, int64_
 
 /* --- inspection (no reference counterpart) ---------------------------------- */
 
+/* Device time (CUDA events on the fit's stream) of the kernels of the fit's last
+ * ccdb_fisher_information call, in seconds; copies to and from the host are
+ * outside it.  0 before any such call. */
+int ccdb_get_last_call_seconds(const ccdb_fit* f, double* seconds);
+
 /* Dependency level of every column in one fused sweep over this matrix
  * (independent-row models: columns conflict when they share a row).  Columns
  * on one level touch disjoint rows; running levels in order reproduces the
