@@ -1,0 +1,180 @@
+"""Known-answer fixtures from the reference's own R tests, read as text.
+
+    make -C oracle ref && python tests/golden/make_known_answers.py
+
+The reference's testthat files compare Cyclops with glm / coxph / clogit on
+small inline data sets.  R is not available here, so this script reads those
+data sets out of the test sources (and the CLR test's infert data from the
+reference's fixture file), builds the same design matrices, and records what
+the reference Cyclops engine (compiled from source) returns for them:
+coefficients, log-likelihood, the Fisher information at the mode and the
+predictions.  The tests check the oracle and the GPU against these fixtures,
+and the fixtures against an independent Newton solve of the same likelihood
+(the stand-in for the R gold packages).  Run only where the reference sources
+are present; the fixtures are committed.
+
+Data sources (paths within the reference project):
+  tests/testthat/test-smallBernoulli.R  binomial_bid / binomial_n / binomial_y
+  tests/testthat/test-smallPoisson.R    dobson: counts, outcome = gl(3,1,9), treatment = gl(3,3)
+  tests/testthat/test-smallCox.R        the inline `read.table(text = ...)` tables
+  inst/extdata/infert_ccd.txt           case ~ spontaneous + induced + strata(stratum)
+"""
+import os
+import re
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from ccd_b200.data import (DENSE, GRADIENT, INDICATOR, INTERCEPT, MODEL_CONDITIONAL_LOGISTIC,  # noqa: E402
+                           MODEL_COX, MODEL_LOGISTIC, MODEL_POISSON, PRIOR_NONE, SPARSE, CyclopsData,
+                           build_columns, cox_sort_order)
+from oracle.checker import ReferenceEngine  # noqa: E402
+
+REF = os.environ.get("CYCLOPS_REFERENCE", "/root/reference")
+TESTS = os.path.join(REF, "tests", "testthat")
+
+
+def r_vector(src: str, name: str) -> np.ndarray:
+    """The first `name <- c(...)` or `name = c(...)` numeric vector in R source."""
+    m = re.search(name + r"\s*(?:<-|=)\s*c\(([^)]*)\)", src)
+    return np.array([float(x) for x in m.group(1).split(",")])
+
+
+def r_gl(src: str, name: str) -> np.ndarray:
+    """`name = gl(n, k[, length])`: levels 1..n, each repeated k times, cycled."""
+    m = re.search(name + r"\s*(?:<-|=)\s*gl\((\d+)\s*,\s*(\d+)(?:\s*,\s*(\d+))?\)", src)
+    n, k = int(m.group(1)), int(m.group(2))
+    length = int(m.group(3)) if m.group(3) else n * k
+    base = np.repeat(np.arange(1, n + 1), k)
+    return np.resize(base, length)
+
+
+def r_tables(src: str):
+    """Every inline `read.table(header=T, sep = ",", text = "...")` table."""
+    out = []
+    for body in re.findall(r'read\.table\(header\s*=\s*T,\s*sep\s*=\s*",",\s*text\s*=\s*"(.*?)"\)', src, re.S):
+        lines = [ln.strip() for ln in body.strip().splitlines() if ln.strip()]
+        head = [h.strip() for h in lines[0].split(",")]
+        rows = np.array([[float(v) for v in ln.split(",")] for ln in lines[1:]])
+        out.append({h: rows[:, i] for i, h in enumerate(head)})
+    return out
+
+
+def dense_data(model, y, cols, fmts, stratum=None, time=None) -> CyclopsData:
+    """CyclopsData from dense covariate vectors; SPARSE / INDICATOR columns keep
+    their nonzero rows."""
+    K = len(y)
+    built = []
+    for x, f in zip(cols, fmts):
+        if f == INTERCEPT:
+            built.append((None, None))
+        elif f == DENSE:
+            built.append((None, np.asarray(x, np.float64)))
+        else:
+            r = np.nonzero(np.asarray(x) != 0)[0].astype(np.int32)
+            built.append((r, None if f == INDICATOR else np.asarray(x, np.float64)[r]))
+    cs, rows, vs, vals, fmt = build_columns(K, built, fmts)
+    J = len(fmts)
+    return CyclopsData(model, np.asarray(y, np.float64), cs, rows, vs, vals, fmt,
+                       np.full(J, PRIOR_NONE, np.int32), np.ones(J),
+                       time=None if time is None else np.asarray(time, np.float64),
+                       stratum=None if stratum is None else np.asarray(stratum, np.int64))
+
+
+def bernoulli(fmt):
+    src = open(os.path.join(TESTS, "test-smallBernoulli.R")).read()
+    bid, n, yy = (r_vector(src, "binomial_bid"), r_vector(src, "binomial_n"), r_vector(src, "binomial_y"))
+    # log(c(rep(bid, n - y), rep(bid, y))) and y = c(rep(0, sum(n - y)), rep(1, sum(y)))
+    log_bid = np.log(np.concatenate([np.repeat(bid, (n - yy).astype(int)), np.repeat(bid, yy.astype(int))]))
+    y = np.concatenate([np.zeros(int(np.sum(n - yy))), np.ones(int(np.sum(yy)))])
+    return dense_data(MODEL_LOGISTIC, y, [None, log_bid], [INTERCEPT, fmt])
+
+
+def dobson(fmt):
+    src = open(os.path.join(TESTS, "test-smallPoisson.R")).read()
+    counts = r_vector(src, "counts")
+    outcome, treatment = r_gl(src, "outcome"), r_gl(src, "treatment")
+    # treatment contrasts: intercept, outcome2, outcome3, treatment2, treatment3
+    cols = [None] + [(outcome == lv).astype(float) for lv in (2, 3)] + [(treatment == lv).astype(float) for lv in (2, 3)]
+    return dense_data(MODEL_POISSON, counts, cols, [INTERCEPT] + [fmt] * 4)
+
+
+def cox_tables():
+    src = open(os.path.join(TESTS, "test-smallCox.R")).read()
+    return r_tables(src)[:4]
+
+
+def cox(table, strata_x2=False):
+    """Surv(length, event) ~ x1 + x2, or ~ x1 + strata(x2); rows in the order the
+    R layer gives the engine (stratum, -time, event)."""
+    t, ev = table["length"], table["event"]
+    stratum = table["x2"].astype(np.int64) if strata_x2 else np.zeros(len(t), np.int64)
+    order = cox_sort_order(stratum, t, ev)
+    cols = [table["x1"][order]] + ([] if strata_x2 else [table["x2"][order]])
+    return dense_data(MODEL_COX, ev[order], cols, [DENSE] * len(cols), stratum=stratum[order], time=t[order])
+
+
+def infert():
+    """inst/extdata/infert_ccd.txt: `stratum y covariate:value ...` per row."""
+    rows = []
+    with open(os.path.join(REF, "inst", "extdata", "infert_ccd.txt")) as fh:
+        for line in fh:
+            if line.startswith("#") or not line.strip():
+                continue
+            parts = line.split()
+            x = {int(k): float(v) for k, v in (p.split(":") for p in parts[2:])}
+            rows.append((int(parts[0]), float(parts[1]), x.get(1, 0.0), x.get(2, 0.0)))
+    a = np.array(rows)
+    order = np.argsort(a[:, 0], kind="stable")
+    a = a[order]
+    return dense_data(MODEL_CONDITIONAL_LOGISTIC, a[:, 1], [a[:, 2], a[:, 3]], [DENSE, DENSE],
+                      stratum=a[:, 0].astype(np.int64))
+
+
+def problems():
+    out = {
+        "bernoulli_dense": (bernoulli(DENSE), None),
+        "bernoulli_sparse": (bernoulli(SPARSE), None),
+        "dobson_dense": (dobson(DENSE), None),
+        "dobson_indicator": (dobson(INDICATOR), None),
+        "dobson_fixed": (dobson(DENSE), np.array([0, 1, 0, 1, 0], np.uint8)),
+        "infert_clr": (infert(), None),
+    }
+    for i, name in enumerate(("cox_no_ties", "cox_time_ties", "cox_failure_ties", "cox_failure_ties_after")):
+        out[name] = (cox(cox_tables()[i]), None)
+    out["cox_strata"] = (cox(cox_tables()[0], strata_x2=True), None)
+    return out
+
+
+TOL = 1e-12  # on the gradient objective: converged far below the R tests' 1e-4
+
+
+def main():
+    for name, (d, fixed) in problems().items():
+        e = ReferenceEngine(d)
+        r = e.fit(GRADIENT, TOL, max_iter=10_000, fixed=fixed)
+        cols = np.array([j for j in range(d.J) if fixed is None or not fixed[j]], np.int32)
+        fisher = e.fisher_information(cols)
+        pred = e.predictive_estimates()
+        e.close()
+        arrays = dict(model_type=np.int32(d.model_type), y=d.y, col_start=d.col_start, rows=d.rows,
+                      val_start=d.val_start, vals=d.vals, fmt=d.fmt, prior_type=d.prior_type,
+                      prior_var=d.prior_var, offset_col0=np.int32(0), beta=r["beta"],
+                      loglik=np.float64(r["loglik"]), iterations=np.int32(r["iterations"]),
+                      flag=np.int32(r["flag"]), fisher_cols=cols, fisher=fisher, pred_est=pred)
+        if d.time is not None:
+            arrays["time"] = d.time
+        if d.stratum is not None:
+            arrays["stratum"] = d.stratum
+        if fixed is not None:
+            arrays["fixed"] = fixed
+        np.savez_compressed(os.path.join(HERE, "known_" + name + ".npz"), **arrays)
+        print(name, d.K, d.J, r["flag"], r["iterations"], np.round(r["beta"], 6), r["loglik"])
+
+
+if __name__ == "__main__":
+    main()

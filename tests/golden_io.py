@@ -12,7 +12,24 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 def case_names():
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if not os.path.basename(p).startswith("logistic_l1_"))
+                  if not os.path.basename(p).startswith(("logistic_l1_", "known_")))
+
+
+def known_names():
+    """Known-answer problems from the reference's R tests (make_known_answers.py)."""
+    return sorted(os.path.basename(p)[len("known_"):-4] for p in glob.glob(os.path.join(GOLDEN, "known_*.npz")))
+
+
+def load_known(name):
+    z = np.load(os.path.join(GOLDEN, "known_" + name + ".npz"))
+    d = CyclopsData(int(z["model_type"]), z["y"], z["col_start"], z["rows"], z["val_start"], z["vals"],
+                    z["fmt"], z["prior_type"], z["prior_var"],
+                    time=z["time"] if "time" in z else None,
+                    stratum=z["stratum"] if "stratum" in z else None)
+    want = {k: z[k] for k in ("beta", "fisher_cols", "fisher", "pred_est")}
+    want.update(loglik=float(z["loglik"]), iterations=int(z["iterations"]), flag=int(z["flag"]),
+                fixed=z["fixed"] if "fixed" in z else None)
+    return d, want
 
 
 def load_case(name):
