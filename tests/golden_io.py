@@ -26,9 +26,11 @@ def load_known(name):
                     z["fmt"], z["prior_type"], z["prior_var"],
                     time=z["time"] if "time" in z else None,
                     stratum=z["stratum"] if "stratum" in z else None)
-    want = {k: z[k] for k in ("beta", "fisher_cols", "fisher", "pred_est")}
-    want.update(loglik=float(z["loglik"]), iterations=int(z["iterations"]), flag=int(z["flag"]),
-                fixed=z["fixed"] if "fixed" in z else None)
+    want = {k: z[k] for k in ("beta", "fisher_cols", "pred_est")}
+    want.update(loglik=float(z["loglik"]), iterations=int(z["iterations"]), flag=int(z["flag"]))
+    for k in ("fixed", "weights", "heldout", "fisher"):  # optional
+        want[k] = z[k] if k in z else None
+    want["pred_ll"] = float(z["pred_ll"]) if "pred_ll" in z else None
     return d, want
 
 
