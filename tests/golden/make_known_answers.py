@@ -21,6 +21,8 @@ Data sources (paths within the reference project):
                                         weights against the subset fit, the Cox
                                         predictive log-likelihood on held-out rows
   inst/extdata/infert_ccd.txt           case ~ spontaneous + induced + strata(stratum)
+  inst/extdata/CCD_LOGISTIC_TEST_17var.txt with the SAS fit's 2 x log-likelihood that
+                                        tests/testthat/test-largeBernoulli.R quotes
 """
 import os
 import re
@@ -183,6 +185,27 @@ def infert():
                       stratum=a[:, 0].astype(np.int64))
 
 
+def large_bernoulli():
+    """CCD_LOGISTIC_TEST_17var.txt (`row_label y covariate:value ...`, intercept
+    added), and the published 2 x log-likelihood of its SAS fit quoted in
+    test-largeBernoulli.R."""
+    rows, ids = [], set()
+    with open(os.path.join(REF, "inst", "extdata", "CCD_LOGISTIC_TEST_17var.txt")) as fh:
+        for line in fh:
+            if line.startswith("#") or not line.strip():
+                continue
+            parts = line.split()
+            x = {int(k): float(v) for k, v in (p.split(":") for p in parts[2:])}
+            ids |= set(x)
+            rows.append((float(parts[1]), x))
+    ids = sorted(ids)
+    y = np.array([a for a, _ in rows])
+    cols = [None] + [np.array([x.get(c, 0.0) for _, x in rows]) for c in ids]
+    src = open(os.path.join(TESTS, "test-largeBernoulli.R")).read()
+    published = float(re.search(r"log_likelihood\s*\*\s*2\s*,\s*(-?[0-9.]+)", src).group(1))
+    return dense_data(MODEL_LOGISTIC, y, cols, [INTERCEPT] + [SPARSE] * len(ids)), published
+
+
 def problems():
     """name -> (data, fixed flags or None, weights or None, held-out weights or None)."""
     out = {
@@ -192,6 +215,7 @@ def problems():
         "dobson_indicator": (dobson(INDICATOR), None, None, None),
         "dobson_fixed": (dobson(DENSE), np.array([0, 1, 0, 1, 0], np.uint8), None, None),
         "infert_clr": (infert(), None, None, None),
+        "bernoulli_17var": (large_bernoulli()[0], None, None, None),
     }
     for i, name in enumerate(("cox_no_ties", "cox_time_ties", "cox_failure_ties", "cox_failure_ties_after")):
         out[name] = (cox(cox_tables()[i]), None, None, None)
@@ -257,6 +281,8 @@ def main():
         if held is not None:
             arrays["heldout"] = held
             arrays["pred_ll"] = np.float64(pred_ll)
+        if name == "bernoulli_17var":
+            arrays["published_2ll"] = np.float64(large_bernoulli()[1])
         if d.time is not None:
             arrays["time"] = d.time
         if d.stratum is not None:

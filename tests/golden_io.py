@@ -31,6 +31,7 @@ def load_known(name):
     for k in ("fixed", "weights", "heldout", "fisher"):  # optional
         want[k] = z[k] if k in z else None
     want["pred_ll"] = float(z["pred_ll"]) if "pred_ll" in z else None
+    want["published_2ll"] = float(z["published_2ll"]) if "published_2ll" in z else None
     return d, want
 
 

@@ -97,3 +97,11 @@ def test_cox_predictive_loglik_of_held_out_rows():
     _, want = load_known("coxw_predictive")
     _, gold = load_known("coxw_predictive_gold")
     assert abs(want["pred_ll"] - gold["loglik"]) <= 1e-10 * abs(gold["loglik"])
+
+
+def test_published_sas_fit():
+    """test-largeBernoulli.R quotes the SAS fit of CCD_LOGISTIC_TEST_17var.txt
+    (22,296 rows, 17 covariates + intercept) as 2 x log-likelihood, to the
+    three decimals it prints."""
+    _, want = load_known("bernoulli_17var")
+    assert abs(2 * want["loglik"] - want["published_2ll"]) <= 5e-4
