@@ -60,15 +60,27 @@ def normal_based_default_var(d: CyclopsData) -> float:
 
 
 def point_estimate(values) -> float:
-    v = np.asarray(values, dtype=np.float64)
-    v = v[v == v]
-    return float(v.sum() / v.size) if v.size else float("nan")
+    """Mean of the non-NaN values, summed in order (computePointEstimate,
+    AbstractCrossValidationDriver.cpp:250-261)."""
+    total, count = 0.0, 0
+    for x in values:
+        x = float(x)
+        if x == x:
+            total += x
+            count += 1
+    return total / count if count else float("nan")
 
 
 def st_dev(values, mean: float) -> float:
-    v = np.asarray(values, dtype=np.float64)
-    v = v[v == v]
-    return math.sqrt(float((v * v).sum()) / v.size - mean * mean) if v.size else float("nan")
+    """sqrt(mean of squares - mean^2) over the non-NaN values, summed in order
+    (computeStDev, AbstractCrossValidationDriver.cpp:263-276)."""
+    inner, count = 0.0, 0
+    for x in values:
+        x = float(x)
+        if x == x:
+            inner += x * x
+            count += 1
+    return math.sqrt(inner / count - mean * mean) if count else float("nan")
 
 
 def quadratic_log_fit(history: dict):

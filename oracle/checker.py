@@ -222,6 +222,33 @@ class ReferenceEngine(_Engine):
         return v.value
 
 
+    def cross_validate(self, auto_search: bool = True, fold: int = 10, grid_steps: int = 10,
+                       lower: float = 0.01, upper: float = 20.0, starting_variance: float = -1.0,
+                       seed: int = 123, conv_type: int = 0, tol: float = 1e-6, max_iter: int = 1000):
+        """CcdInterface::runCrossValidation with one thread and cold starts:
+        the reference selector's fold map, the grid (grid search), the drivers'
+        log, the selected variance and the refit there."""
+        lib = self.lib()
+        fn = lib.ref_cross_validate
+        fn.argtypes = [_P, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_long,
+                       C.c_int, C.c_double, C.c_int, _P, _P, _P, C.c_int, _P, _P, _P, _P, C.c_char_p,
+                       C.c_int, C.c_char_p, C.c_int]
+        row_fold = np.zeros(self.d.K, np.int32)
+        pts, vals = np.zeros(max(grid_steps, 1)), np.zeros(max(grid_steps, 1))
+        n = C.c_int()
+        var, ll = C.c_double(), C.c_double()
+        beta = np.zeros(self.d.J)
+        log = C.create_string_buffer(1 << 20)
+        err = C.create_string_buffer(512)
+        rc = fn(self.h, int(auto_search), fold, grid_steps, lower, upper, starting_variance, seed, conv_type,
+                tol, max_iter, _ptr(row_fold), _ptr(pts), _ptr(vals), len(pts), C.byref(n), C.byref(var),
+                _ptr(beta), C.byref(ll), log, 1 << 20, err, 512)
+        if rc != 0:
+            raise RuntimeError(err.value.decode())
+        return {"row_fold": row_fold, "points": pts[:n.value], "values": vals[:n.value], "variance": var.value,
+                "beta": beta, "loglik": ll.value, "log": log.value.decode()}
+
+
 class ReferenceOnB200Engine(ReferenceEngine):
     """The reference's own CyclicCoordinateDescent driving the B200 engine
     through ccd_b200/integration/B200ModelSpecifics.h (the drop-in)."""

@@ -24,6 +24,10 @@
 
 #include "ModelData.h"
 #include "CyclicCoordinateDescent.h"
+#include "CcdInterface.h"
+#include "drivers/AutoSearchCrossValidationDriver.h"
+#include "drivers/CrossValidationSelector.h"
+#include "drivers/GridSearchCrossValidationDriver.h"
 #include "priors/JointPrior.h"
 #include "priors/CovariatePrior.h"
 #ifdef CCDB_B200_ADAPTER
@@ -40,6 +44,20 @@ struct QuietLogger : loggers::ProgressLogger {
 };
 struct ThrowingErrors : loggers::ErrorHandler {
     void throwError(const std::ostringstream& s) override { throw std::runtime_error(s.str()); }
+};
+
+// Keeps every line the cross-validation drivers log (their per-step summaries).
+struct RecordingLogger : loggers::ProgressLogger {
+    std::string text;
+    void writeLine(const std::ostringstream& s) override { text += s.str() + "\n"; }
+    void yield() override {}
+};
+
+// The grid driver's evaluated points and values (protected members).
+struct GridDriver : GridSearchCrossValidationDriver {
+    using GridSearchCrossValidationDriver::GridSearchCrossValidationDriver;
+    const std::vector<double>& points() const { return gridPoint; }
+    const std::vector<double>& values() const { return gridValue; }
 };
 
 // Column format codes: the reference's FormatType (CompressedDataMatrix.h:36-38).
@@ -368,6 +386,83 @@ int ref_asymptotic_variance(void* hp, int i, int j, double* out, char* err, int 
         set_err(err, errlen, e->what());
         delete e;
         return -2;
+    } catch (const std::exception& e) {
+        set_err(err, errlen, e.what());
+        return -1;
+    }
+}
+
+// Cross-validation as CcdInterface::runCrossValidation (CcdInterface.cpp:731-790)
+// runs it: a CrossValidationSelector over the data's ids (by row for Cox, by
+// id otherwise, getDefaultSelectorTypeOrOverride :675-690), the auto-search or
+// grid driver, then resetForOptimal and the fit at the selected variance.
+// One thread and cold starts (resetCoefficients), so the run is deterministic.
+// row_fold_out[K]: the held-out fold of each row under the selector's first
+// permutation (the one every step reuses after reseed()).  Grid: points_out /
+// values_out receive the grid (n_points).  log_out receives the drivers' log.
+int ref_cross_validate(void* hp, int auto_search, int fold, int grid_steps, double lower, double upper,
+                       double starting_variance, long seed, int conv_type, double tol, int max_iter,
+                       int32_t* row_fold_out, double* points_out, double* values_out, int max_points,
+                       int* n_points, double* variance_out, double* beta_out, double* ll_out, char* log_out,
+                       int log_len, char* err, int errlen) {
+    auto h = static_cast<RefHandle*>(hp);
+    try {
+        CCDArguments args = CCDArguments();
+        args.threads = 1;
+        args.resetCoefficients = true;
+        args.seed = seed;
+        args.useHierarchy = false;
+        args.noiseLevel = SILENT;
+        args.useNormalPrior = false;
+        args.crossValidation.doCrossValidation = true;
+        args.crossValidation.useAutoSearchCV = auto_search != 0;
+        args.crossValidation.fold = fold;
+        args.crossValidation.foldToCompute = fold;
+        args.crossValidation.gridSteps = grid_steps;
+        args.crossValidation.lowerLimit = lower;
+        args.crossValidation.upperLimit = upper;
+        args.crossValidation.startingVariance = starting_variance;
+        args.modeFinding.tolerance = tol;
+        args.modeFinding.convergenceType = conv_type;
+        args.modeFinding.maxIterations = max_iter;
+        const SelectorType type = (h->data->getModelType() == ModelType::COX) ? SelectorType::BY_ROW
+                                                                               : SelectorType::BY_PID;
+        auto log = std::make_shared<RecordingLogger>();
+        CrossValidationSelector selector(fold, h->data->getPidVectorSTL(), type, seed, log, h->err, nullptr,
+                                         nullptr);
+        selector.reseed();
+        selector.permute();
+        std::vector<double> w;
+        for (int f = 0; f < fold; ++f) {
+            selector.getWeights(f, w);
+            for (int64_t k = 0; k < h->K; ++k)
+                if (w[k] == 0.0) row_fold_out[k] = f;
+        }
+        std::unique_ptr<AbstractCrossValidationDriver> driver;
+        GridDriver* grid = nullptr;
+        if (auto_search) {
+            driver.reset(new AutoSearchCrossValidationDriver(*h->data, args, log, h->err));
+        } else {
+            grid = new GridDriver(args, log, h->err);
+            driver.reset(grid);
+        }
+        driver->drive(*h->ccd, selector, args);
+        driver->resetForOptimal(*h->ccd, selector, args);
+        h->ccd->update(args.modeFinding);
+        *variance_out = h->ccd->getHyperprior()[0];
+        for (int j = 0; j < h->J; ++j) beta_out[j] = h->ccd->getBeta(j);
+        *ll_out = h->ccd->getLogLikelihood();
+        *n_points = 0;
+        if (grid) {
+            const int n = std::min<int>(max_points, (int)grid->points().size());
+            for (int i = 0; i < n; ++i) {
+                points_out[i] = grid->points()[i];
+                values_out[i] = grid->values()[i];
+            }
+            *n_points = n;
+        }
+        set_err(log_out, log_len, log->text.c_str());
+        return 0;
     } catch (const std::exception& e) {
         set_err(err, errlen, e.what());
         return -1;
