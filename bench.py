@@ -998,6 +998,12 @@ def main():
     world, rank, local = dist_setup()
     if args.impl == "reference" and args.workload in VARIANTS:
         run_variant_reference(args, world, rank)
+    elif args.impl == "reference" and args.workload in ("cv_grid", "serve"):
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "workload": args.workload, "unavailable":
+                              "no standalone reference arm for this workload: its CPU baseline needs the "
+                              "grid's sweep counts / the request trace of the GPU run and is reported as "
+                              "cpu_baseline in that run's line"}), flush=True)
     elif args.impl == "reference":
         run_reference(args, world, rank)
     elif args.workload in VARIANTS:
