@@ -1059,6 +1059,13 @@ int ccdb_get_predictive_estimates(ccdb_fit* f, const double* weights, double* y)
     });
 }
 
+int ccdb_set_fixed(ccdb_fit* f, const uint8_t* fixed) {
+    return guard([&] {
+        require(f && fixed, "NULL argument");
+        for (int j = 0; j < f->J; ++j) f->fixed[j] = (fixed[j] != 0 || (f->offset_col0 && j == 0)) ? 1 : 0;
+    });
+}
+
 int ccdb_get_last_call_seconds(const ccdb_fit* f, double* seconds) {
     return guard([&] {
         require(f && seconds, "NULL argument");

@@ -137,6 +137,7 @@ def lib() -> C.CDLL:
         L.ccdb_get_predictive_estimates.argtypes = [_P, _P, _P]
         L.ccdb_compute_mm_gradient_hessian.argtypes = [_P, _P, _P, _P]
         L.ccdb_get_last_call_seconds.argtypes = [_P, _P]
+        L.ccdb_set_fixed.argtypes = [_P, _P]
         _lib = L
     return _lib
 
@@ -322,6 +323,11 @@ class Fit:
         g, h = np.zeros(self.d.J), np.zeros(self.d.J)
         _check(lib().ccdb_compute_mm_gradient_hessian(self.h, _p(fx), _p(g), _p(h)))
         return g, h
+
+    def set_fixed(self, fixed: np.ndarray) -> None:
+        """setFixedBeta for every column (the offset stays fixed)."""
+        fx = _c(fixed, np.uint8)
+        _check(lib().ccdb_set_fixed(self.h, _p(fx)))
 
     def last_call_seconds(self) -> float:
         """Device time of the kernels of the last compute_fisher_information."""

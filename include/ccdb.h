@@ -116,6 +116,10 @@ int ccdb_get_xbeta(ccdb_fit* f, double* out);
 int ccdb_get_beta(ccdb_fit* f, double* out);
 /* getGradientObjective (ModelSpecifics.hpp:103-120): sum of y * xBeta (* weight). */
 int ccdb_get_gradient_objective(ccdb_fit* f, double* out);
+/* CyclicCoordinateDescent::setFixedBeta for every column (.cpp:384-386):
+ * fixed[j] != 0 holds column j at its current beta in later mode finding; the
+ * offset column stays fixed.  Host state only. */
+int ccdb_set_fixed(ccdb_fit* f, const uint8_t* fixed);
 
 /* --- calls on a fitted state ------------------------------------------------ */
 

@@ -249,6 +249,25 @@ class ReferenceEngine(_Engine):
                 "beta": beta, "loglik": ll.value, "log": log.value.decode()}
 
 
+    def profile(self, cols, threshold: float = 1.920729, include_penalty: bool = False,
+                override_no_regularization: bool = False, conv_type: int = 0, tol: float = 1e-6,
+                max_iter: int = 1000):
+        """CcdInterface::profileModel around the current mode: (lower, upper,
+        objective evaluations) per column."""
+        fn = self.lib().ref_profile
+        fn.argtypes = [_P, _P, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int,
+                       _P, _P, _P, C.c_char_p, C.c_int]
+        cols = np.ascontiguousarray(cols, np.int32)
+        lo, up = np.zeros(len(cols)), np.zeros(len(cols))
+        ev = np.zeros(len(cols), np.int32)
+        err = C.create_string_buffer(512)
+        rc = fn(self.h, _ptr(cols), len(cols), threshold, int(include_penalty), int(override_no_regularization),
+                conv_type, tol, max_iter, _ptr(lo), _ptr(up), _ptr(ev), err, 512)
+        if rc != 0:
+            raise RuntimeError(err.value.decode())
+        return lo, up, ev
+
+
 class ReferenceOnB200Engine(ReferenceEngine):
     """The reference's own CyclicCoordinateDescent driving the B200 engine
     through ccd_b200/integration/B200ModelSpecifics.h (the drop-in)."""

@@ -60,6 +60,23 @@ struct GridDriver : GridSearchCrossValidationDriver {
     const std::vector<double>& values() const { return gridValue; }
 };
 
+// A CcdInterface used only for profileModel (CcdInterface.cpp:262-525); the
+// model-building hooks of the R and command-line front ends are not needed.
+struct ProfileInterface : CcdInterface {
+    ProfileInterface(loggers::ProgressLoggerPtr l, loggers::ErrorHandlerPtr e, const ModeFindingArguments& mf) {
+        logger = l;
+        error = e;
+        arguments.modeFinding = mf;
+        arguments.noiseLevel = SILENT;
+    }
+
+protected:
+    void initializeModelImpl(AbstractModelData**, CyclicCoordinateDescent**, AbstractModelSpecifics**) override {}
+    void predictModelImpl(CyclicCoordinateDescent*, AbstractModelData*) override {}
+    void logModelImpl(CyclicCoordinateDescent*, AbstractModelData*, ProfileInformationMap&, bool) override {}
+    void diagnoseModelImpl(CyclicCoordinateDescent*, AbstractModelData*, double, double) override {}
+};
+
 // Column format codes: the reference's FormatType (CompressedDataMatrix.h:36-38).
 enum { F_DENSE = 0, F_SPARSE = 1, F_INDICATOR = 2, F_INTERCEPT = 3 };
 
@@ -462,6 +479,41 @@ int ref_cross_validate(void* hp, int auto_search, int fold, int grid_steps, doub
             *n_points = n;
         }
         set_err(log_out, log_len, log->text.c_str());
+        return 0;
+    } catch (const std::exception& e) {
+        set_err(err, errlen, e.what());
+        return -1;
+    }
+}
+
+// Profile-likelihood bounds of columns cols[0..n) around the current mode,
+// one thread (CcdInterface::profileModel, CcdInterface.cpp:262-525): per
+// column the upper then the lower bound, each a sign-change bracket and a
+// zeroin root of LL(beta_j fixed) + threshold - LL(mode).  NaN where no sign
+// change was found.  The engine must hold a fitted mode.
+int ref_profile(void* hp, const int32_t* cols, int n, double threshold, int include_penalty,
+                int override_no_regularization, int conv_type, double tol, int max_iter, double* lower_out,
+                double* upper_out, int32_t* evals_out, char* err, int errlen) {
+    auto h = static_cast<RefHandle*>(hp);
+    try {
+        ModeFindingArguments mf;
+        mf.tolerance = tol;
+        mf.maxIterations = max_iter;
+        mf.convergenceType = conv_type;
+        ProfileInterface iface(h->log, h->err, mf);
+        ProfileVector labels;
+        const bool offset = h->data->getHasOffsetCovariate();
+        for (int i = 0; i < n; ++i)  // the labels build_data gave the columns
+            labels.push_back((offset && cols[i] == 0) ? IdType(1000000000) : IdType(cols[i] + 1));
+        ProfileInformationMap out;
+        iface.profileModel(h->ccd.get(), h->data.get(), labels, out, 1, threshold,
+                           override_no_regularization != 0, include_penalty != 0);
+        for (int i = 0; i < n; ++i) {
+            const ProfileInformation& p = out.at(labels[i]);
+            lower_out[i] = p.lower95Bound;
+            upper_out[i] = p.upper95Bound;
+            evals_out[i] = p.evaluations;
+        }
         return 0;
     } catch (const std::exception& e) {
         set_err(err, errlen, e.what());
