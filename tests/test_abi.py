@@ -20,7 +20,10 @@ def declared_functions():
 def test_header_declares_the_operator_api():
     names = declared_functions()
     for must in ("ccdb_compute_gradient_hessian", "ccdb_update_xbeta", "ccdb_find_mode",
-                 "ccdb_fit_model", "ccdb_matrix_create", "ccdb_set_weights"):
+                 "ccdb_fit_model", "ccdb_matrix_create", "ccdb_set_weights",
+                 # the rest of the AbstractModelSpecifics operator API and setFixedBeta
+                 "ccdb_fisher_information", "ccdb_compute_mm_gradient_hessian",
+                 "ccdb_get_predictive_log_likelihood", "ccdb_get_predictive_estimates", "ccdb_set_fixed"):
         assert must in names
 
 
