@@ -794,12 +794,45 @@ int ccdb_context_memory(const ccdb_context* ctx, size_t* bytes) {
     });
 }
 
+// The CompressedDataMatrix contract every matrix is checked against before any
+// device work (host only).
+static void validate_matrix(int64_t K, int32_t J, const int64_t* col_start, const int32_t* rows,
+                            const int64_t* val_start, const double* vals, const uint8_t* fmt) {
+    require(col_start && val_start && fmt, "NULL argument");
+    require(K > 0 && K < (int64_t(1) << 31) && J > 0, "bad dimensions");
+    const int64_t nnz = col_start[J], nv = val_start[J];
+    require(col_start[0] == 0 && val_start[0] == 0 && nnz >= 0 && nv >= 0, "bad offsets");
+    require(nnz == 0 || rows, "rows is NULL");
+    require(nv == 0 || vals, "vals is NULL");
+    for (int j = 0; j < J; ++j) {
+        const int64_t nr = col_start[j + 1] - col_start[j], nvj = val_start[j + 1] - val_start[j];
+        require(nr >= 0 && nvj >= 0, "offsets must be non-decreasing");
+        switch (fmt[j]) {
+        case F_DENSE: require(nr == 0 && nvj == K, "DENSE column needs K values, no rows"); break;
+        case F_INTERCEPT: require(nr == 0 && nvj == 0, "INTERCEPT column takes no data"); break;
+        case F_INDICATOR: require(nvj == 0, "INDICATOR column takes no values"); break;
+        case F_SPARSE: require(nvj == nr, "SPARSE column needs one value per row"); break;
+        default: require(false, "unknown column format");
+        }
+        int32_t last = -1;
+        for (int64_t p = col_start[j]; p < col_start[j + 1]; ++p) {
+            require(rows[p] > last && rows[p] < K, "row ids must be ascending and < K");
+            last = rows[p];
+        }
+    }
+}
+
+int ccdb_matrix_validate(int64_t K, int32_t J, const int64_t* col_start, const int32_t* rows,
+                         const int64_t* val_start, const double* vals, const uint8_t* fmt) {
+    return guard([&] { validate_matrix(K, J, col_start, rows, val_start, vals, fmt); });
+}
+
 int ccdb_matrix_create(ccdb_context* ctx, int64_t K, int32_t J, const int64_t* col_start,
                        const int32_t* rows, const int64_t* val_start, const double* vals,
                        const uint8_t* fmt, ccdb_matrix** out) {
     return guard([&] {
-        require(ctx && out && col_start && val_start && fmt, "NULL argument");
-        require(K > 0 && K < (int64_t(1) << 31) && J > 0, "bad dimensions");
+        require(ctx && out, "NULL argument");
+        validate_matrix(K, J, col_start, rows, val_start, vals, fmt);
         check_cuda(cudaSetDevice(ctx->device), "cudaSetDevice");
         std::unique_ptr<ccdb_matrix> m(new ccdb_matrix());
         m->ctx = ctx;
@@ -809,25 +842,6 @@ int ccdb_matrix_create(ccdb_context* ctx, int64_t K, int32_t J, const int64_t* c
         m->val_start.assign(val_start, val_start + J + 1);
         m->fmt.assign(fmt, fmt + J);
         const int64_t nnz = col_start[J], nv = val_start[J];
-        require(col_start[0] == 0 && val_start[0] == 0 && nnz >= 0 && nv >= 0, "bad offsets");
-        require(nnz == 0 || rows, "rows is NULL");
-        require(nv == 0 || vals, "vals is NULL");
-        for (int j = 0; j < J; ++j) {
-            const int64_t nr = col_start[j + 1] - col_start[j], nvj = val_start[j + 1] - val_start[j];
-            require(nr >= 0 && nvj >= 0, "offsets must be non-decreasing");
-            switch (fmt[j]) {
-            case F_DENSE: require(nr == 0 && nvj == K, "DENSE column needs K values, no rows"); break;
-            case F_INTERCEPT: require(nr == 0 && nvj == 0, "INTERCEPT column takes no data"); break;
-            case F_INDICATOR: require(nvj == 0, "INDICATOR column takes no values"); break;
-            case F_SPARSE: require(nvj == nr, "SPARSE column needs one value per row"); break;
-            default: require(false, "unknown column format");
-            }
-            int32_t last = -1;
-            for (int64_t p = col_start[j]; p < col_start[j + 1]; ++p) {
-                require(rows[p] > last && rows[p] < K, "row ids must be ascending and < K");
-                last = rows[p];
-            }
-        }
         m->rows_h.assign(rows, rows + nnz);
         m->vals_h.assign(vals, vals + nv);
         cudaStream_t s = ctx->stream;

@@ -138,6 +138,7 @@ def lib() -> C.CDLL:
         L.ccdb_compute_mm_gradient_hessian.argtypes = [_P, _P, _P, _P]
         L.ccdb_get_last_call_seconds.argtypes = [_P, _P]
         L.ccdb_set_fixed.argtypes = [_P, _P]
+        L.ccdb_matrix_validate.argtypes = [C.c_int64, C.c_int32, _P, _P, _P, _P, _P]
         _lib = L
     return _lib
 
@@ -410,6 +411,13 @@ def fit_model(ctx: Context, d: CyclopsData, args: Optional[ModeFindingArguments]
     return FitResult(beta, res.return_flag, res.iterations, res.log_likelihood, res.objective,
                      res.coordinate_updates, res.device_seconds, res.kernel_seconds,
                      res.kernel_launches)
+
+
+def validate_matrix(d: CyclopsData) -> None:
+    """The checks a matrix upload applies (host only); raises CcdbError."""
+    arrs = [_c(d.col_start, np.int64), _c(d.rows, np.int32), _c(d.val_start, np.int64),
+            _c(d.vals, np.float64), _c(d.fmt, np.uint8)]
+    _check(lib().ccdb_matrix_validate(d.K, d.J, *[_p(a) for a in arrs]))
 
 
 def sweep_levels(d: CyclopsData, fixed: Optional[np.ndarray] = None):

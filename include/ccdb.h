@@ -285,6 +285,14 @@ int ccdb_column_gradient_hessian_noalloc(int32_t model_type, int32_t fmt, int64_
 
 /* --- inspection (no reference counterpart) ---------------------------------- */
 
+/* The checks ccdb_matrix_create applies before any device work: offsets start
+ * at 0 and never decrease; DENSE columns hold K values and no rows, INTERCEPT
+ * nothing, INDICATOR rows only, SPARSE one value per row; row ids strictly
+ * ascending within a column and < K.  CCDB_ERR_INVALID with the first
+ * violation in ccdb_last_error.  Host-only: needs no GPU. */
+int ccdb_matrix_validate(int64_t K, int32_t J, const int64_t* col_start, const int32_t* rows,
+                         const int64_t* val_start, const double* vals, const uint8_t* fmt);
+
 /* Device time (CUDA events on the fit's stream) of the kernels of the fit's last
  * ccdb_fisher_information call, in seconds; copies to and from the host are
  * outside it.  0 before any such call. */
