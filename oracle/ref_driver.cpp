@@ -148,9 +148,13 @@ AbstractModelData* build_data(ModelType mt, int64_t K, int J, const double* y, c
             throw std::runtime_error("unknown column format");
         }
         const IdType label = (offset_col0 && j == 0) ? IdType(1000000000) : IdType(j + 1);
-        if (fmt[j] == F_INDICATOR && r.empty()) {
-            // an empty indicator column: loadX needs no values to keep it INDICATOR
-            md->loadX(label, r, v, false, false, false);
+        if ((fmt[j] == F_INDICATOR || fmt[j] == F_SPARSE) && r.empty()) {
+            // An empty column: loadX would read "no rows, no values" as an
+            // intercept (ModelData.cpp:257-263) and move it to the front, so the
+            // empty column goes into the matrix directly, as the reference's other
+            // constructors build columns (CompressedDataMatrix::push_back).
+            md->getX().push_back(fmt[j] == F_INDICATOR ? INDICATOR : SPARSE);
+            md->getX().getColumn(md->getX().getNumberOfColumns() - 1).add_label(label);
         } else {
             md->loadX(label, r, v, false, false, forceSparse);
         }
