@@ -13,12 +13,14 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
 
 #include "../../include/ccdb.h"
 #include "batch.h"
+#include "csr_host.h"
 #include "engine.h"
 
 namespace ccdb {
@@ -85,41 +87,14 @@ Matrix::~Matrix() {
 }
 
 // Row-major copy for computeXBeta: per row, entries in increasing column order
-// (dense-like columns included), built once by a stable counting sort.
+// (dense-like columns included), built once on the host threads (csr_host.cpp).
 void Matrix::ensure_csr(cudaStream_t s) {
     if (d_row_ptr) return;
-    std::vector<int64_t> cnt(K + 1, 0);
-    for (int j = 0; j < J; ++j) {
-        if (fmt[j] == F_DENSE || fmt[j] == F_INTERCEPT) {
-            for (int64_t k = 0; k < K; ++k) cnt[k + 1]++;
-        } else {
-            for (int64_t p = col_start[j]; p < col_start[j + 1]; ++p) cnt[rows_h[p] + 1]++;
-        }
-    }
-    for (int64_t k = 0; k < K; ++k) cnt[k + 1] += cnt[k];
-    const int64_t n = cnt[K];
-    std::vector<int32_t> col(n);
-    std::vector<double> val(n);
-    std::vector<int64_t> pos(cnt.begin(), cnt.end() - 1);
-    for (int j = 0; j < J; ++j) {
-        const uint8_t f = fmt[j];
-        if (f == F_DENSE || f == F_INTERCEPT) {
-            for (int64_t k = 0; k < K; ++k) {
-                const int64_t q = pos[k]++;
-                col[q] = j;
-                val[q] = (f == F_DENSE) ? vals_h[val_start[j] + k] : 1.0;
-            }
-        } else {
-            for (int64_t p = col_start[j]; p < col_start[j + 1]; ++p) {
-                const int64_t q = pos[rows_h[p]]++;
-                col[q] = j;
-                val[q] = (f == F_SPARSE) ? vals_h[val_start[j] + (p - col_start[j])] : 1.0;
-            }
-        }
-    }
-    d_row_ptr = upload(ctx, cnt.data(), cnt.size(), s);
-    d_csr_col = upload(ctx, col.data(), col.size(), s);
-    d_csr_val = upload(ctx, val.data(), val.size(), s);
+    const HostCsr h = build_csr(K, J, col_start.data(), rows_h.data(), val_start.data(), vals_h.data(),
+                                fmt.data(), (int)std::max(1u, std::thread::hardware_concurrency()));
+    d_row_ptr = upload(ctx, h.row_ptr.data(), h.row_ptr.size(), s);
+    d_csr_col = upload(ctx, h.col.data(), h.col.size(), s);
+    d_csr_val = upload(ctx, h.val.data(), h.val.size(), s);
     check_cuda(cudaStreamSynchronize(s), "csr upload");
 }
 

@@ -1,8 +1,9 @@
 """Host code under AddressSanitizer / UndefinedBehaviorSanitizer (no GPU):
 the dependency-level schedule builder of the fused sweep
-(ccd_b200/csrc/schedule.cpp) with a fuzz test of its invariants, and the
-oracle restatement (oracle/ccd_oracle.c) through every call on random
-problems.  compute-sanitizer is not used for the device side; these cover the
+(ccd_b200/csrc/schedule.cpp) with a fuzz test of its invariants, the
+multi-threaded row-major copy (ccd_b200/csrc/csr_host.cpp) against a plain
+counting sort (also under ThreadSanitizer), and the oracle restatement
+(oracle/ccd_oracle.c) through every call on random problems.  compute-sanitizer is not used for the device side; these cover the
 host side the way the reference's ASAN/UBSAN builds cover its C++."""
 import os
 import shutil
@@ -41,3 +42,14 @@ def test_oracle_under_sanitizers(tmp_path):
                           os.path.join(ROOT, "tests", "native", "oracle_check.c"),
                           os.path.join(ROOT, "oracle", "ccd_oracle.c"), "-lm", "-o", exe], exe, ["200"])
     assert "ran clean" in out
+
+
+@pytest.mark.timeout(900)
+@pytest.mark.parametrize("sanitizer", [SAN, ["-O1", "-g", "-fsanitize=thread"]], ids=["asan_ubsan", "tsan"])
+def test_row_major_copy_under_sanitizers(tmp_path, sanitizer):
+    exe = str(tmp_path / "csr_check")
+    csrc = os.path.join(ROOT, "ccd_b200", "csrc")
+    out = _build_and_run(["g++", "-std=c++17"] + sanitizer + ["-I" + csrc,
+                          os.path.join(ROOT, "tests", "native", "csr_check.cpp"),
+                          os.path.join(csrc, "csr_host.cpp"), "-lpthread", "-o", exe], exe, ["100"])
+    assert "identical" in out
