@@ -203,10 +203,6 @@ private:
             throw std::runtime_error(s.str());
         }
     }
-    [[noreturn]] static void unsupported(const char* what) {
-        throw std::logic_error(std::string(what) + " is not provided by the B200 engine");
-    }
-
     const ModelData<double>& data_;
     ModelType modelType_;
     int device_;
