@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from ccd_b200 import native
-from ccd_b200.data import GRADIENT, MITTAL
+from ccd_b200.data import GRADIENT, MITTAL, MODEL_COX
 from oracle import checker
 
 from .edge_cases import cases
@@ -31,7 +31,10 @@ def test_gpu_edge_case(gpu_ctx, name, conv):
     if w is not None:
         f.set_weights(w)
     gh = np.array([f.compute_gradient_and_hessian(j) for j in range(d.J)])
-    np.testing.assert_allclose(gh, gh_want, rtol=1e-10, atol=1e-10)
+    # 1e-10 as the other per-coordinate tests; 1e-9 for Cox, whose gradient is
+    # reassociated through per-group suffix sums
+    tol = 1e-9 if d.model_type == MODEL_COX else 1e-10
+    np.testing.assert_allclose(gh, gh_want, rtol=tol, atol=tol)
     r = f.find_mode(native.ModeFindingArguments(convergence_type=conv, tolerance=1e-7))
     assert r.return_flag == want["flag"]
     assert abs(r.iterations - want["iterations"]) <= 2
