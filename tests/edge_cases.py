@@ -67,6 +67,12 @@ def cases():
     d = CyclopsData(MODEL_CONDITIONAL_LOGISTIC, y, cs, r, vs, v, fm, np.full(5, PRIOR_NORMAL, np.int32),
                     np.ones(5), stratum=stratum)
     out["clr_singletons_no_events"] = (d, None)
+    # conditional logistic with zero weights on single rows inside strata
+    w = (np.arange(K) % 5 != 3).astype(float)
+    out["clr_row_zero_weights"] = (d, w)
+    # Poisson with an offset, Laplace priors and fractional weights
+    d = synthetic.small(MODEL_POISSON, seed=186, K=200, P=6, offset=True, prior=PRIOR_LAPLACE, variance=0.5)
+    out["poisson_offset_laplace_fractional_weights"] = (d, 0.25 + (np.arange(d.K) % 4) * 0.5)
     # Cox: one stratum entirely censored, one with zero weights throughout, every time tied
     d = synthetic.small(MODEL_COX, seed=184, K=240, P=5, n_strata=4, tie_days=1, prior=PRIOR_NORMAL)
     s0 = d.stratum == d.stratum.min()
