@@ -630,15 +630,22 @@ void Fit::find_mode(const ccdb_mode_args& a, double* beta_inout, ccdb_fit_result
     const int64_t launches0 = launches;
     check_cuda(cudaEventRecord(evc0, stream), "event");
     double bound = a.initial_bound;
-    int count = 0, flag = R_FAIL, iters = 0;
+    int count = 0, flag = R_FAIL;
     double obj = 0.0, secs = 0.0;
     int64_t updates = 0;
     for (;;) {
         float ms = 0.f;
+        // A swindle whose active set stays empty runs no findMode and leaves the
+        // count as it was: the reference then reports its lastIterationCount from
+        // the previous fit (CyclicCoordinateDescent.cpp:696-709, :1209).
+        int iters = -1;
         if (swindle) kkt_swindle(a, bound, &flag, &iters, &obj, &ms);
         else find_mode_once(a, bound, &flag, &iters, &obj, &ms);
         secs += ms * 1e-3;
-        updates += (int64_t)iters * active;
+        if (iters >= 0) {
+            last_iterations = iters;
+            updates += (int64_t)iters * active;
+        }
         ++count;
         if (beta_dirty_host) {
             download_beta();
@@ -663,7 +670,7 @@ void Fit::find_mode(const ccdb_mode_args& a, double* beta_inout, ccdb_fit_result
     check_cuda(cudaEventElapsedTime(&call_ms, evc0, evc1), "elapsed");
     if (res) {
         res->return_flag = flag;
-        res->iterations = iters;
+        res->iterations = last_iterations;
         res->objective = obj;
         res->log_likelihood = ll;
         res->coordinate_updates = updates;
@@ -936,6 +943,16 @@ int ccdb_set_beta(ccdb_fit* f, const double* beta) {
         f->upload_beta();
         f->xb_known = false;
         f->suff_known = false;
+    });
+}
+
+int ccdb_compute_xbeta(ccdb_fit* f, const double* beta) {
+    return guard([&] {
+        require(f && beta, "NULL argument");
+        require_fp64(f);
+        f->beta_h.assign(beta, beta + f->J);
+        f->upload_beta();
+        f->compute_xbeta_transpose();  // the statistics stay stale until computeRemainingStatistics
     });
 }
 

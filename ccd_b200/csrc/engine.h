@@ -131,6 +131,7 @@ struct Fit {
     cudaEvent_t evc0 = nullptr, evc1 = nullptr;  // around a whole find_mode
     int64_t launches = 0;                        // engine kernels launched so far
     double last_call_seconds = 0.0;              // device time of the last fisher_information passes
+    int last_iterations = 0;                     // getIterationCount: the last findMode's cycles
     std::unique_ptr<DevSchedule> sched;
     CoxDev cox;
 
@@ -152,6 +153,7 @@ struct Fit {
     void ensure_schedule();
     void apply_weights();
     void compute_xbeta();
+    void compute_xbeta_transpose();  // the MM cycle's product (ModelSpecifics::computeXBeta(beta))
     void remaining_statistics();
     void check_lazy();
     void upload_beta();

@@ -756,15 +756,19 @@ __global__ void xjy_kernel(const int64_t* col_ptr, const int32_t* rows, const in
 
 // xBeta = X beta, per row in increasing column order over the row-major copy
 // (the same sequence of additions as the column axpy loop of
-// CyclicCoordinateDescent::computeXBeta, .cpp:1452-1470).
+// CyclicCoordinateDescent::computeXBeta, .cpp:1452-1470).  With `unit_values`
+// every entry of non-zero value counts as 1: the product over an INDICATOR
+// transpose (ModelSpecifics::computeXBeta, ModelSpecifics.hpp:313-361).
 __global__ void xbeta_csr_kernel(const int64_t* row_ptr, const int32_t* col_idx, const double* val,
-                                 const double* beta, int64_t K, double* xb) {
+                                 const double* beta, int64_t K, int unit_values, double* xb) {
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K;
          k += (int64_t)gridDim.x * blockDim.x) {
         double s = 0.0;
         for (int64_t p = row_ptr[k]; p < row_ptr[k + 1]; ++p) {
             const double b = beta[col_idx[p]];
-            if (b != 0.0) s += b * val[p];
+            if (b == 0.0) continue;
+            if (!unit_values) s += b * val[p];
+            else if (val[p] != 0.0) s += b;
         }
         xb[k] = s;
     }
@@ -879,8 +883,9 @@ cudaError_t launch_xjy(const int64_t* col_ptr, const int32_t* rows, const int64_
 }
 
 cudaError_t launch_xbeta_csr(const int64_t* row_ptr, const int32_t* col_idx, const double* val,
-                             const double* beta, int64_t K, double* xb, cudaStream_t stream) {
-    xbeta_csr_kernel<<<1184, 256, 0, stream>>>(row_ptr, col_idx, val, beta, K, xb);
+                             const double* beta, int64_t K, double* xb, cudaStream_t stream,
+                             int unit_values) {
+    xbeta_csr_kernel<<<1184, 256, 0, stream>>>(row_ptr, col_idx, val, beta, K, unit_values, xb);
     return cudaGetLastError();
 }
 

@@ -72,7 +72,9 @@ cudaError_t launch_xjy(const int64_t* col_ptr, const int32_t* rows, const int64_
                        int64_t K, int32_t J, double* xjy, cudaStream_t stream);
 cudaError_t launch_xbeta_dense(const double* vals, double b, int64_t K, double* xb,
                                cudaStream_t stream);
+// unit_values: count every non-zero entry as 1 (the MM product, see xbeta_csr_kernel)
 cudaError_t launch_xbeta_csr(const int64_t* row_ptr, const int32_t* col_idx, const double* val,
-                             const double* beta, int64_t K, double* xb, cudaStream_t stream);
+                             const double* beta, int64_t K, double* xb, cudaStream_t stream,
+                             int unit_values = 0);
 
 }  // namespace ccdb

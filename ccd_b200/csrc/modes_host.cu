@@ -64,13 +64,34 @@ void Fit::mm_gradient_hessian(const uint8_t* fixed_flags, double2* out) {
     ctx->release(d_fixed);
 }
 
+// xBeta from the device beta as ModelSpecifics::computeXBeta(double* beta, bool)
+// (ModelSpecifics.hpp:313-361) forms it: row by row over hX.transpose(), whose
+// rows all take one format (CompressedDataMatrix.cpp:151-209), INDICATOR when
+// some column is INDICATOR and none is DENSE.  That transpose keeps no values,
+// so a SPARSE column then counts 1 for each of its non-zero entries; the
+// product here follows the same rule (unit_values).
+void Fit::compute_xbeta_transpose() {
+    bool any_indicator = false, any_dense = false;
+    for (int j = 0; j < J; ++j) {
+        any_indicator |= m->fmt[j] == F_INDICATOR;
+        any_dense |= m->fmt[j] == F_DENSE;
+    }
+    const_cast<Matrix*>(m)->ensure_csr(stream);
+    check_cuda(launch_xbeta_csr(m->d_row_ptr, m->d_csr_col, m->d_csr_val, beta, K, xb_tmp, stream,
+                                any_indicator && !any_dense),
+               "xbeta (transpose)");
+    ++launches;
+    xb_pending = true;
+    xb_known = true;
+    suff_known = false;
+}
+
 // findMode with AlgorithmType::MM (CyclicCoordinateDescent.cpp:957-1001 and
 // the MM check :1032-1048): per cycle, every free coordinate steps from one
 // all-coordinate (g, h) (mmUpdateAllBeta, .cpp:1354-1391), xBeta is recomputed
-// from beta (ModelSpecifics::computeXBeta, ModelSpecifics.hpp:313-361) and the
-// remaining statistics follow; a log posterior that decreases is the
-// reference's "Non-increasing!" error.  Convergence as findMode's
-// performCheckConvergence.
+// from beta (compute_xbeta_transpose) and the remaining statistics follow; a
+// log posterior that decreases is the reference's "Non-increasing!" error.
+// Convergence as findMode's performCheckConvergence.
 void Fit::find_mode_mm(const ccdb_mode_args& a, int* flag, int* iters, double* obj) {
     uint8_t* d_fixed = static_cast<uint8_t*>(ctx->alloc(std::max(1, J)));
     double2* d_gh = static_cast<double2*>(ctx->alloc(sizeof(double2) * std::max(1, J)));
@@ -104,12 +125,8 @@ void Fit::find_mode_mm(const ccdb_mode_args& a, int* flag, int* iters, double* o
             P.nEv = cox.nEv;
             P.denom = cox.denom;
             check_cuda(launch_mm_gradient_hessian(P, stream), "mm step");
-            check_cuda(launch_xbeta_csr(m->d_row_ptr, m->d_csr_col, m->d_csr_val, beta, K, xb_tmp, stream),
-                       "mm xbeta");
-            launches += 2;
-            xb_pending = true;
-            xb_known = true;
-            suff_known = false;
+            ++launches;
+            compute_xbeta_transpose();
             remaining_statistics();
             download_beta();
             ++iteration;

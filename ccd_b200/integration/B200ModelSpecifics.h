@@ -110,9 +110,12 @@ public:
         beta_[j] += b;
         dirty_ = true;
     }
+    // ModelSpecifics::computeXBeta(double*, bool) (ModelSpecifics.hpp:313-361),
+    // called by the MM cycle: the product over the one-format transpose.
     void computeXBeta(double* beta, bool) override {
         beta_.assign(beta, beta + J_);
-        dirty_ = true;
+        check(ccdb_compute_xbeta(fit_, beta_.data()), "computeXBeta");
+        dirty_ = false;
     }
 
     void computeRemainingStatistics(bool) override {

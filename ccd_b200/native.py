@@ -118,6 +118,7 @@ def lib() -> C.CDLL:
         L.ccdb_fit_destroy.argtypes = [_P]
         L.ccdb_set_weights.argtypes = [_P, _P]
         L.ccdb_set_beta.argtypes = [_P, _P]
+        L.ccdb_compute_xbeta.argtypes = [_P, _P]
         L.ccdb_compute_gradient_hessian.argtypes = [_P, C.c_int32, _P, _P]
         L.ccdb_update_xbeta.argtypes = [_P, C.c_int32, C.c_double]
         L.ccdb_compute_remaining_statistics.argtypes = [_P]
@@ -274,6 +275,12 @@ class Fit:
     def set_beta(self, beta: np.ndarray) -> None:
         b = _c(beta, np.float64)
         _check(lib().ccdb_set_beta(self.h, _p(b)))
+
+    def compute_xbeta(self, beta: np.ndarray) -> None:
+        """xBeta from beta as the MM cycle forms it (ModelSpecifics::computeXBeta:
+        with INDICATOR and no DENSE columns every non-zero entry counts 1)."""
+        b = _c(beta, np.float64)
+        _check(lib().ccdb_compute_xbeta(self.h, _p(b)))
 
     def compute_gradient_and_hessian(self, j: int):
         g, h = C.c_double(), C.c_double()

@@ -102,6 +102,13 @@ int ccdb_set_weights(ccdb_fit* f, const double* weights);
 /* beta[J] -> xBeta, offsExpXBeta, denominators (computeXBeta + computeRemainingStatistics,
  * CyclicCoordinateDescent.cpp:1452-1470, ModelSpecifics.hpp:1588-1633). */
 int ccdb_set_beta(ccdb_fit* f, const double* beta);
+/* beta[J] -> xBeta by ModelSpecifics::computeXBeta(double* beta, bool)
+ * (ModelSpecifics.hpp:313-361), the MM cycle's product over hX.transpose():
+ * that transpose gives every row one format (CompressedDataMatrix.cpp:151-209),
+ * and when the matrix has an INDICATOR column and no DENSE column it keeps no
+ * values, so every non-zero entry counts as 1.  Other matrices get X beta.
+ * The remaining statistics are left to ccdb_compute_remaining_statistics. */
+int ccdb_compute_xbeta(ccdb_fit* f, const double* beta);
 /* computeNumeratorForGradient + computeGradientAndHessian for column j
  * (ModelSpecifics.hpp:1353-1464, 711-766). */
 int ccdb_compute_gradient_hessian(ccdb_fit* f, int32_t j, double* gradient, double* hessian);

@@ -214,6 +214,33 @@ static void compute_xbeta(Orc* o) {
     }
 }
 
+/* The MM cycle's xBeta: ModelSpecifics::computeXBeta (MS.hpp:313-361) over
+ * hX.transpose() (CompressedDataMatrix.cpp:151-209).  The transpose gives all
+ * rows one format: INDICATOR when some column is INDICATOR and none is DENSE,
+ * DENSE when some column is DENSE and none is INDICATOR, else SPARSE.  Only
+ * the INDICATOR transpose changes the product: it keeps no values, so every
+ * entry of non-zero value counts as 1 (a SPARSE column's values are lost).
+ * The row sums run in increasing column order, as compute_xbeta's do. */
+static void compute_xbeta_mm(Orc* o) {
+    int any_indicator = 0, any_dense = 0;
+    for (int j = 0; j < o->J; ++j) {
+        any_indicator |= o->fmt[j] == F_INDICATOR;
+        any_dense |= o->fmt[j] == F_DENSE;
+    }
+    if (!any_indicator || any_dense) {
+        compute_xbeta(o);
+        return;
+    }
+    memset(o->xb, 0, sizeof(double) * o->K);
+    for (int j = 0; j < o->J; ++j) {
+        double b = o->beta[j];
+        if (b == 0.0) continue;
+        int64_t n = col_len(o, j);
+        for (int64_t p = 0; p < n; ++p)
+            if (col_val(o, j, p) != 0.0) o->xb[col_row(o, j, p)] += b;
+    }
+}
+
 /* computeAccumlatedDenominator, MS.hpp:1670-1715 (Breslow: one-way scan) */
 static void acc_denominator(Orc* o) {
     if (!is_cox(o)) return;
@@ -649,7 +676,7 @@ static int find_mode_mm(Orc* o, int max_iter, int conv, double eps, const char**
         }
         for (int j = 0; j < o->J; ++j)
             if (!o->fix[j] && delta[j] != 0.0) o->beta[j] += delta[j];
-        compute_xbeta(o);
+        compute_xbeta_mm(o);
         remaining_statistics(o);
         iteration++;
         const double lp = log_likelihood(o) + log_prior(o);

@@ -23,7 +23,8 @@ def test_header_declares_the_operator_api():
                  "ccdb_fit_model", "ccdb_matrix_create", "ccdb_set_weights",
                  # the rest of the AbstractModelSpecifics operator API and setFixedBeta
                  "ccdb_fisher_information", "ccdb_compute_mm_gradient_hessian",
-                 "ccdb_get_predictive_log_likelihood", "ccdb_get_predictive_estimates", "ccdb_set_fixed"):
+                 "ccdb_get_predictive_log_likelihood", "ccdb_get_predictive_estimates", "ccdb_set_fixed",
+                 "ccdb_compute_xbeta"):
         assert must in names
 
 

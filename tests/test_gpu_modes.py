@@ -6,6 +6,7 @@ same variants over the drop-in adapter.
 Tolerances as for plain fits: same iteration count and return flag,
 coefficients within 1e-6 relative to the largest, log-likelihood 1e-9."""
 import os
+import re
 
 import numpy as np
 import pytest
@@ -14,6 +15,8 @@ from ccd_b200 import native, synthetic
 from ccd_b200.data import (GRADIENT, LANGE, MITTAL, MODEL_CONDITIONAL_LOGISTIC, MODEL_CONDITIONAL_POISSON,
                            MODEL_COX, MODEL_LOGISTIC, MODEL_POISSON, PRIOR_LAPLACE, PRIOR_NORMAL)
 from oracle import checker
+
+from .test_oracle_postfit import _dense
 
 pytestmark = pytest.mark.gpu
 
@@ -100,6 +103,62 @@ def test_mm_with_kkt_swindle_matches_oracle(gpu_ctx):
     _agree(got, want)
 
 
+@pytest.mark.parametrize("formats", [("sparse", "indicator"), ("sparse",), ("indicator", "dense", "sparse")])
+def test_mm_product_follows_the_transpose_format(gpu_ctx, formats):
+    """The MM cycle's xBeta over the reference's one-format transpose
+    (CompressedDataMatrix.cpp:151-209): SPARSE + INDICATOR without DENSE counts
+    each non-zero entry as 1, which on this problem makes the log posterior
+    fall by 0.05 in the third cycle ("Non-increasing!", as the reference)."""
+    d = synthetic.small(MODEL_CONDITIONAL_LOGISTIC, seed=150, n_strata=20, formats=formats,
+                        prior=PRIOR_NORMAL, variance=4.0)
+    try:
+        want = _oracle_fit(d, conv_type=MITTAL, tol=1e-8, algorithm=1)
+    except RuntimeError as ex:
+        with pytest.raises(native.CcdbError, match=re.escape(str(ex))):
+            _gpu_fit(gpu_ctx, d, convergence_type=MITTAL, tolerance=1e-8, algorithm=native.ALGORITHM_MM)
+        return
+    got = _gpu_fit(gpu_ctx, d, convergence_type=MITTAL, tolerance=1e-8, algorithm=native.ALGORITHM_MM)
+    _agree(got, want)
+
+
+@pytest.mark.parametrize("formats,unit", [(("sparse", "indicator"), True), (("sparse", "indicator", "dense"), False)])
+def test_mm_cycle_xbeta_is_the_transpose_product(gpu_ctx, formats, unit):
+    """After one MM cycle the device xBeta is X' beta, X' = X with every
+    non-zero entry 1 when the matrix has INDICATOR and no DENSE columns."""
+    d = synthetic.small(MODEL_CONDITIONAL_LOGISTIC, seed=151, n_strata=15, formats=formats,
+                        prior=PRIOR_NORMAL, variance=4.0)
+    m = native.Matrix(gpu_ctx, d)
+    f = native.Fit(gpu_ctx, m, d)
+    r = f.find_mode(native.ModeFindingArguments(convergence_type=MITTAL, tolerance=1e-8, max_iterations=1,
+                                                algorithm=native.ALGORITHM_MM))
+    X = _dense(d)
+    if unit:
+        X = (X != 0).astype(float)
+    np.testing.assert_allclose(f.get_xbeta(), X @ r.beta, rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("formats,unit", [(("sparse", "indicator"), True), (("indicator",), True),
+                                          (("sparse", "dense"), False), (("sparse",), False)])
+def test_compute_xbeta_from_beta(gpu_ctx, formats, unit):
+    """ccdb_compute_xbeta, ModelSpecifics::computeXBeta(double* beta, bool):
+    X' beta against numpy, X' = X with non-zero entries 1 exactly when the
+    matrix has INDICATOR and no DENSE columns; the statistics follow on demand."""
+    d = synthetic.small(MODEL_CONDITIONAL_LOGISTIC, seed=152, n_strata=15, formats=formats)
+    m = native.Matrix(gpu_ctx, d)
+    f = native.Fit(gpu_ctx, m, d)
+    beta = np.random.default_rng(152).normal(0.0, 0.5, d.J)
+    f.compute_xbeta(beta)
+    X = _dense(d)
+    if unit:
+        X = (X != 0).astype(float)
+    np.testing.assert_allclose(f.get_xbeta(), X @ beta, rtol=1e-12, atol=1e-12)
+    f.compute_remaining_statistics()
+    e = checker.RestatementEngine(d)
+    e.set_beta(beta)
+    if not unit:  # the oracle's state from beta is X beta
+        assert abs(f.get_log_likelihood() - e.loglik()) <= 1e-11 * abs(e.loglik())
+
+
 @pytest.mark.parametrize("model", [MODEL_LOGISTIC, MODEL_POISSON])
 def test_mm_refused_without_strata(gpu_ctx, model):
     d = synthetic.small(model, seed=138, offset=(model == MODEL_POISSON))
@@ -175,3 +234,26 @@ def test_reference_solver_variants_on_b200(model, kw, fit_kw):
     err = np.max(np.abs(got["beta"] - want["beta"])) / max(np.max(np.abs(want["beta"])), 1e-8)
     assert err <= 1e-6
     assert abs(got["loglik"] - want["loglik"]) <= 1e-9 * abs(want["loglik"])
+
+
+@dropin
+@pytest.mark.parametrize("formats", [("sparse", "indicator"), ("sparse", "dense")])
+def test_reference_solver_mm_over_the_transpose_product(formats):
+    """The reference's MM cycle calls computeXBeta(beta) on the adapter, which
+    forms the one-format transpose product as the reference's own
+    ModelSpecifics does: the same end, a fit or "Non-increasing!"."""
+    d = synthetic.small(MODEL_CONDITIONAL_LOGISTIC, seed=150, n_strata=20, formats=formats,
+                        prior=PRIOR_NORMAL, variance=4.0)
+    out = []
+    for E in (checker.ReferenceEngine, checker.ReferenceOnB200Engine):
+        try:
+            out.append(E(d).fit(MITTAL, 1e-8, algorithm=1))
+        except RuntimeError as ex:
+            out.append(str(ex))
+    want, got = out
+    if isinstance(want, str):
+        assert got == want
+        return
+    assert got["flag"] == want["flag"] and got["iterations"] == want["iterations"]
+    err = np.max(np.abs(got["beta"] - want["beta"])) / max(np.max(np.abs(want["beta"])), 1e-8)
+    assert err <= 1e-6

@@ -19,6 +19,8 @@ from ccd_b200.data import (GRADIENT, LANGE, MITTAL, MODEL_CONDITIONAL_LOGISTIC, 
                            MODEL_COX, MODEL_LOGISTIC, MODEL_POISSON, PRIOR_LAPLACE, PRIOR_NORMAL)
 from oracle import checker
 
+from .test_oracle_postfit import _dense
+
 needs_ref = pytest.mark.skipif(not checker.reference_available(),
                                reason="reference engine not built (no reference sources here)")
 
@@ -92,6 +94,45 @@ def test_mm_with_kkt_swindle_bit_exact(model, kw):
     d = synthetic.small(model, **kw)
     a, b = _both(d, conv_type=GRADIENT, tol=1e-7, algorithm=1, kkt_swindle=True)
     _same(a, b)
+
+
+@needs_ref
+@pytest.mark.parametrize("formats", [("sparse", "indicator"), ("sparse", "dense"), ("sparse",),
+                                     ("indicator", "dense", "sparse")])
+@pytest.mark.parametrize("model", [MODEL_CONDITIONAL_LOGISTIC, MODEL_COX])
+def test_mm_product_follows_the_transpose_format(model, formats):
+    """The MM cycle's xBeta runs over hX.transpose(), whose rows take one
+    format (CompressedDataMatrix.cpp:151-209): with INDICATOR and SPARSE columns
+    and no DENSE one the transpose is INDICATOR and a SPARSE entry counts 1.
+    The restatement follows the same rule, bit for bit, under every mix; the
+    inconsistent product often ends the reference's fit with "Non-increasing!",
+    and then the restatement's too."""
+    d = synthetic.small(model, seed=150, n_strata=20, formats=formats, prior=PRIOR_NORMAL, variance=4.0)
+    out = []
+    for E in (checker.ReferenceEngine, checker.RestatementEngine):
+        try:
+            out.append(E(d).fit(MITTAL, 1e-8, algorithm=1))
+        except RuntimeError as ex:
+            out.append(str(ex))
+    if isinstance(out[0], str) or isinstance(out[1], str):
+        assert out[0] == out[1]
+    else:
+        _same(*out)
+
+
+def test_mm_product_counts_sparse_entries_as_one_without_dense_columns():
+    """The same rule shown on the restatement alone: after one MM cycle on a
+    SPARSE + INDICATOR matrix the state's xBeta is X' beta with every non-zero
+    entry of X' equal to 1; with a DENSE column added it is X beta."""
+    for formats, unit in ((("sparse", "indicator"), True), (("sparse", "indicator", "dense"), False)):
+        d = synthetic.small(MODEL_CONDITIONAL_LOGISTIC, seed=151, n_strata=15, formats=formats,
+                            prior=PRIOR_NORMAL, variance=4.0)
+        e = checker.RestatementEngine(d)
+        r = e.fit(MITTAL, 1e-8, max_iter=1, algorithm=1)
+        X = _dense(d)
+        if unit:
+            X = (X != 0).astype(float)
+        np.testing.assert_allclose(e.xbeta(), X @ r["beta"], rtol=1e-12, atol=1e-12)
 
 
 @pytest.mark.parametrize("model", [MODEL_LOGISTIC, MODEL_POISSON])
