@@ -9,6 +9,7 @@ library is missing or no GPU is present, constructing a ``Context`` raises.
 from __future__ import annotations
 
 import ctypes as C
+import dataclasses
 import weakref
 import os
 from dataclasses import dataclass
@@ -384,6 +385,46 @@ class Fit:
                 "updates": r.updates, "update_entries": r.update_entries,
                 "gradient_entries": r.gradient_entries} for r in res]
         return beta, out, secs.value
+
+    def fold_instances(self, variances, holdout, row_fold, args: Optional[ModeFindingArguments] = None):
+        """Cross-validation instances as standalone fits on this handle, for
+        any model: instance i weights the rows 1 off fold holdout[i] and 0 on
+        it (CrossValidationSelector::getWeights), runs its columns at the J
+        prior variances variances[i], starts cold, and reports the held-out
+        fold's predictive log-likelihood when it succeeded
+        (AbstractCrossValidationDriver.cpp:180-232).  Serves what one batched
+        launch does not: several variance parameters, and the conditional
+        and Cox models.  The handle is left unweighted.  Returns
+        (beta[n, J], list of per-instance dicts, device seconds)."""
+        args = args or ModeFindingArguments()
+        var = np.ascontiguousarray(variances, dtype=np.float64)
+        if var.ndim != 2 or var.shape[1] != self.d.J:
+            raise ValueError("variances must be n x J")
+        hold = np.asarray(holdout, dtype=np.int64)
+        fold = np.asarray(row_fold)
+        start = np.zeros(self.d.J)
+        if self.d.offset_col0:
+            start[0] = 1.0
+        beta = np.zeros((var.shape[0], self.d.J))
+        out, secs = [], 0.0
+        try:
+            for i in range(var.shape[0]):
+                w = (fold != hold[i]).astype(np.float64)
+                self.set_weights(w)
+                keep = []
+                ma = _mode_args(dataclasses.replace(self.d, prior_var=var[i]), args, keep)
+                b = start.copy()
+                res = _FitResult()
+                _check(lib().ccdb_find_mode(self.h, C.byref(ma), _p(b), C.byref(res)))
+                pred = (self.get_predictive_log_likelihood(1.0 - w) if res.return_flag == 0
+                        else float("nan"))
+                beta[i] = b
+                secs += res.device_seconds
+                out.append({"flag": res.return_flag, "iterations": res.iterations,
+                            "loglik": res.log_likelihood, "objective": res.objective, "pred_loglik": pred})
+        finally:
+            self.set_weights(None)
+        return beta, out, secs
 
     # --- CyclicCoordinateDescent::update
     def find_mode(self, args: Optional[ModeFindingArguments] = None,

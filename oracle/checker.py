@@ -213,6 +213,19 @@ class ReferenceEngine(_Engine):
     libpath = REF_LIB
 
 
+    @classmethod
+    def quadr_log_fit(cls, history: dict):
+        """The auto search's quadratic fit (utils/HParSearch.cpp:22-64) of a
+        {x: (mean, stdev)} history: (c0, c1, c2)."""
+        fn = cls.lib().ref_quadr_log_fit
+        fn.argtypes = [C.c_int, _P, _P, _P, _P]
+        xs = np.array(sorted(history), dtype=np.float64)
+        m = np.array([history[x][0] for x in xs], dtype=np.float64)
+        sd = np.array([history[x][1] for x in xs], dtype=np.float64)
+        out = np.zeros(3)
+        fn(len(xs), _ptr(xs), _ptr(m), _ptr(sd), _ptr(out))
+        return float(out[0]), float(out[1]), float(out[2])
+
     def asymptotic_variance(self, i: int, j: int) -> float:
         v = C.c_double()
         err = C.create_string_buffer(512)
@@ -232,21 +245,24 @@ class ReferenceEngine(_Engine):
         fn = lib.ref_cross_validate
         fn.argtypes = [_P, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_long,
                        C.c_int, C.c_double, C.c_int, _P, _P, _P, C.c_int, _P, _P, _P, _P, C.c_char_p,
-                       C.c_int, C.c_char_p, C.c_int]
+                       C.c_int, _P, C.c_int, _P, C.c_char_p, C.c_int]
         row_fold = np.zeros(self.d.K, np.int32)
         pts, vals = np.zeros(max(grid_steps, 1)), np.zeros(max(grid_steps, 1))
         n = C.c_int()
         var, ll = C.c_double(), C.c_double()
         beta = np.zeros(self.d.J)
-        log = C.create_string_buffer(1 << 20)
+        log = C.create_string_buffer(1 << 24)
         err = C.create_string_buffer(512)
+        hyper = np.zeros(64)
+        nh = C.c_int()
         rc = fn(self.h, int(auto_search), fold, grid_steps, lower, upper, starting_variance, seed, conv_type,
                 tol, max_iter, _ptr(row_fold), _ptr(pts), _ptr(vals), len(pts), C.byref(n), C.byref(var),
-                _ptr(beta), C.byref(ll), log, 1 << 20, err, 512)
+                _ptr(beta), C.byref(ll), log, 1 << 24, _ptr(hyper), len(hyper), C.byref(nh), err, 512)
         if rc != 0:
             raise RuntimeError(err.value.decode())
         return {"row_fold": row_fold, "points": pts[:n.value], "values": vals[:n.value], "variance": var.value,
-                "beta": beta, "loglik": ll.value, "log": log.value.decode()}
+                "variances": hyper[:min(nh.value, len(hyper))].copy(), "beta": beta, "loglik": ll.value,
+                "log": log.value.decode()}
 
 
     def profile(self, cols, threshold: float = 1.920729, include_penalty: bool = False,

@@ -30,6 +30,7 @@
 #include "drivers/GridSearchCrossValidationDriver.h"
 #include "priors/JointPrior.h"
 #include "priors/CovariatePrior.h"
+#include "utils/HParSearch.h"
 #ifdef CCDB_B200_ADAPTER
 #include "B200ModelSpecifics.h"
 #endif
@@ -421,11 +422,13 @@ int ref_asymptotic_variance(void* hp, int i, int j, double* out, char* err, int 
 // row_fold_out[K]: the held-out fold of each row under the selector's first
 // permutation (the one every step reuses after reseed()).  Grid: points_out /
 // values_out receive the grid (n_points).  log_out receives the drivers' log.
+// hyper_out: every variance parameter of the joint prior after the refit
+// (n_hyper of them; the auto search tunes each in turn when there are several).
 int ref_cross_validate(void* hp, int auto_search, int fold, int grid_steps, double lower, double upper,
                        double starting_variance, long seed, int conv_type, double tol, int max_iter,
                        int32_t* row_fold_out, double* points_out, double* values_out, int max_points,
                        int* n_points, double* variance_out, double* beta_out, double* ll_out, char* log_out,
-                       int log_len, char* err, int errlen) {
+                       int log_len, double* hyper_out, int max_hyper, int* n_hyper, char* err, int errlen) {
     auto h = static_cast<RefHandle*>(hp);
     try {
         CCDArguments args = CCDArguments();
@@ -470,7 +473,10 @@ int ref_cross_validate(void* hp, int auto_search, int fold, int grid_steps, doub
         driver->drive(*h->ccd, selector, args);
         driver->resetForOptimal(*h->ccd, selector, args);
         h->ccd->update(args.modeFinding);
-        *variance_out = h->ccd->getHyperprior()[0];
+        const std::vector<double> hyper = h->ccd->getHyperprior();
+        *variance_out = hyper[0];
+        *n_hyper = (int)hyper.size();
+        for (int i = 0; i < std::min<int>(max_hyper, (int)hyper.size()); ++i) hyper_out[i] = hyper[i];
         for (int j = 0; j < h->J; ++j) beta_out[j] = h->ccd->getBeta(j);
         *ll_out = h->ccd->getLogLikelihood();
         *n_points = 0;
@@ -532,6 +538,18 @@ int ref_predictive_estimates(void* hp, const double* w, double* y) {
     std::vector<double> wb;
     if (w) wb.assign(w, w + h->K);
     h->ccd->getPredictiveEstimates(y, w ? wb.data() : nullptr);
+    return 0;
+}
+
+// The auto search's quadratic fit (utils/HParSearch.cpp:22-64) on a history of
+// n points (x, mean, stdev); out: c0, c1, c2.
+int ref_quadr_log_fit(int n, const double* x, const double* m, const double* sd, double* out) {
+    std::map<double, UniModalSearch::MS> h;
+    for (int i = 0; i < n; ++i) h[x[i]] = UniModalSearch::MS(m[i], sd[i]);
+    const QuadrCoefs c = QuadrLogFit(h);
+    out[0] = c.c0;
+    out[1] = c.c1;
+    out[2] = c.c2;
     return 0;
 }
 

@@ -96,3 +96,38 @@ def test_swindle_with_no_active_column_keeps_the_last_count():
     (fa, aa, ba), (fb, ab, bb) = outs
     assert fa == fb and aa == ab == fa
     assert np.array_equal(ba, bb)
+
+
+@pytest.mark.parametrize("seed", range(300))
+def test_random_problem_calls_at_the_mode_bit_exact(seed):
+    """The operator calls on the fitted state of each random problem: every
+    column's (gradient, Hessian), xBeta, the log prior, and the Fisher
+    information over every column (refused alike on a weighted fit)."""
+    d, w, fit_kw = random_case(seed)
+    outs = []
+    for E in (checker.ReferenceEngine, checker.RestatementEngine):
+        e = E(d)
+        if w is not None:
+            e.set_weights(w)
+        try:
+            e.fit(**fit_kw)
+        except RuntimeError as ex:
+            outs.append(("error", str(ex)))
+            continue
+        gh = np.array([e.grad_hess(j) for j in range(d.J)]).reshape(d.J, 2)
+        try:
+            fi = e.fisher_information(np.arange(d.J, dtype=np.int32))
+        except checker.FisherRefused as ex:
+            fi = ("refused", str(ex))
+        outs.append((gh, e.xbeta(), e.log_prior(), fi))
+    a, b = outs
+    if isinstance(a[0], str) or isinstance(b[0], str):
+        assert a == b
+        return
+    assert np.array_equal(a[0], b[0], equal_nan=True)
+    assert np.array_equal(a[1], b[1], equal_nan=True)
+    assert a[2] == b[2] or (np.isnan(a[2]) and np.isnan(b[2]))
+    if isinstance(a[3], tuple) or isinstance(b[3], tuple):
+        assert a[3] == b[3]
+    else:
+        assert np.array_equal(a[3], b[3], equal_nan=True)

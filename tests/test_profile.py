@@ -131,3 +131,35 @@ def test_dobson_profile_bounds_are_the_exact_profile():
                 else:
                     b = m
             assert abs(bound - 0.5 * (a + b)) < 2e-3
+
+
+@needs_ref
+@pytest.mark.parametrize("seed", range(40))
+def test_profile_random_problems_match_the_reference(seed):
+    """Seeded random problems (tests/test_oracle_fuzz.py's generator: every
+    model, formats, mixed priors, an offset, weights with zeros): one or two
+    columns profiled, with or without the penalty, around the mode of a plain
+    fit; bounds, NaN where no sign change was found, and evaluation counts as
+    the reference's profileModel."""
+    from .test_oracle_fuzz import random_case
+    d, w, _ = random_case(seed)
+    rng = np.random.default_rng(10_000 + seed)
+    first = 1 if d.offset_col0 else 0
+    if d.J - first < 1:
+        pytest.skip("no coefficient column")
+    cols = sorted(rng.choice(np.arange(first, d.J), size=min(2, d.J - first), replace=False).tolist())
+    kw = dict(override_no_regularization=True, include_penalty=bool(rng.integers(2)))
+    ref = checker.ReferenceEngine(d)
+    e = checker.RestatementEngine(d)
+    if w is not None:
+        ref.set_weights(w)
+        e.set_weights(w)
+    r = ref.fit(GRADIENT, 1e-6)
+    if r["flag"] != 0 or not np.all(np.isfinite(r["beta"])):
+        pytest.skip("the plain fit has no finite mode")
+    lo, up, ev = ref.profile(cols, **kw)
+    e.fit(GRADIENT, 1e-6)
+    glo, gup, gev = inference.profile_bounds(OracleProfileBackend(e), d, cols, **kw)
+    np.testing.assert_allclose(glo, lo, rtol=1e-8, atol=1e-10)
+    np.testing.assert_allclose(gup, up, rtol=1e-8, atol=1e-10)
+    assert gev.tolist() == ev.tolist()
