@@ -568,15 +568,7 @@ def run_cv(args, world, rank, local):
         "higher_is_better": True, "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
         "dtype": "f32/f64 (f32 exp, ratios, per-entry terms; f64 state, reductions, step)" if mixed else "f64",
         "data": "synthetic (seeded PCG64, workload shapes of the benchmark config)",
-        "config": {"workload": "cv_grid" + ("_small" if args.small else "")
-                   + ("" if args.cv_columns == 20_000 else f"_{args.cv_columns}cols"), "model": "logistic",
-                   "rows": d.K, "columns": d.J, "nnz": d.nnz, "instances": len(var),
-                   "folds": 10, "variances": "20 log-uniform in [1e-4, 1] (Laplace)",
-                   "convergence": "gradient, tol 1e-6", "start": "cold (beta = 0) per instance",
-                   "precision": args.precision, "group": args.group or "engine's choice",
-                   "parallelism": f"instances round-robin over {world} GPUs" if world > 1 else "1 GPU",
-                   "step": "one grid of 200 fits to convergence",
-                   "l2": "flushed between timed steps (512 MiB device write)"},
+        "config": cv_config(args, d, len(var), world),
         "e2e": {"value": world * len(var) * args.steps / e2e_t, "unit": "fits/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "plain_fits_per_s": plain_n / plain_t if plain_n else None,
@@ -596,6 +588,78 @@ def run_cv(args, world, rank, local):
     if world > 1:
         tdist.barrier()
         tdist.destroy_process_group()
+
+
+def cv_config(args, d, instances: int, world: int) -> dict:
+    """The cv_grid workload's config, the same on both arms."""
+    return {"workload": "cv_grid" + ("_small" if args.small else "")
+            + ("" if args.cv_columns == 20_000 else f"_{args.cv_columns}cols"), "model": "logistic",
+            "rows": d.K, "columns": d.J, "nnz": d.nnz, "instances": instances,
+            "folds": 10, "variances": "20 log-uniform in [1e-4, 1] (Laplace)",
+            "convergence": "gradient, tol 1e-6", "start": "cold (beta = 0) per instance",
+            "precision": args.precision, "group": args.group or "engine's choice",
+            "parallelism": f"instances round-robin over {world} GPUs" if world > 1 else "1 GPU",
+            "step": "one grid of 200 fits to convergence",
+            "l2": "flushed between timed steps (512 MiB device write)"}
+
+
+CV_REF_FOLDS = 4  # folds of the split the reference arm fits per step
+
+
+def run_cv_reference(args, world, rank):
+    """The reference's own cross-validation on the host cores: its
+    GridSearchCrossValidationDriver (CcdInterface::runCrossValidation's grid
+    path) with one host thread per fold task, on a bounded sample of the grid: at the
+    smallest variance, the first 4 folds of the 10-fold split
+    (foldToCompute = 4), then the refit on all rows.  Those are the grid's
+    cheapest fits (the fewest sweeps), so the sample overstates the
+    reference's throughput on the whole grid."""
+    if rank != 0:
+        return
+    from oracle import checker
+    d, fold, hold, var = cv_workload(args.small, args.cv_columns)
+    lo = float(np.min(var))
+    # one thread per fold task: the driver clones the engine for every thread
+    # it is given, and more threads than tasks only add clones
+    threads = min(os.cpu_count() or 1, CV_REF_FOLDS)
+    eng_cls = checker.best_engine()
+    kind = "reference" if eng_cls is checker.ReferenceEngine else "port"
+    eng = eng_cls(d.with_prior(1, lo))
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        if kind == "reference":
+            eng.cross_validate(auto_search=False, fold=10, grid_steps=1, lower=lo, upper=lo, seed=7,
+                               threads=threads, fold_to_compute=CV_REF_FOLDS)
+        else:  # the oracle port has no driver: the same fits one after another
+            for h in range(CV_REF_FOLDS):
+                eng.set_weights((fold != h).astype(float))
+                eng.set_beta(cold_beta(d))
+                eng.fit(GRADIENT, 1e-6)
+            eng.set_weights(None)
+            eng.set_beta(cold_beta(d))
+            eng.fit(GRADIENT, 1e-6)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    eng.close()
+    total = float(np.sum(times))
+    v = (CV_REF_FOLDS + 1) * args.steps / total
+    sample = (f"per step: {CV_REF_FOLDS} of the 10 fold fits at the grid's smallest variance ({lo:g}) and "
+              f"the refit on all "
+              f"rows, {'the reference GridSearchCrossValidationDriver on ' + str(threads) + ' threads' if kind == 'reference' else 'one thread'}; "
+              f"the grid's cheapest fits, so this overstates the reference on the whole grid")
+    line = {
+        "impl": "reference", "metric": "converged fits/s", "value": v, "unit": "fits/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded PCG64, workload shapes of the benchmark config)",
+        "config": cv_config(args, d, len(var), 1),
+        "cpu_baseline": {"value": v, "unit": "fits/s", "cores": threads if kind == "reference" else 1,
+                         "kind": kind, "sample": sample},
+        "e2e": {"value": v, "unit": "fits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
 
 
 def cv_cpu_sample(d, fold, hold, var, res):
@@ -998,12 +1062,14 @@ def main():
     world, rank, local = dist_setup()
     if args.impl == "reference" and args.workload in VARIANTS:
         run_variant_reference(args, world, rank)
-    elif args.impl == "reference" and args.workload in ("cv_grid", "serve"):
+    elif args.impl == "reference" and args.workload == "cv_grid":
+        run_cv_reference(args, world, rank)
+    elif args.impl == "reference" and args.workload == "serve":
         if rank == 0:
             print(json.dumps({"impl": "reference", "workload": args.workload, "unavailable":
                               "no standalone reference arm for this workload: its CPU baseline needs the "
-                              "grid's sweep counts / the request trace of the GPU run and is reported as "
-                              "cpu_baseline in that run's line"}), flush=True)
+                              "request trace of the GPU run and is reported as cpu_baseline in that run's "
+                              "line"}), flush=True)
     elif args.impl == "reference":
         run_reference(args, world, rank)
     elif args.workload in VARIANTS:

@@ -237,7 +237,8 @@ class ReferenceEngine(_Engine):
 
     def cross_validate(self, auto_search: bool = True, fold: int = 10, grid_steps: int = 10,
                        lower: float = 0.01, upper: float = 20.0, starting_variance: float = -1.0,
-                       seed: int = 123, conv_type: int = 0, tol: float = 1e-6, max_iter: int = 1000):
+                       seed: int = 123, conv_type: int = 0, tol: float = 1e-6, max_iter: int = 1000,
+                       threads: int = 1, fold_to_compute: int = 0):
         """CcdInterface::runCrossValidation with one thread and cold starts:
         the reference selector's fold map, the grid (grid search), the drivers'
         log, the selected variance and the refit there."""
@@ -245,7 +246,7 @@ class ReferenceEngine(_Engine):
         fn = lib.ref_cross_validate
         fn.argtypes = [_P, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_long,
                        C.c_int, C.c_double, C.c_int, _P, _P, _P, C.c_int, _P, _P, _P, _P, C.c_char_p,
-                       C.c_int, _P, C.c_int, _P, C.c_char_p, C.c_int]
+                       C.c_int, _P, C.c_int, _P, C.c_int, C.c_int, C.c_char_p, C.c_int]
         row_fold = np.zeros(self.d.K, np.int32)
         pts, vals = np.zeros(max(grid_steps, 1)), np.zeros(max(grid_steps, 1))
         n = C.c_int()
@@ -257,7 +258,8 @@ class ReferenceEngine(_Engine):
         nh = C.c_int()
         rc = fn(self.h, int(auto_search), fold, grid_steps, lower, upper, starting_variance, seed, conv_type,
                 tol, max_iter, _ptr(row_fold), _ptr(pts), _ptr(vals), len(pts), C.byref(n), C.byref(var),
-                _ptr(beta), C.byref(ll), log, 1 << 24, _ptr(hyper), len(hyper), C.byref(nh), err, 512)
+                _ptr(beta), C.byref(ll), log, 1 << 24, _ptr(hyper), len(hyper), C.byref(nh), int(threads),
+                int(fold_to_compute), err, 512)
         if rc != 0:
             raise RuntimeError(err.value.decode())
         return {"row_fold": row_fold, "points": pts[:n.value], "values": vals[:n.value], "variance": var.value,

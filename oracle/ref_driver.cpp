@@ -418,7 +418,9 @@ int ref_asymptotic_variance(void* hp, int i, int j, double* out, char* err, int 
 // runs it: a CrossValidationSelector over the data's ids (by row for Cox, by
 // id otherwise, getDefaultSelectorTypeOrOverride :675-690), the auto-search or
 // grid driver, then resetForOptimal and the fit at the selected variance.
-// One thread and cold starts (resetCoefficients), so the run is deterministic.
+// Cold starts (resetCoefficients); with threads = 1 the run is deterministic
+// (more threads run the (fold, variance) tasks on clones of the engine).
+// fold_to_compute: the folds of the split actually fitted (0: all).
 // row_fold_out[K]: the held-out fold of each row under the selector's first
 // permutation (the one every step reuses after reseed()).  Grid: points_out /
 // values_out receive the grid (n_points).  log_out receives the drivers' log.
@@ -428,11 +430,12 @@ int ref_cross_validate(void* hp, int auto_search, int fold, int grid_steps, doub
                        double starting_variance, long seed, int conv_type, double tol, int max_iter,
                        int32_t* row_fold_out, double* points_out, double* values_out, int max_points,
                        int* n_points, double* variance_out, double* beta_out, double* ll_out, char* log_out,
-                       int log_len, double* hyper_out, int max_hyper, int* n_hyper, char* err, int errlen) {
+                       int log_len, double* hyper_out, int max_hyper, int* n_hyper, int threads,
+                       int fold_to_compute, char* err, int errlen) {
     auto h = static_cast<RefHandle*>(hp);
     try {
         CCDArguments args = CCDArguments();
-        args.threads = 1;
+        args.threads = threads > 0 ? threads : 1;
         args.resetCoefficients = true;
         args.seed = seed;
         args.useHierarchy = false;
@@ -441,7 +444,7 @@ int ref_cross_validate(void* hp, int auto_search, int fold, int grid_steps, doub
         args.crossValidation.doCrossValidation = true;
         args.crossValidation.useAutoSearchCV = auto_search != 0;
         args.crossValidation.fold = fold;
-        args.crossValidation.foldToCompute = fold;
+        args.crossValidation.foldToCompute = fold_to_compute > 0 ? fold_to_compute : fold;
         args.crossValidation.gridSteps = grid_steps;
         args.crossValidation.lowerLimit = lower;
         args.crossValidation.upperLimit = upper;

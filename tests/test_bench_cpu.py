@@ -29,9 +29,18 @@ def test_reference_arm_line_for_the_fisher_workload():
 
 
 def test_workloads_without_a_reference_arm_say_so():
-    for w in ("cv_grid", "serve"):
-        line = _bench("--impl", "reference", "--workload", w)
-        assert line["impl"] == "reference" and "unavailable" in line
+    line = _bench("--impl", "reference", "--workload", "serve")
+    assert line["impl"] == "reference" and "unavailable" in line
+
+
+def test_cv_reference_arm_runs_the_reference_driver():
+    """The cv_grid reference arm: the reference's grid-search driver on a
+    bounded sample (4 folds at the smallest variance and the refit)."""
+    line = _bench("--impl", "reference", "--workload", "cv_grid", "--small", "--steps", "1", "--warmup", "0")
+    assert line["impl"] == "reference" and line["unit"] == "fits/s" and line["value"] > 0
+    assert line["config"]["workload"] == "cv_grid_small"
+    assert line["cpu_baseline"]["kind"] in ("reference", "port")
+    assert line["e2e"]["h2d_bytes_per_step"] == 0
 
 
 def test_fisher_and_mm_byte_counts():
