@@ -722,7 +722,6 @@ def run_serve(args, world, rank, local):
     finally:
         srv.close()
     s = summaries[-1]
-    kinds = collections.Counter(int(d.model_type) for _, d in stream)
     h2d = sum(d.rows.nbytes + d.vals.nbytes + d.col_start.nbytes + d.val_start.nbytes + d.y.nbytes
               + (d.time.nbytes if d.time is not None else 0) + (d.stratum.nbytes if d.stratum is not None else 0)
               for _, d in stream)
@@ -733,14 +732,7 @@ def run_serve(args, world, rank, local):
         "warmup": args.warmup, "ms_per_step": 1e3 * s["makespan_s"], "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded PCG64 problems and arrival trace)",
-        "config": {"workload": "serve", "requests": len(stream), "arrivals": "Poisson, 50/s",
-                   "mix": {str(k): v for k, v in sorted(kinds.items())},
-                   "K": "log-uniform 1e3..1e5", "J": "log-uniform 1e2..1e4",
-                   "density": "uniform 0.001..0.02", "prior": "Laplace, variance 0.1",
-                   "slots": args.serve_slots, "hbm_budget_bytes": 150e9,
-                   "step": "replay of the whole stream; latency = completion - arrival",
-                   "strategy": "logistic: dependency-level sweeps on the slot's share of the SMs; "
-                               "grouped models: their engines"},
+        "config": serve_config(args, stream),
         "p99_s": s["p99_s"], "mean_s": s["mean_s"], "fits_per_s": s["fits_per_s"],
         "failed": s["failed"], "errors": dict(errors.most_common(5)), "peak_concurrent_fits": peak,
         "service_by_model": service,
@@ -750,10 +742,23 @@ def run_serve(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
-def serve_cpu_sample(stream, n: int = 40):
-    """The reference CPU engine serving the first n requests of the same trace:
-    FIFO over a pool of all host cores, each fit single-threaded, replayed at
-    the trace's arrival times."""
+def serve_config(args, stream) -> dict:
+    """The serve workload's config, the same on both arms."""
+    kinds = collections.Counter(int(d.model_type) for _, d in stream)
+    return {"workload": "serve", "requests": len(stream), "arrivals": "Poisson, 50/s",
+            "mix": {str(k): v for k, v in sorted(kinds.items())},
+            "K": "log-uniform 1e3..1e5", "J": "log-uniform 1e2..1e4",
+            "density": "uniform 0.001..0.02", "prior": "Laplace, variance 0.1",
+            "slots": args.serve_slots, "hbm_budget_bytes": 150e9,
+            "step": "replay of the whole stream; latency = completion - arrival",
+            "strategy": "logistic: dependency-level sweeps on the slot's share of the SMs; "
+                        "grouped models: their engines"}
+
+
+def _serve_cpu_latencies(stream, n: int):
+    """Latencies of the reference CPU engine serving the first n requests of
+    the trace: FIFO over a pool of all host cores, each fit single-threaded,
+    replayed at the trace's arrival times."""
     import concurrent.futures as cf
     from oracle import checker
     eng_cls = checker.best_engine()
@@ -778,9 +783,49 @@ def serve_cpu_sample(stream, n: int = 40):
                 time.sleep(delay)
             futs.append((t0 + t_arr, ex.submit(one, d)))
         lat = np.array([f.result() - a for a, f in futs])
+    return lat, cores, kind
+
+
+def serve_cpu_sample(stream, n: int = 40):
+    """The reference CPU engine serving the first n requests of the same trace
+    (the GPU line's cpu_baseline)."""
+    lat, cores, kind = _serve_cpu_latencies(stream, n)
     return {"value": float(np.percentile(lat, 50)), "unit": "s", "cores": cores, "kind": kind,
             "p99_s": float(np.percentile(lat, 99)),
-            "sample": f"first {len(sub)} requests of the same trace, FIFO over {cores} host threads"}
+            "sample": f"first {len(lat)} requests of the same trace, FIFO over {cores} host threads"}
+
+
+SERVE_REF_REQUESTS = 40  # requests of the trace the reference arm serves per step
+
+
+def run_serve_reference(args, world, rank):
+    """The reference CPU engine serving the same seeded trace: per step the
+    first 40 requests, replayed at their arrival times, FIFO over a pool of
+    all host cores (each fit single-threaded, as the reference's inner loop
+    is serial); the p50 latency over the timed steps' requests."""
+    if rank != 0:
+        return
+    stream = synthetic.serving_stream(args.serve_requests, seed=11, **SERVE_RANGES)
+    lats, spans, cores, kind = [], [], 1, "port"
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        lat, cores, kind = _serve_cpu_latencies(stream, SERVE_REF_REQUESTS)
+        if i >= args.warmup:
+            lats.extend(lat.tolist())
+            spans.append(time.perf_counter() - t0)
+    p50 = float(np.percentile(lats, 50))
+    line = {
+        "impl": "reference", "metric": "p50 fit latency", "value": p50, "unit": "s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(spans)),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded PCG64 problems and arrival trace)", "config": serve_config(args, stream),
+        "p99_s": float(np.percentile(lats, 99)),
+        "cpu_baseline": {"value": p50, "unit": "s", "cores": cores, "kind": kind,
+                         "sample": f"per step the first {SERVE_REF_REQUESTS} of the trace's {len(stream)} "
+                                   f"requests, FIFO over {cores} host threads"},
+        "e2e": {"value": p50, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
 
 
 # ------------------------------------------------------------------ variants
@@ -1065,11 +1110,7 @@ def main():
     elif args.impl == "reference" and args.workload == "cv_grid":
         run_cv_reference(args, world, rank)
     elif args.impl == "reference" and args.workload == "serve":
-        if rank == 0:
-            print(json.dumps({"impl": "reference", "workload": args.workload, "unavailable":
-                              "no standalone reference arm for this workload: its CPU baseline needs the "
-                              "request trace of the GPU run and is reported as cpu_baseline in that run's "
-                              "line"}), flush=True)
+        run_serve_reference(args, world, rank)
     elif args.impl == "reference":
         run_reference(args, world, rank)
     elif args.workload in VARIANTS:

@@ -28,9 +28,13 @@ def test_reference_arm_line_for_the_fisher_workload():
     assert line["cpu_baseline"]["kind"] in ("reference", "port") and line["cpu_baseline"]["cores"] == 1
 
 
-def test_workloads_without_a_reference_arm_say_so():
-    line = _bench("--impl", "reference", "--workload", "serve")
-    assert line["impl"] == "reference" and "unavailable" in line
+def test_serve_reference_arm_serves_the_same_trace():
+    """The serve reference arm: the reference CPU engine on the first requests
+    of the same seeded trace, FIFO over the host threads; p50 latency."""
+    line = _bench("--impl", "reference", "--workload", "serve", "--steps", "1", "--warmup", "0")
+    assert line["impl"] == "reference" and line["unit"] == "s" and line["value"] > 0
+    assert line["higher_is_better"] is False and line["config"]["workload"] == "serve"
+    assert line["cpu_baseline"]["kind"] in ("reference", "port")
 
 
 def test_cv_reference_arm_runs_the_reference_driver():
