@@ -178,3 +178,18 @@ def test_quadratic_fit_is_the_references_bit_for_bit(flat):
         sds = np.where(rng.random(n) < 0.1, 0.0, rng.uniform(0.1, 3.0, n))
         h = {float(x): (float(m), float(s)) for x, m, s in zip(xs, ms, sds)}
         assert cv.quadratic_log_fit(h) == checker.ReferenceEngine.quadr_log_fit(h)
+
+
+def test_variance_parameters_in_the_references_order():
+    """cv.variance_groups against the reference's getHyperprior(): a one-point
+    grid moves the first variance parameter to the grid's point and leaves the
+    others at the prior's values, in registration order."""
+    d = synthetic.small(MODEL_LOGISTIC, seed=170, K=300, P=6, prior=PRIOR_NONE)
+    d.prior_type[:] = [0, 2, 1, 2, 1, 0, 1]
+    d.prior_var[:] = [1.0, 2.0, 1.0, 2.0, 3.0, 1.0, 1.0]
+    groups = cv.variance_groups(d)
+    assert [g.tolist() for g in groups] == [[1, 3], [2, 6], [4]]
+    ref = checker.ReferenceEngine(d).cross_validate(auto_search=False, fold=3, grid_steps=1, lower=0.5,
+                                                    upper=0.5, seed=3)
+    assert ref["variances"].tolist() == [0.5, 1.0, 3.0]
+    np.testing.assert_array_equal(cv.column_variances(d, 0.5), [1.0, 0.5, 1.0, 0.5, 3.0, 1.0, 1.0])
