@@ -1,7 +1,8 @@
 """Seeded random problems, oracle against the reference engine compiled from
 source, bit for bit: random model, column formats and densities, per-column
 priors and variances, an offset, weights (with zeros), fixed columns, the
-convergence criterion, the algorithm (CCD, KKT swindle, MM where it runs)."""
+convergence criterion, the algorithm (CCD, KKT swindle, MM on the stratified
+models)."""
 import numpy as np
 import pytest
 
@@ -45,7 +46,7 @@ def random_case(seed):
         fixed[int(rng.integers(lo, d.J))] = 1
     fit_kw = dict(conv_type=int(rng.integers(0, 3)), tol=1e-7, fixed=fixed,
                   kkt_swindle=bool(rng.random() < 0.3))
-    if model in (MODEL_CONDITIONAL_LOGISTIC, MODEL_CONDITIONAL_POISSON) and rng.random() < 0.3:
+    if model in (MODEL_CONDITIONAL_LOGISTIC, MODEL_CONDITIONAL_POISSON, MODEL_COX) and rng.random() < 0.3:
         fit_kw["algorithm"] = 1
     return d, w, fit_kw
 
