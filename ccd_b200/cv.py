@@ -28,7 +28,8 @@ registered in column order, none for a flat column (variance_groups).  When
 every regularised column shares one prior -- a single prior type with some
 columns excluded, the usual set-up -- a variance is one launch of the batched
 engine for logistic and Poisson models.  Otherwise each (fold, variances)
-instance is a standalone device fit (native.Fit.fold_instances).  Every
+instance is a standalone device fit (native.Fit.fold_instances), which
+needs an FP64 fit.  Every
 column flat is refused as the R front end refuses it (createPrior,
 R/ModelFit.R:600-602); the engine's own driver would index a variance
 parameter that does not exist.

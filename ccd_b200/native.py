@@ -394,8 +394,10 @@ class Fit:
         fold's predictive log-likelihood when it succeeded
         (AbstractCrossValidationDriver.cpp:180-232).  Serves what one batched
         launch does not: several variance parameters, and the conditional
-        and Cox models.  The handle is left unweighted.  Returns
-        (beta[n, J], list of per-instance dicts, device seconds)."""
+        and Cox models.  Needs an FP64 handle (the mixed-precision engine
+        runs batched launches only; ccdb_find_mode refuses it).  The handle
+        is left unweighted.  Returns (beta[n, J], list of per-instance
+        dicts, device seconds)."""
         args = args or ModeFindingArguments()
         var = np.ascontiguousarray(variances, dtype=np.float64)
         if var.ndim != 2 or var.shape[1] != self.d.J:
