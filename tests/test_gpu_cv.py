@@ -126,3 +126,17 @@ def test_auto_search_two_variance_parameters(gpu_ctx, oracle_engine):
     dv.prior_var = cv.column_variances(d, got.variances)
     ref = oracle_engine(dv).fit(GRADIENT, 1e-6)
     assert np.max(np.abs(r.beta - ref["beta"])) <= 1e-6 * max(np.max(np.abs(ref["beta"])), 1e-8)
+
+
+def test_grid_search_two_variance_parameters(gpu_ctx, oracle_engine):
+    """The grid moves the first variance parameter only (standalone device
+    fits with per-column variances); the second keeps the prior's value."""
+    d, fold = _problem()
+    d.prior_type[13:] = PRIOR_NORMAL
+    d.prior_var[13:] = 2.0
+    m = native.Matrix(gpu_ctx, d)
+    got = cv.grid_search(native.Fit(gpu_ctx, m, d), fold, 5, lower=0.01, upper=10.0, steps=6)
+    want = cv.grid_search(OracleBatch(oracle_engine, d), fold, 5, lower=0.01, upper=10.0, steps=6)
+    assert got.variance == want.variance
+    for (v1, m1, _), (v2, m2, _) in zip(got.tried, want.tried):
+        assert v1 == v2 and m1 == pytest.approx(m2, rel=1e-8)
