@@ -16,6 +16,7 @@
 #include <cstdint>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <sstream>
 #include <stdexcept>
 #include <string>
@@ -48,9 +49,15 @@ struct ThrowingErrors : loggers::ErrorHandler {
 };
 
 // Keeps every line the cross-validation drivers log (their per-step summaries).
+// Worker threads of a multi-threaded cross-validation write lines concurrently
+// (AbstractCrossValidationDriver.cpp:196-235), so appends are serialised.
 struct RecordingLogger : loggers::ProgressLogger {
     std::string text;
-    void writeLine(const std::ostringstream& s) override { text += s.str() + "\n"; }
+    std::mutex lock;
+    void writeLine(const std::ostringstream& s) override {
+        std::lock_guard<std::mutex> g(lock);
+        text += s.str() + "\n";
+    }
     void yield() override {}
 };
 
