@@ -75,7 +75,7 @@ def parse():
                     help="cv_grid: covariate columns (fewer for short profiling captures)")
     ap.add_argument("--fp64-check", type=int, default=4,
                     help="cv_grid, mixed: instances also fitted by the FP64 engine to report the error")
-    ap.add_argument("--strategy", choices=["auto", "levels", "speculative"], default="auto",
+    ap.add_argument("--strategy", choices=["auto", "levels", "speculative", "grid_levels"], default="auto",
                     help="sweep strategy of the independent-row engine (CCDB_SWEEP_*)")
     ap.add_argument("--trace", default=None,
                     help="write a per-level timestamp trace of the last timed findMode's first "
@@ -830,7 +830,7 @@ def run_serve_reference(args, world, rank):
 
 # ------------------------------------------------------------------ variants
 VARIANTS = ("kkt_l1", "mm_clr", "fisher_l1")
-STRATEGIES = {"auto": 0, "levels": 1, "speculative": 2}
+STRATEGIES = {"auto": 0, "levels": 1, "speculative": 2, "grid_levels": 3}
 
 
 def variant_problem(name: str):

@@ -115,7 +115,7 @@ void Fit::release_schedule() {
     if (!sched) return;
     for (void* p : {(void*)sched->segs, (void*)sched->cta_seg, (void*)sched->tasks,
                     (void*)sched->level_need, (void*)sched->level_done, (void*)sched->col_arrive,
-                    (void*)sched->partials})
+                    (void*)sched->partials, (void*)sched->level_split})
         ctx->release(p);
     sched.reset();
 }
@@ -151,6 +151,7 @@ IndepParams Fit::params() const {
         P.level_need = sched->level_need;
         P.col_arrive = sched->col_arrive;
         P.partials = sched->partials;
+        P.level_split = sched->level_split;
     }
     return P;
 }
@@ -248,9 +249,46 @@ void Fit::download_beta() {
     check_cuda(cudaStreamSynchronize(stream), "beta sync");
 }
 
-void Fit::ensure_schedule() {
-    if (sched && sched->fixed == fixed) return;
+int Fit::sweep_kind(const ccdb_mode_args& a) const {
+    return a.strategy == CCDB_SWEEP_GRID_LEVELS ? kSchedGrid : kSchedCluster;
+}
+
+void Fit::ensure_schedule(int kind) {
+    if (sched && sched->fixed == fixed && sched->kind == kind) return;
     release_schedule();
+    if (kind == kSchedCluster) {
+        if (ctx->sweep_cluster < 0) {
+            int c = 0;
+            check_cuda(cluster_sweep_max_size(model, &c), "cluster occupancy");
+            ctx->sweep_cluster = c;
+        }
+        int C = ctx->sweep_cluster;
+        if (C < 1) throw Error(CCDB_ERR_CUDA, "the cluster sweep kernel cannot be resident");
+        while (ctx->max_ctas > 0 && C > ctx->max_ctas && C > 1) C /= 2;
+        ScheduleParams sp;
+        sp.n_cta = C;
+        sp.warps_per_cta = indep_threads() / 32;
+        sp.warp_max = 128;   // warp tasks stage 4 entries per lane
+        sp.cta_max = 4096;   // CTA tasks and chunks stage 8 entries per thread
+        sp.chunk = 4096;
+        std::vector<int64_t> entries(J);
+        for (int j = 0; j < J; ++j) entries[j] = m->entries(j);
+        auto s = std::make_unique<DevSchedule>();
+        s->fixed = fixed;
+        s->kind = kind;
+        s->cluster = C;
+        s->host = build_schedule(K, J, m->col_start.data(), m->rows_h.data(), m->fmt.data(),
+                                 fixed.data(), nullptr, K, entries.data(), sp);
+        if (s->host.max_split_per_seg > indep_max_split() || s->host.max_split_per_level > indep_max_split())
+            throw Error(CCDB_ERR_UNSUPPORTED, "too many split columns on one level");
+        s->segs = upload(ctx, s->host.segs.data(), s->host.segs.size(), stream);
+        s->cta_seg = upload(ctx, s->host.cta_seg.data(), s->host.cta_seg.size(), stream);
+        s->tasks = upload(ctx, s->host.tasks.data(), s->host.tasks.size(), stream);
+        s->level_split = upload(ctx, s->host.level_split.data(), s->host.level_split.size(), stream);
+        check_cuda(cudaStreamSynchronize(stream), "schedule upload");
+        sched = std::move(s);
+        return;
+    }
     int bps = 0;
     check_cuda(indep_sweep_occupancy(model, &bps), "occupancy");
     if (bps < 1) throw Error(CCDB_ERR_CUDA, "sweep kernel does not fit on an SM");
@@ -267,6 +305,7 @@ void Fit::ensure_schedule() {
     for (int j = 0; j < J; ++j) entries[j] = m->entries(j);
     auto s = std::make_unique<DevSchedule>();
     s->fixed = fixed;
+    s->kind = kind;
     s->host = build_schedule(K, J, m->col_start.data(), m->rows_h.data(), m->fmt.data(),
                              fixed.data(), nullptr, K, entries.data(), sp);
     if (s->host.max_split_per_seg > indep_max_split())
@@ -424,7 +463,8 @@ void Fit::find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* 
         *ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
         return;
     }
-    ensure_schedule();
+    const int kind = sweep_kind(a);
+    ensure_schedule(kind);
     if (sched->host.n_levels == 0) {
         // every coordinate is fixed: each cycle changes nothing, so the first
         // convergence check sees conv = 0 (findMode with an empty cycle)
@@ -438,16 +478,18 @@ void Fit::find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* 
     DevStatus zero{};
     zero.flag = R_FAIL;
     check_cuda(cudaMemcpyAsync(st, &zero, sizeof(zero), cudaMemcpyHostToDevice, stream), "status");
-    check_cuda(cudaMemsetAsync(sched->level_done, 0, sizeof(unsigned) * std::max(1, sched->host.n_levels), stream), "reset");
-    check_cuda(cudaMemsetAsync(sched->col_arrive, 0, sizeof(unsigned) * std::max(1, J), stream), "reset");
-    check_cuda(cudaMemsetAsync(grid_bar, 0, sizeof(unsigned), stream), "reset");
+    if (kind == kSchedGrid) {
+        check_cuda(cudaMemsetAsync(sched->level_done, 0, sizeof(unsigned) * std::max(1, sched->host.n_levels), stream), "reset");
+        check_cuda(cudaMemsetAsync(sched->col_arrive, 0, sizeof(unsigned) * std::max(1, J), stream), "reset");
+        check_cuda(cudaMemsetAsync(grid_bar, 0, sizeof(unsigned), stream), "reset");
+    }
     IndepParams P = params();
     P.conv = a.convergence_type;
     P.tol = a.tolerance;
     P.max_iter = a.max_iterations;
     // CCDB_TRACE_FILE=<path>: dump per-segment timestamps of the first sweep
     // together with the schedule (profiling aid; off by default)
-    const char* trace_path = std::getenv("CCDB_TRACE_FILE");
+    const char* trace_path = (kind == kSchedGrid) ? std::getenv("CCDB_TRACE_FILE") : nullptr;
     unsigned long long* d_trace = nullptr;
     const size_t n_seg = sched->host.segs.size();
     if (trace_path) {
@@ -457,7 +499,8 @@ void Fit::find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* 
         P.trace2 = d_trace + 3 * n_seg;
     }
     check_cuda(cudaEventRecord(ev0, stream), "event");
-    check_cuda(launch_indep_sweep(P, sched->host.n_cta, stream), "sweep launch");
+    if (kind == kSchedCluster) check_cuda(launch_cluster_sweep(P, sched->cluster, stream), "sweep launch");
+    else check_cuda(launch_indep_sweep(P, sched->host.n_cta, stream), "sweep launch");
     ++launches;
     check_cuda(cudaEventRecord(ev1, stream), "event");
     DevStatus out{};
@@ -588,7 +631,7 @@ void Fit::apply_step(int j, double delta) {
 // L1 fits, where most steps are zero and a batch of gradients advances many
 // coordinates per launch.
 bool Fit::use_speculative(const ccdb_mode_args& a) const {
-    if (a.strategy == CCDB_SWEEP_LEVELS) return false;
+    if (a.strategy == CCDB_SWEEP_LEVELS || a.strategy == CCDB_SWEEP_GRID_LEVELS) return false;
     if (a.strategy == CCDB_SWEEP_SPECULATIVE) return true;
     int active = 0, laplace = 0;
     for (int j = 0; j < J; ++j) {
@@ -1072,6 +1115,15 @@ int ccdb_set_fixed(ccdb_fit* f, const uint8_t* fixed) {
     });
 }
 
+int ccdb_fit_set_wait_limit(ccdb_fit* f, int64_t nanoseconds) {
+    return guard([&] {
+        require(f != nullptr, "NULL fit");
+        require(nanoseconds >= 0, "the wait limit must be >= 0");
+        f->wait_limit_ns = nanoseconds ? nanoseconds : Fit::kDefaultWaitNs;
+        f->xch_wait_ns = nanoseconds ? nanoseconds : Fit::kDefaultXchWaitNs;
+    });
+}
+
 int ccdb_get_last_call_seconds(const ccdb_fit* f, double* seconds) {
     return guard([&] {
         require(f && seconds, "NULL argument");
@@ -1287,8 +1339,10 @@ int ccdb_batch_find_mode(ccdb_fit* f, const ccdb_batch_desc* b, const ccdb_mode_
             }
             if (C > 1) P.split = (const int32_t*)keep(upload(ctx, split.data(), split.size(), s));
             P.stage_cap = max_slice <= 1024 ? 1024 : 3072;
-            P.queue = (int32_t*)keep(ctx->alloc(sizeof(int32_t)));
-            check_cuda(cudaMemsetAsync(P.queue, 0, sizeof(int32_t), s), "batch queue");
+            P.queue = (int32_t*)keep(ctx->alloc(sizeof(int32_t) * 2));
+            P.abort = P.queue + 1;
+            P.xch_wait_ns = f->xch_wait_ns;
+            check_cuda(cudaMemsetAsync(P.queue, 0, sizeof(int32_t) * 2, s), "batch queue");
             P.xg = (double*)keep(ctx->alloc(sizeof(double) * (size_t)K * G * n_groups));
             P.beta_g = (double*)keep(ctx->alloc(sizeof(double) * (size_t)J * G * n_groups));
             P.hd_g = (double*)keep(ctx->alloc(sizeof(double) * (size_t)J * G * n_groups));
@@ -1318,6 +1372,9 @@ int ccdb_batch_find_mode(ccdb_fit* f, const ccdb_batch_desc* b, const ccdb_mode_
         std::vector<BatchResult> res(n);
         check_cuda(cudaMemcpyAsync(res.data(), P.results, sizeof(BatchResult) * n, cudaMemcpyDeviceToHost, s),
                    "results");
+        int32_t aborted = 0;
+        if (P.abort)
+            check_cuda(cudaMemcpyAsync(&aborted, P.abort, sizeof(int32_t), cudaMemcpyDeviceToHost, s), "abort word");
         std::vector<double> bg;
         if (beta_out && mixed) {
             bg.resize((size_t)J * G * n_groups);
@@ -1347,9 +1404,10 @@ int ccdb_batch_find_mode(ccdb_fit* f, const ccdb_batch_desc* b, const ccdb_mode_
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         if (device_seconds) *device_seconds = ms * 1e-3;
-        for (int i = 0; i < n; ++i)
-            if (res[i].flag == kBatchTimeoutFlag)
-                throw Error(CCDB_ERR_CUDA, "batched fits: a bounded device wait between cluster CTAs ran out");
+        bool timed_out = aborted != 0;
+        for (int i = 0; i < n; ++i) timed_out |= (res[i].flag == kBatchTimeoutFlag);
+        if (timed_out)
+            throw Error(CCDB_ERR_TIMEOUT, "batched fits: a bounded wait for the other CTAs of a cluster ran out");
         if (results)
             for (int i = 0; i < n; ++i) {
                 results[i].return_flag = res[i].flag;

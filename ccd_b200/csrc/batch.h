@@ -74,6 +74,10 @@ struct BatchParams {
     int32_t pad4;
     const int32_t* split;
     int32_t* queue;            // mixed: next group to fit (zeroed before the launch)
+    // mixed, clusters: raised (set to 1) by a CTA whose wait for the other CTAs'
+    // column sums ran out; zeroed before the launch
+    int32_t* abort;
+    long long xch_wait_ns;     // mixed, clusters: bound on one exchange wait before abort
 };
 
 constexpr int kKeyRowBits = 24;

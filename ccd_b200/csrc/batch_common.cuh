@@ -249,7 +249,12 @@ __device__ __forceinline__ void inst_sum(const Inst<G>& I, double (&v)[NV], doub
 // which each sends only after consuming column j.
 
 constexpr int kMaxCluster = 16;
-constexpr unsigned long long kXchWaitNs = 2000000000ull;  // bound on one exchange wait
+// After a wait has run past the caller's bound (BatchParams::xch_wait_ns) and
+// raised the abort word, it keeps waiting up to this much longer before giving
+// up: peers that are slow but running still deliver, so every CTA of the
+// cluster finishes the sweep's exchanges in step and no st.async is left in
+// flight towards a CTA that leaves.
+constexpr unsigned long long kXchGiveUpNs = 2000000000ull;
 
 struct __align__(16) ColXch {  // st.async of two doubles needs 16-byte aligned slots
     double part[2][kMaxCluster][4][2];  // [slot][rank][instance][g, h]
@@ -270,10 +275,13 @@ __device__ __forceinline__ unsigned long long xch_now() {
     return t;
 }
 
-// Cluster-wide (g, h) of column j for the thread's instance; false when the
-// wait for the other CTAs' sums ran out (the caller stops the kernel).
+// Cluster-wide (g, h) of column j for the thread's instance.  A wait that runs
+// past `limit_ns` raises the launch's abort word (the caller then stops
+// stepping and reports a timeout) and goes on waiting up to kXchGiveUpNs;
+// false only when even that ran out (the sums are then not valid).
 template <int G>
-__device__ __forceinline__ bool xch_sum(const Inst<G>& I, double (&v)[2], ColXch& x, int j, unsigned& phase_bits) {
+__device__ __forceinline__ bool xch_sum(const Inst<G>& I, double (&v)[2], ColXch& x, int j, unsigned& phase_bits,
+                                        unsigned long long limit_ns, int32_t* abort) {
     const int slot = j & 1;
     if (I.sl == 0)
         for (int r = 0; r < I.C; ++r) {
@@ -295,6 +303,7 @@ __device__ __forceinline__ bool xch_sum(const Inst<G>& I, double (&v)[2], ColXch
     phase_bits ^= 1u << slot;
     const unsigned a = smem_addr(&x.bar[slot]);
     const unsigned long long t0 = xch_now();
+    bool raised = false;
     for (;;) {
         unsigned done;
         asm volatile(
@@ -304,7 +313,13 @@ __device__ __forceinline__ bool xch_sum(const Inst<G>& I, double (&v)[2], ColXch
             : "r"(a), "r"(parity)
             : "memory");
         if (done) break;
-        if (xch_now() - t0 > kXchWaitNs) return false;
+        const unsigned long long dt = xch_now() - t0;
+        if (!raised && dt > limit_ns) {
+            atomicExch(abort, 1);
+            __threadfence();
+            raised = true;
+        }
+        if (dt > limit_ns + kXchGiveUpNs) return false;
     }
     double sg = 0.0, sh = 0.0;  // rank order, own sums in place: the same bits in every CTA
     for (int r = 0; r < I.C; ++r) {

@@ -63,6 +63,7 @@ __global__ void __launch_bounds__(kMT, 1) batch_mixed_kernel(BatchParams P) {
     const int rank = (int)(blockIdx.x % C);
     const int n_groups = (P.n_inst + G - 1) / G;
     __shared__ int s_grp;
+    __shared__ int s_abv[2];  // per sweep parity: this CTA stopped or saw the abort word
     __shared__ InstCounters s_cnt[4];
     int rb2 = 0, rb4 = 0, xb2 = 0, xb4 = 0;
     unsigned xph = 0;  // parity bits of the exchange slots
@@ -87,7 +88,13 @@ __global__ void __launch_bounds__(kMT, 1) batch_mixed_kernel(BatchParams P) {
         const int g = I.g, sl = I.sl, hold = I.hold, J = I.J;
         double* X = I.X;
         inst_setup<G>(P, I, s_red2, rb2, s_xch2, xb2);  // ends with a cluster barrier
-        bool late = false;
+        // `late`: this thread's exchange gave up (sums not valid); `aborted`: some
+        // CTA's exchange wait ran past its bound.  Either way the group stops
+        // stepping but keeps exchanging to the end of the sweep, so every CTA of the
+        // cluster takes the same exchanges and barriers; after the sweep's closing
+        // cluster barrier every CTA reads the abort word and all leave together.
+        bool late = false, aborted = false;
+        int sweep_par = 0;
 
         const int j0 = P.offset_vals ? 1 : 0;
         const bool need_ll = P.conv != C_GRADIENT;
@@ -144,6 +151,8 @@ __global__ void __launch_bounds__(kMT, 1) batch_mixed_kernel(BatchParams P) {
 
             for (int j = j0; j < J; ++j) {
                 if (tr) tr[6 * j] = clock64();
+                // the abort word, read at the start of the column and tested at its end
+                const int ab = (I.C > 1 && threadIdx.x == 0) ? ld_volatile_i32(P.abort) : 0;
                 const MMeta m = s_meta[j & (kRing - 1)];
                 const int n = m.n;
                 const bool ind = (m.fmt == F_INDICATOR || m.fmt == F_INTERCEPT);
@@ -205,11 +214,13 @@ __global__ void __launch_bounds__(kMT, 1) batch_mixed_kernel(BatchParams P) {
                 double gh[2] = {(double)gs + (double)gc, (double)hs + (double)hc};
                 if (tr) tr[6 * j + 2] = clock64();
                 group_sum<G, 2>(gh, s_red2, rb2);
-                if (I.C > 1 && !xch_sum<G>(I, gh, s_xch, j, xph)) late = true;
+                if (I.C > 1 && !xch_sum<G>(I, gh, s_xch, j, xph, (unsigned long long)P.xch_wait_ns, P.abort))
+                    late = true;
                 if (tr) tr[6 * j + 3] = clock64();
 
                 // the step, computed identically by every thread of the instance
-                const double d = active ? inst_step<G>(I, j, m.ntot, gh[0], gh[1], b0, hd0, xjy0, pt, cnt) : 0.0;
+                const double d = (active && !late) ? inst_step<G>(I, j, m.ntot, gh[0], gh[1], b0, hd0, xjy0, pt, cnt)
+                                                   : 0.0;
                 // update xBeta (FP64) from the gathered registers
                 if (d != 0.0) {
                     if (staged) {
@@ -234,20 +245,34 @@ __global__ void __launch_bounds__(kMT, 1) batch_mixed_kernel(BatchParams P) {
                 if (threadIdx.x == 0 && j + kAhead + 1 < J) s_meta[(j + kAhead + 1) & (kRing - 1)] = I.cook(nm);
                 if (tr) tr[6 * j + 4] = clock64();
                 cp_async_wait_but_last();
-                if (__syncthreads_or(late)) {
-                    late = true;
-                    break;
+                if (__syncthreads_or(late || ab != 0)) {
+                    aborted = true;
+                    active = false;  // no more steps; the exchanges go on to the sweep's end
                 }
                 if (tr) tr[6 * j + 5] = clock64();
             }
             cp_async_wait_all();
-            if (late) break;
+            if (I.C > 1) {
+                // One decision for the whole cluster: every CTA publishes whether it
+                // stopped or sees the abort word raised (by any cluster), and after the
+                // barrier every CTA ORs the same C values.  Slots alternate by sweep.
+                namespace cg = cooperative_groups;
+                cg::cluster_group cl = cg::this_cluster();
+                if (threadIdx.x == 0) s_abv[sweep_par] = (aborted || ld_volatile_i32(P.abort) != 0) ? 1 : 0;
+                cl.sync();
+                int any = 0;
+                for (int r = 0; r < I.C; ++r) any |= *cl.map_shared_rank(&s_abv[sweep_par], r);
+                sweep_par ^= 1;
+                aborted = any != 0;
+                if (aborted) cl.sync();  // no CTA leaves while a peer still reads its slot
+            }
+            if (aborted) break;
 
             if (active) ++iteration;
             const double cur = inst_objective<MODEL, G>(P, I, active, need_ll, ll, s_red4, rb4, s_xch4, xb4);
             if (active) inst_converge(P, cur, last, iteration, flag, active);
         }
-        if (late) {  // a wait for the other CTAs' sums ran out: report, no more cluster barriers
+        if (aborted) {  // the same decision in every CTA of the cluster: report and leave
             if (I.exists && I.sl == 0 && I.rank == 0) {
                 BatchResult r{};
                 r.flag = kBatchTimeoutFlag;

@@ -34,6 +34,7 @@ struct Context {
     int device = 0;
     int n_sm = 0;
     int max_ctas = 0;  // persistent sweep grids: at most this many CTAs (0: n_sm)
+    int sweep_cluster = -1;  // largest resident cluster of the cluster sweep (-1: not queried)
     size_t budget = 0;
     size_t in_use = 0;
     cudaStream_t stream = nullptr;
@@ -70,6 +71,9 @@ struct Matrix {
 
 struct DevSchedule {
     std::vector<uint8_t> fixed;
+    int kind = 0;     // kSchedGrid or kSchedCluster
+    int cluster = 0;  // CTAs of the cluster sweep
+    uint8_t* level_split = nullptr;
     Schedule host;
     Seg* segs = nullptr;
     int64_t* cta_seg = nullptr;
@@ -110,7 +114,12 @@ struct Fit {
     int32_t J = 0;
     bool offset_col0 = false;
     cudaStream_t stream = nullptr;
-    long long wait_limit_ns = 20LL * 1000 * 1000 * 1000;
+    // bounds on device-side waits (ccdb_fit_set_wait_limit): the grid sweep's level,
+    // column and grid waits, and the mixed batch engine's cluster exchange
+    static constexpr long long kDefaultWaitNs = 20LL * 1000 * 1000 * 1000;
+    static constexpr long long kDefaultXchWaitNs = 2LL * 1000 * 1000 * 1000;
+    long long wait_limit_ns = kDefaultWaitNs;
+    long long xch_wait_ns = kDefaultXchWaitNs;
 
     // device state
     double2* row = nullptr;
@@ -150,7 +159,12 @@ struct Fit {
     ~Fit();
     IndepParams params() const;
     void release_schedule();
-    void ensure_schedule();
+    // kSchedGrid: the grid-wide persistent sweep (one CTA per SM, levels ordered
+    // by global counters); kSchedCluster: one cluster, levels ordered by cluster
+    // barriers
+    static constexpr int kSchedGrid = 0, kSchedCluster = 1;
+    void ensure_schedule(int kind);
+    int sweep_kind(const ccdb_mode_args& a) const;
     void apply_weights();
     void compute_xbeta();
     void compute_xbeta_transpose();  // the MM cycle's product (ModelSpecifics::computeXBeta(beta))

@@ -652,6 +652,320 @@ __global__ void __launch_bounds__(kThreads, 1) indep_sweep_kernel(IndepParams P)
     }
 }
 
+// ---------------------------------------------------------------- cluster sweep
+// One thread-block cluster of C CTAs (one per SM) runs a whole findMode.  The
+// levels of the schedule are separated by hardware cluster barriers
+// (barrier.cluster.arrive.release / wait.acquire), so a level costs one
+// barrier instead of a release/acquire round trip through global counters
+// across the whole GPU; a level holding a split column costs two, with the
+// CTAs' partial sums of that column exchanged through distributed shared
+// memory in between.  Every CTA runs the same sequence of barriers: the level
+// count, the per-level split flags and the convergence decision are the same
+// in every CTA, so no barrier can be left waiting.  There is no spin-wait.
+//
+// Per level, a CTA: (before the barrier that opens the level) loads the
+// metadata of its first tasks and prefetches their entries and row state;
+// then runs its CTA tasks (gather, CTA reduction, step, update), its warp
+// tasks (one column per warp) and the gather of its split-column chunks,
+// sending each chunk's partial (g, h) to every CTA of the cluster; after the
+// second barrier every chunk's CTA sums the C partials in rank order, so all
+// of them take the same step, and updates its own chunk.
+
+__device__ __forceinline__ void cl_arrive() { asm volatile("barrier.cluster.arrive.release;" ::: "memory"); }
+__device__ __forceinline__ void cl_wait() { asm volatile("barrier.cluster.wait.acquire;" ::: "memory"); }
+__device__ __forceinline__ unsigned cl_rank() {
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+// store v into CTA `rank`'s copy of the shared variable at p
+__device__ __forceinline__ void st_peer_d2(const void* p, unsigned rank, double2 v) {
+    unsigned a = (unsigned)__cvta_generic_to_shared(p), ra;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(a), "r"(rank));
+    asm volatile("st.shared::cluster.v2.f64 [%0], {%1, %2};" ::"r"(ra), "d"(v.x), "d"(v.y) : "memory");
+}
+
+// CTA-wide sum of (g, h) with a fixed combination order, returned to every
+// thread with identical bits: warp butterflies, one barrier, then every warp
+// combines the kWarps per-warp sums by the same half-warp butterfly.
+// red[2][kWarps] alternates buffers (`buf`), so consecutive calls need one
+// barrier each.
+__device__ __forceinline__ double2 cta_sum2(double2 v, double2 (*red)[kWarps], int& buf) {
+    v = warp_sum2(v);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) red[buf][wid] = v;
+    __syncthreads();
+    double2 t = (lane < kWarps) ? red[buf][lane] : make_double2(0.0, 0.0);
+#pragma unroll
+    for (int o = kWarps / 2; o > 0; o >>= 1) {
+        t.x += __shfl_xor_sync(0xffffffffu, t.x, o);
+        t.y += __shfl_xor_sync(0xffffffffu, t.y, o);
+    }
+    t.x = __shfl_sync(0xffffffffu, t.x, 0);
+    t.y = __shfl_sync(0xffffffffu, t.y, 0);
+    buf ^= 1;
+    return t;
+}
+
+// This CTA's share of the objective terms (rows [K r / C, K (r+1) / C)),
+// valid in every thread.
+template <int MODEL>
+__device__ double4 objective_share(const IndepParams& P, unsigned r, unsigned C, double4* s_red4) {
+    double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
+    const int64_t k0 = P.K * r / C, k1 = P.K * (r + 1) / C;
+    for (int64_t k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+        const double2 a = __ldcg(P.row + 2 * k);
+        const double2 dw = __ldcg(P.row + 2 * k + 1);
+        const double yk = P.y[k];
+        acc.x += (double)((int)yk) * a.x * dw.y;
+        if (MODEL == M_LOGISTIC) acc.y += dw.y * log(dw.x);
+        else acc.y += dw.y * dw.x;
+        acc.z += a.x * yk * dw.y;
+    }
+    const int64_t j0 = (int64_t)P.J * r / C, j1 = (int64_t)P.J * (r + 1) / C;
+    for (int64_t j = j0 + threadIdx.x; j < j1; j += blockDim.x)
+        acc.w += log_prior_one(__ldcg(P.beta + j), P.ptype[j], P.pvar[j]);
+    return block_sum4<kWarps>(acc, s_red4);
+}
+
+template <int MODEL>
+__global__ void __launch_bounds__(kThreads, 1) cluster_sweep_kernel(IndepParams P) {
+    __shared__ double4 s_red4[kWarps];
+    __shared__ double2 s_red2[2][kWarps];
+    __shared__ double2 s_split[kMaxSplit][kMaxClusterSweep];  // [slot][rank] chunk partials
+    __shared__ double2 s_obj[kMaxClusterSweep][2];             // [rank] objective terms
+    __shared__ double2 s_stash[kMaxSplit];  // {beta, hDelta} of this CTA's chunks, read in phase A
+    __shared__ ColMeta s_meta[kWarps + 1];
+    __shared__ Staged<kEw> s_wstage[kThreads];
+    extern __shared__ __align__(16) double2 s_gath[];
+
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const unsigned C = gridDim.x, rank = cl_rank();
+    const int64_t seg0 = P.cta_seg[rank], seg1 = P.cta_seg[rank + 1];
+    int rb = 0;
+
+    // the objective of the current state, combined in rank order in every CTA
+    auto objective_all = [&](double& ll) -> double4 {
+        const double4 o = objective_share<MODEL>(P, rank, C, s_red4);
+        if (tid < (int)C) {
+            st_peer_d2(&s_obj[rank][0], tid, make_double2(o.x, o.y));
+            st_peer_d2(&s_obj[rank][1], tid, make_double2(o.z, o.w));
+        }
+        cl_arrive();
+        cl_wait();
+        double4 t = make_double4(0.0, 0.0, 0.0, 0.0);
+        for (unsigned c = 0; c < C; ++c) {
+            t.x += s_obj[c][0].x;
+            t.y += s_obj[c][0].y;
+            t.z += s_obj[c][1].x;
+            t.w += s_obj[c][1].y;
+        }
+        ll = (t.x - t.y) + P.ll_fixed;
+        return t;
+    };
+    // every CTA of the cluster is running before any shared memory of a peer is written
+    cl_arrive();
+    cl_wait();
+    double ll0;
+    const double4 t0 = objective_all(ll0);
+    double last = (P.conv == C_GRADIENT) ? t0.z : (P.conv == C_MITTAL ? ll0 : ll0 + t0.w);
+    cl_arrive();  // s_obj is read; the first level's wait completes this barrier
+
+    for (int it = 0; it < P.max_iter; ++it) {
+        int64_t si = seg0;
+        for (int L = 0; L < P.n_levels; ++L) {
+            Seg sg{};
+            const bool mine = si < seg1 && P.segs[si].level == L;
+            if (mine) sg = P.segs[si];
+            const Task* T = P.tasks + sg.t0;
+            const int n_cl = sg.n_chunk + sg.n_cta;
+            const int qw0 = n_cl, qw1 = qw0 + sg.n_warp;
+
+            // ---- before the level opens: immutable entries, metadata of the first tasks
+            Task tc{}, tw{};
+            bool c_staged = false, w_has = false, w_staged = false;
+            int qw_first = -1;
+            if (mine) {
+                if (n_cl > 0) {
+                    tc = T[sg.n_cta > 0 ? sg.n_chunk : 0];  // the first CTA task, else the first chunk
+                    c_staged = stageable<kE>(tc, blockDim.x);
+                    if (c_staged) {
+                        Staged<kE> st;
+                        stage_entries(P, tc, tid, blockDim.x, st);
+                        prefetch_rows_l2(P, st);
+                    } else {
+                        prefetch_entries(P, tc, tid, blockDim.x);
+                    }
+                    if (tid == 0) s_meta[kWarps] = load_meta(P, tc.col);
+                }
+                if (sg.n_warp > 0) {
+                    for (int q0 = qw0; q0 < qw1 && qw_first < 0; q0 += 32) {
+                        const int q = q0 + lane;
+                        const bool own = (q < qw1) && (T[q].warp == wid);
+                        const unsigned bal = __ballot_sync(0xffffffffu, own);
+                        if (bal) qw_first = q0 + __ffs(bal) - 1;
+                    }
+                    if (qw_first >= 0) {
+                        w_has = true;
+                        tw = T[qw_first];
+                        w_staged = stageable<kEw>(tw, 32);
+                        if (w_staged) {
+                            Staged<kEw> st;
+                            stage_entries(P, tw, lane, 32, st);
+                            prefetch_rows_l2(P, st);
+                            s_wstage[tid] = st;
+                        } else {
+                            prefetch_entries(P, tw, lane, 32);
+                        }
+                        if (lane == 0) s_meta[wid] = load_meta(P, tw.col);
+                    }
+                }
+            }
+            cl_wait();  // the previous level (or the objective) is complete in every CTA
+            if (mine) {
+                __syncthreads();  // s_meta, s_wstage of this level
+                // ---- CTA tasks
+                for (int q = sg.n_chunk; q < n_cl; ++q) {
+                    const Task t = T[q];
+                    const bool first = (q == sg.n_chunk);
+                    const ColMeta m = first ? s_meta[kWarps] : load_meta(P, t.col);
+                    const uint8_t f = (uint8_t)m.fmt;
+                    const bool ind = (f == F_INDICATOR || f == F_INTERCEPT);
+                    const bool staged = first ? c_staged : stageable<kE>(t, blockDim.x);
+                    double g = 0.0, h = 0.0;
+                    Staged<kE> sc;
+                    if (staged) {
+                        stage_entries(P, t, tid, blockDim.x, sc);
+                        staged_gh_smem<MODEL>(P, ind, sc, s_gath, tid, g, h);
+                    } else {
+                        gh_dispatch<MODEL>(P, t.col, f, t.p0, t.p1, tid, blockDim.x, g, h);
+                    }
+                    const double2 s = cta_sum2(make_double2(g, h), s_red2, rb);
+                    double hd;
+                    const double d = meta_step(m, t.p1, s.x, s.y, hd);
+                    if (tid == 0) meta_write(P, t.col, m, d, hd);
+                    if (d != 0.0) {
+                        if (staged) staged_update_smem(P, sc, s_gath, tid, d);
+                        else update_dispatch(P, t.col, f, t.p0, t.p1, tid, blockDim.x, d);
+                    }
+                }
+                // ---- warp tasks
+                if (sg.n_warp > 0) {
+                    for (int q = (w_has ? qw_first : qw1); q < qw1; ++q) {
+                        const Task t = (q == qw_first) ? tw : T[q];
+                        if (t.warp != wid) continue;
+                        const ColMeta m = (q == qw_first) ? s_meta[wid] : load_meta(P, t.col);
+                        const uint8_t f = (uint8_t)m.fmt;
+                        const bool ind = (f == F_INDICATOR || f == F_INTERCEPT);
+                        const bool staged = (q == qw_first) ? w_staged : stageable<kEw>(t, 32);
+                        double g = 0.0, h = 0.0;
+                        Staged<kEw> sw;
+                        if (staged) {
+                            if (q == qw_first) sw = s_wstage[tid];
+                            else stage_entries(P, t, lane, 32, sw);
+                            staged_gh_smem<MODEL>(P, ind, sw, s_gath, tid, g, h);
+                        } else {
+                            gh_dispatch<MODEL>(P, t.col, f, t.p0, t.p1, lane, 32, g, h);
+                        }
+                        // the butterfly leaves the same sums in every lane: every lane
+                        // takes the same step
+                        const double2 s = warp_sum2(make_double2(g, h));
+                        double hd;
+                        const double d = meta_step(m, t.p1, s.x, s.y, hd);
+                        if (lane == 0) meta_write(P, t.col, m, d, hd);
+                        if (d != 0.0) {
+                            if (staged) staged_update_smem(P, sw, s_gath, tid, d);
+                            else update_dispatch(P, t.col, f, t.p0, t.p1, lane, 32, d);
+                        }
+                    }
+                }
+                // ---- split-column chunks: partial sums to every CTA of the cluster
+                for (int q = 0; q < sg.n_chunk; ++q) {
+                    const Task t = T[q];
+                    const ColMeta m = (q == 0 && sg.n_cta == 0) ? s_meta[kWarps] : load_meta(P, t.col);
+                    const uint8_t f = (uint8_t)m.fmt;
+                    const bool ind = (f == F_INDICATOR || f == F_INTERCEPT);
+                    double g = 0.0, h = 0.0;
+                    if (stageable<kE>(t, blockDim.x)) {
+                        Staged<kE> sc;
+                        stage_entries(P, t, tid, blockDim.x, sc);
+                        staged_gh_smem<MODEL>(P, ind, sc, s_gath, tid, g, h);
+                    } else {
+                        gh_dispatch<MODEL>(P, t.col, f, t.p0, t.p1, tid, blockDim.x, g, h);
+                    }
+                    const double2 s = cta_sum2(make_double2(g, h), s_red2, rb);
+                    if (tid == 0) s_stash[q] = make_double2(m.beta, m.hd);
+                    if (tid < (int)C) st_peer_d2(&s_split[t.slot][rank], tid, s);
+                }
+            }
+            if (P.level_split[L]) {
+                cl_arrive();
+                cl_wait();  // every chunk's partial has arrived
+                if (mine) {
+                    for (int q = 0; q < sg.n_chunk; ++q) {
+                        const Task t = T[q];
+                        double2 s = make_double2(0.0, 0.0);
+                        for (int c = 0; c < t.nchunks; ++c) {
+                            s.x += s_split[t.slot][c].x;
+                            s.y += s_split[t.slot][c].y;
+                        }
+                        ColMeta m = load_meta(P, t.col);
+                        m.beta = s_stash[q].x;  // read before any chunk's CTA could write them
+                        m.hd = s_stash[q].y;
+                        double hd;
+                        const double d = meta_step(m, 1, s.x, s.y, hd);  // split columns are never empty
+                        if (t.chunk == 0 && tid == 0) meta_write(P, t.col, m, d, hd);
+                        if (d != 0.0) {
+                            const uint8_t f = (uint8_t)m.fmt;
+                            if (q == sg.n_chunk - 1 && stageable<kE>(t, blockDim.x)) {
+                                // the last chunk's gathered state is still in this thread's slots
+                                Staged<kE> s2;
+                                stage_entries(P, t, tid, blockDim.x, s2);
+                                staged_update_smem(P, s2, s_gath, tid, d);
+                            } else {
+                                update_dispatch(P, t.col, f, t.p0, t.p1, tid, blockDim.x, d);
+                            }
+                        }
+                    }
+                }
+            }
+            cl_arrive();  // this CTA's updates of level L are released to the cluster
+            if (mine) ++si;
+        }
+        cl_wait();  // every level of the sweep is complete
+        double ll;
+        const double4 tot = objective_all(ll);
+        const int iteration = it + 1;
+        const double cur = (P.conv == C_GRADIENT) ? tot.z : (P.conv == C_MITTAL ? ll : ll + tot.w);
+        double conv;
+        bool ill = false;
+        if (cur != cur) {
+            conv = 0.0;
+            ill = true;
+        } else {
+            conv = fabs(cur - last) / (fabs(cur) + 1.0);
+        }
+        last = cur;
+        int done = 0, flag = R_SUCCESS;
+        if (P.tol > 0 && conv < P.tol) {
+            flag = ill ? R_ILLCONDITIONED : R_SUCCESS;
+            done = 1;
+        } else if (iteration == P.max_iter) {
+            flag = R_MAX_ITERATIONS;
+            done = 1;
+        }
+        if (rank == 0 && tid == 0) {
+            P.st->iterations = iteration;
+            P.st->objective = cur;
+            P.st->loglik = ll;
+            P.st->log_prior = tot.w;
+            if (done) P.st->flag = flag;
+        }
+        if (done) break;  // the same decision in every CTA: no barrier is left open
+        cl_arrive();      // s_obj is read; the next sweep's first wait completes this barrier
+    }
+}
+
 // ---------------------------------------------------------------- per-coordinate kernels
 
 template <int MODEL>
@@ -820,6 +1134,71 @@ cudaError_t launch_indep_sweep(const IndepParams& P, int n_cta, cudaStream_t str
     cudaError_t e = indep_sweep_smem_attr();
     if (e != cudaSuccess) return e;
     return cudaLaunchCooperativeKernel(fn, dim3(n_cta), dim3(kThreads), args, kGatherSmem, stream);
+}
+
+template <int MODEL>
+static cudaError_t cluster_attrs() {
+    cudaError_t e = cudaFuncSetAttribute(cluster_sweep_kernel<MODEL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kGatherSmem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(cluster_sweep_kernel<MODEL>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+}
+
+template <int MODEL>
+static cudaError_t cluster_config(int C, cudaStream_t stream, cudaLaunchConfig_t& cfg, cudaLaunchAttribute* at) {
+    cfg = cudaLaunchConfig_t{};
+    cfg.gridDim = dim3(C);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = kGatherSmem;
+    cfg.stream = stream;
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cluster_attrs<MODEL>();
+}
+
+cudaError_t cluster_sweep_max_size(int model, int* cluster) {
+    *cluster = 0;
+    for (int C = kMaxClusterSweep; C >= 1; C /= 2) {
+        cudaLaunchConfig_t cfg;
+        cudaLaunchAttribute at[1];
+        int n = 0;
+        cudaError_t e;
+        if (model == M_LOGISTIC) {
+            e = cluster_config<M_LOGISTIC>(C, 0, cfg, at);
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveClusters(&n, cluster_sweep_kernel<M_LOGISTIC>, &cfg);
+        } else {
+            e = cluster_config<M_POISSON>(C, 0, cfg, at);
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveClusters(&n, cluster_sweep_kernel<M_POISSON>, &cfg);
+        }
+        if (e != cudaSuccess) {
+            cudaGetLastError();  // an unsupported size is not an error here: try the next
+            continue;
+        }
+        if (n >= 1) {
+            *cluster = C;
+            return cudaSuccess;
+        }
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_cluster_sweep(const IndepParams& P, int C, cudaStream_t stream) {
+    if (C < 1 || C > kMaxClusterSweep) return cudaErrorInvalidValue;
+    cudaLaunchConfig_t cfg;
+    cudaLaunchAttribute at[1];
+    cudaError_t e;
+    if (P.model == M_LOGISTIC) {
+        e = cluster_config<M_LOGISTIC>(C, stream, cfg, at);
+        if (e != cudaSuccess) return e;
+        return cudaLaunchKernelEx(&cfg, cluster_sweep_kernel<M_LOGISTIC>, P);
+    }
+    e = cluster_config<M_POISSON>(C, stream, cfg, at);
+    if (e != cudaSuccess) return e;
+    return cudaLaunchKernelEx(&cfg, cluster_sweep_kernel<M_POISSON>, P);
 }
 
 cudaError_t launch_indep_gh(const IndepParams& P, int j, int64_t entries, double2* parts,

@@ -51,12 +51,20 @@ struct IndepParams {
     unsigned long long* trace;
     // finer points: trace2[2*si] = end of phase 1, trace2[2*si+1] = last warp's end of phase 2
     unsigned long long* trace2;
+    // cluster sweep: per level, 1 when it holds a split column (a second cluster barrier)
+    const uint8_t* level_split;
 };
 
 int indep_threads();
 int indep_max_split();
 cudaError_t indep_sweep_occupancy(int model, int* blocks_per_sm);
 cudaError_t launch_indep_sweep(const IndepParams& P, int n_cta, cudaStream_t stream);
+// The cluster sweep: one thread-block cluster of `cluster` CTAs runs the whole
+// findMode, levels separated by hardware cluster barriers.
+constexpr int kMaxClusterSweep = 16;
+// largest cluster size (16, 8, 4, 2, 1) of which one can be resident; 0 if none
+cudaError_t cluster_sweep_max_size(int model, int* cluster);
+cudaError_t launch_cluster_sweep(const IndepParams& P, int cluster, cudaStream_t stream);
 cudaError_t launch_indep_gh(const IndepParams& P, int j, int64_t entries, double2* parts,
                             int max_parts, double2* out, cudaStream_t stream);
 cudaError_t launch_indep_gh_batch(const IndepParams& P, const int32_t* cols, int ncols, double2* out,

@@ -104,6 +104,7 @@ Schedule build_schedule(int64_t K, int32_t J, const int64_t* col_start, const in
             return idx;
         };
         // split columns: chunks on distinct CTAs
+        int32_t slot = 0;
         for (int32_t j : big) {
             const int64_t e = entries_of[j];
             const int C = (int)std::min<int64_t>((e + sp.chunk - 1) / sp.chunk, G);
@@ -119,11 +120,15 @@ Schedule build_schedule(int64_t K, int32_t J, const int64_t* col_start, const in
                 t.part_base = s.n_partials;
                 t.p0 = e * c / C;
                 t.p1 = e * (c + 1) / C;
+                t.slot = slot;
                 chunk_t[ctas[c]].push_back(t);
                 load[ctas[c]] += (t.p1 - t.p0) / threads + 2.0;
             }
             s.n_partials += C;
+            ++slot;
         }
+        s.level_split.push_back(slot > 0 ? 1 : 0);
+        s.max_split_per_level = std::max<int64_t>(s.max_split_per_level, slot);
         for (int32_t j : mid) {
             auto c = least_loaded(1)[0];
             Task t{};

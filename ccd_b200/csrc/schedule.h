@@ -35,7 +35,9 @@ struct Schedule {
     std::vector<int64_t> cta_seg;    // n_cta + 1 offsets into segs
     std::vector<int32_t> level_need; // CTAs active per level
     std::vector<int32_t> col_chunks; // J: number of chunks (0 = not split)
+    std::vector<uint8_t> level_split; // n_levels: the level holds a split column
     int64_t max_split_per_seg = 0;
+    int64_t max_split_per_level = 0;
 };
 
 // key_of_row: the conflict key of each row (row id for independent-row models,

@@ -24,7 +24,7 @@ struct Task {
     int32_t chunk, nchunks;
     int32_t part_base;  // first partial slot of the split column
     int32_t p0, p1;     // entry range within the column
-    int32_t pad;
+    int32_t slot;       // split columns: index among the level's split columns
 };
 static_assert(sizeof(Task) == 32, "Task layout");
 

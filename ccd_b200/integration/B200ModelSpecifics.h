@@ -186,6 +186,19 @@ public:
         return new B200ModelSpecifics(data_, modelType_, device_);
     }
 
+    // For B200CyclicCoordinateDescent, which runs a whole findMode in one
+    // ccdb_find_mode call on this fit: the handle, and the mode the device now
+    // holds (its xBeta and remaining statistics already match these
+    // coefficients, so no ccdb_set_beta follows).
+    ccdb_fit* handle() {
+        sync_beta();
+        return fit_;
+    }
+    void adopt_device_beta(const std::vector<double>& beta) {
+        beta_ = beta;
+        dirty_ = false;
+    }
+
 protected:
     void deviceInitialization() override {}
     bool allocateXjY() override { return true; }

@@ -26,7 +26,7 @@ OK = 0
 ERR_INVALID, ERR_CUDA, ERR_UNSUPPORTED, ERR_BUDGET, ERR_TIMEOUT = -1, -2, -3, -4, -5
 ALGORITHM_CCD, ALGORITHM_MM = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
-SWEEP_AUTO, SWEEP_LEVELS, SWEEP_SPECULATIVE = 0, 1, 2
+SWEEP_AUTO, SWEEP_LEVELS, SWEEP_SPECULATIVE, SWEEP_GRID_LEVELS = 0, 1, 2, 3
 
 
 class CcdbError(RuntimeError):
@@ -140,6 +140,7 @@ def lib() -> C.CDLL:
         L.ccdb_compute_mm_gradient_hessian.argtypes = [_P, _P, _P, _P]
         L.ccdb_get_last_call_seconds.argtypes = [_P, _P]
         L.ccdb_set_fixed.argtypes = [_P, _P]
+        L.ccdb_fit_set_wait_limit.argtypes = [_P, C.c_int64]
         L.ccdb_matrix_validate.argtypes = [C.c_int64, C.c_int32, _P, _P, _P, _P, _P]
         _lib = L
     return _lib
@@ -337,6 +338,11 @@ class Fit:
         """setFixedBeta for every column (the offset stays fixed)."""
         fx = _c(fixed, np.uint8)
         _check(lib().ccdb_set_fixed(self.h, _p(fx)))
+
+    def set_wait_limit(self, nanoseconds: int) -> None:
+        """Bound on every single device-side wait of later launches (0: the
+        defaults, 20 s for the grid sweep, 2 s for the batch exchange)."""
+        _check(lib().ccdb_fit_set_wait_limit(self.h, int(nanoseconds)))
 
     def last_call_seconds(self) -> float:
         """Device time of the kernels of the last compute_fisher_information."""

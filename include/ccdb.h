@@ -194,8 +194,9 @@ typedef struct {
 #define CCDB_ALGORITHM_MM 1
 
 #define CCDB_SWEEP_AUTO 0
-#define CCDB_SWEEP_LEVELS 1
+#define CCDB_SWEEP_LEVELS 1        /* one thread-block cluster, levels ordered by cluster barriers */
 #define CCDB_SWEEP_SPECULATIVE 2
+#define CCDB_SWEEP_GRID_LEVELS 3   /* one CTA per SM, levels ordered by global counters */
 
 typedef struct {
     int32_t return_flag;        /* UpdateReturnFlags */
@@ -299,6 +300,16 @@ int ccdb_column_gradient_hessian_noalloc(int32_t model_type, int32_t fmt, int64_
  * violation in ccdb_last_error.  Host-only: needs no GPU. */
 int ccdb_matrix_validate(int64_t K, int32_t J, const int64_t* col_start, const int32_t* rows,
                          const int64_t* val_start, const double* vals, const uint8_t* fmt);
+
+/* Bound, in nanoseconds, on every single device-side wait of this fit's later
+ * launches: the grid-wide level sweep's waits for a level, a split column and
+ * the grid barrier (default 20 s), and the mixed batch engine's wait for the
+ * per-column sums of the other CTAs of its cluster (default 2 s).  0 restores
+ * the defaults.  A wait that runs out ends the call with CCDB_ERR_TIMEOUT and
+ * leaves the context usable; the fit's state is then undefined until the next
+ * ccdb_set_beta or ccdb_find_mode with starting values.  The cluster sweep
+ * (CCDB_SWEEP_LEVELS) has no such wait.  No reference counterpart. */
+int ccdb_fit_set_wait_limit(ccdb_fit* f, int64_t nanoseconds);
 
 /* Device time (CUDA events on the fit's stream) of the kernels of the fit's last
  * ccdb_fisher_information call, in seconds; copies to and from the host are

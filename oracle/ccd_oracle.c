@@ -30,6 +30,36 @@ enum { R_SUCCESS = 0, R_MAX_ITERATIONS = 2, R_ILLCONDITIONED = 3 };
 
 #define ORC_PI 3.14159265358979323851280895940618620443274267017841339111328125
 
+/* Test hook: a copy of the arithmetic with exp moved by one unit in the last
+ * place on a deterministic pseudo-random share of its arguments (2 in
+ * `one_in`, chosen by a hash of the argument's bits and `salt`; 0 turns it
+ * off).  Parity tests use it to see whether a problem's result is decided by
+ * rounding: glibc's exp itself is not correctly rounded on every argument,
+ * and the CUDA engine's exp is a different implementation, so a result that
+ * moves when exp moves by one ulp cannot be held to a tolerance tighter than
+ * that movement.  Off by default; nothing in the product calls it. */
+static unsigned g_exp_one_in = 0, g_exp_salt = 0;
+void orc_set_exp_perturbation(unsigned one_in, unsigned salt) {
+    g_exp_one_in = one_in;
+    g_exp_salt = salt;
+}
+static double orc_exp(double x) {
+    double r = exp(x);
+    if (g_exp_one_in == 0) return r;
+    uint64_t b;
+    memcpy(&b, &x, sizeof b);
+    b ^= (uint64_t)g_exp_salt * 0x9e3779b97f4a7c15ULL;
+    b ^= b >> 33;
+    b *= 0xff51afd7ed558ccdULL;
+    b ^= b >> 33;
+    b *= 0xc4ceb9fe1a85ec53ULL;
+    b ^= b >> 33;
+    const unsigned m = (unsigned)(b % g_exp_one_in);
+    if (m == 0) return nextafter(r, INFINITY);
+    if (m == 1) return nextafter(r, -INFINITY);
+    return r;
+}
+
 typedef struct {
     int model;
     int64_t K;
@@ -260,8 +290,8 @@ static void acc_denominator(Orc* o) {
 static void remaining_statistics(Orc* o) {
     for (int i = 0; i < o->N; ++i) o->denom[i] = null_denom(o);
     for (int64_t k = 0; k < o->K; ++k) {
-        o->e[k] = exp(o->xb[k]);
-        if (is_cox(o)) o->denom[group_of(o, k)] += o->w ? o->kw[k] * exp(o->xb[k]) : exp(o->xb[k]);
+        o->e[k] = orc_exp(o->xb[k]);
+        if (is_cox(o)) o->denom[group_of(o, k)] += o->w ? o->kw[k] * orc_exp(o->xb[k]) : orc_exp(o->xb[k]);
         else o->denom[group_of(o, k)] += o->e[k];
     }
     acc_denominator(o);
@@ -469,12 +499,12 @@ static void update_xbeta_ms(Orc* o, int j, double delta) {
         int g = group_of(o, k);
         if (is_cox(o)) {
             double oldE = o->w ? o->kw[k] * o->e[k] : o->e[k];
-            o->e[k] = exp(o->xb[k]);
+            o->e[k] = orc_exp(o->xb[k]);
             double newE = o->w ? o->kw[k] * o->e[k] : o->e[k];
             o->denom[g] += (newE - oldE);
         } else {
             double oldE = o->e[k];
-            double newE = o->e[k] = exp(o->xb[k]);
+            double newE = o->e[k] = orc_exp(o->xb[k]);
             o->denom[g] += (newE - oldE);
         }
     }
@@ -1087,7 +1117,7 @@ int orc_predictive_loglik(void* hp, const double* w, double* out) {
             ll += yk * wk * (xbk - log(o->denom[k]));
             break;
         case MT_POISSON:
-            ll += (yk * xbk - exp(xbk)) * wk;
+            ll += (yk * xbk - orc_exp(xbk)) * wk;
             break;
         case MT_CLR:
         case MT_CPR:
@@ -1226,10 +1256,10 @@ int orc_predictive_estimates(void* hp, const double* w, double* y) {
         if (w && !w[k]) continue;
         const double xb = o->xb[k];
         if (o->model == MT_LOGISTIC) {
-            const double t = exp(xb);
+            const double t = orc_exp(xb);
             y[k] = t / (t + 1.0);
         } else if (o->model == MT_POISSON) {
-            y[k] = exp(xb);
+            y[k] = orc_exp(xb);
         } else {
             y[k] = xb;
         }

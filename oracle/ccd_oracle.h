@@ -42,6 +42,8 @@ int orc_num_patients(void* h);
 int orc_fisher_information(void* h, const int32_t* idx, int n, double* out);
 /* predictEstimate per row; rows whose weight is zero keep y (w may be NULL). */
 int orc_predictive_estimates(void* h, const double* w, double* y);
+/* Test hook: exp moved by one ulp on 2 in one_in arguments (0: off); see ccd_oracle.c. */
+void orc_set_exp_perturbation(unsigned one_in, unsigned salt);
 /* Cox grouping as setPidForAccumulation computes it: group id per row (N for
  * dropped rows), the stratum-start list accReset, returns N. */
 int orc_cox_groups(void* h, int32_t* group_out, int32_t* acc_reset_out, int* n_reset_out);

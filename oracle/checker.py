@@ -77,7 +77,14 @@ class _Engine:
                 lib.orc_fisher_information.argtypes = [_P, _P, C.c_int, _P]
             getattr(lib, p + "predictive_estimates").argtypes = [_P, _P, _P]
             _Engine._lib_cache[cls.libpath] = lib
-        return _Engine._lib_cache[cls.libpath]
+        lib = _Engine._lib_cache[cls.libpath]
+        # engines sharing a library may use different constructors
+        cname = cls.create_name or (cls.prefix + "create")
+        fn = getattr(lib, cname)
+        if fn.restype is not _P:
+            fn.restype = _P
+            fn.argtypes = [C.c_int, C.c_int, C.c_int64, C.c_int] + [_P] * 8 + [C.c_int, _P, _P, C.c_char_p, C.c_int]
+        return lib
 
     def __init__(self, d, fp32: bool = False):
         self.d = d
@@ -294,9 +301,32 @@ class ReferenceOnB200Engine(ReferenceEngine):
     create_name = "ref_create_b200"
 
 
+class ReferenceOnB200FusedEngine(ReferenceEngine):
+    """The reference's solver as B200CyclicCoordinateDescent
+    (ccd_b200/integration/B200CyclicCoordinateDescent.h): each findMode of
+    update() is one ccdb_find_mode call on the device."""
+    prefix = "ref_"
+    libpath = REF_B200_LIB
+    create_name = "ref_create_b200_fused"
+
+    def device_calls(self) -> int:
+        fn = self.lib().ref_device_calls
+        fn.argtypes = [_P]
+        fn.restype = C.c_int64
+        return int(fn(self.h))
+
+
 class RestatementEngine(_Engine):
     prefix = "orc_"
     libpath = PORT_LIB
+
+    @classmethod
+    def set_exp_perturbation(cls, one_in: int, salt: int = 0):
+        """Move exp by one ulp on 2 in `one_in` arguments (0: off), for every
+        restatement engine of the process (see orc_set_exp_perturbation)."""
+        fn = cls.lib().orc_set_exp_perturbation
+        fn.argtypes = [C.c_uint, C.c_uint]
+        fn(int(one_in), int(salt))
 
 
 def best_engine():

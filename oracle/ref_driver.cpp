@@ -33,6 +33,7 @@
 #include "priors/CovariatePrior.h"
 #include "utils/HParSearch.h"
 #ifdef CCDB_B200_ADAPTER
+#include "B200CyclicCoordinateDescent.h"
 #include "B200ModelSpecifics.h"
 #endif
 
@@ -95,6 +96,9 @@ struct RefHandle {
     std::unique_ptr<AbstractModelSpecifics> ms;
     priors::JointPriorPtr prior;
     std::unique_ptr<CyclicCoordinateDescent> ccd;
+#ifdef CCDB_B200_ADAPTER
+    B200CyclicCoordinateDescent* fused = nullptr;  // ccd, when it is the fused solver
+#endif
     int J = 0;
     int64_t K = 0;
     bool weighted = false;
@@ -178,7 +182,7 @@ extern "C" {
 // Build ModelData + ModelSpecifics + MixtureJointPrior + CyclicCoordinateDescent.
 // model_type uses the reference's ModelType numbering (Types.h:134-147).
 // prior_type per column: 0 none, 1 Laplace, 2 Normal (priors::PriorType, Types.h:100-105).
-static void* create_impl(bool on_b200, int model_type, int fp32, int64_t K, int J, const double* y,
+static void* create_impl(bool on_b200, bool fused, int model_type, int fp32, int64_t K, int J, const double* y,
                          const double* time, const int64_t* stratum, const int64_t* col_start,
                          const int32_t* rows, const int64_t* val_start, const double* vals,
                          const uint8_t* fmt, int offset_col0, const int32_t* prior_type,
@@ -224,7 +228,19 @@ static void* create_impl(bool on_b200, int model_type, int fp32, int64_t K, int 
         auto mix = std::make_shared<priors::MixtureJointPrior>(getPrior(prior_type[0], prior_var[0]), J);
         for (int j = 1; j < J; ++j) mix->changePrior(getPrior(prior_type[j], prior_var[j]), j);
         h->prior = mix;
-        h->ccd.reset(new CyclicCoordinateDescent(*h->data, *h->ms, h->prior, h->log, h->err));
+        if (fused) {
+#ifdef CCDB_B200_ADAPTER
+            auto* c = new B200CyclicCoordinateDescent(
+                *h->data, static_cast<B200ModelSpecifics&>(*h->ms), h->prior, h->log, h->err,
+                std::vector<int32_t>(prior_type, prior_type + J), std::vector<double>(prior_var, prior_var + J));
+            h->fused = c;
+            h->ccd.reset(c);
+#else
+            throw std::runtime_error("built without the B200 adapter");
+#endif
+        } else {
+            h->ccd.reset(new CyclicCoordinateDescent(*h->data, *h->ms, h->prior, h->log, h->err));
+        }
         h->ccd->setNoiseLevel(SILENT);
         return h;
     } catch (const std::exception& e) {
@@ -237,7 +253,7 @@ void* ref_create(int model_type, int fp32, int64_t K, int J, const double* y, co
                  const int64_t* stratum, const int64_t* col_start, const int32_t* rows,
                  const int64_t* val_start, const double* vals, const uint8_t* fmt, int offset_col0,
                  const int32_t* prior_type, const double* prior_var, char* err, int errlen) {
-    return create_impl(false, model_type, fp32, K, J, y, time, stratum, col_start, rows, val_start,
+    return create_impl(false, false, model_type, fp32, K, J, y, time, stratum, col_start, rows, val_start,
                        vals, fmt, offset_col0, prior_type, prior_var, err, errlen);
 }
 
@@ -247,8 +263,29 @@ void* ref_create_b200(int model_type, int fp32, int64_t K, int J, const double* 
                       const int64_t* stratum, const int64_t* col_start, const int32_t* rows,
                       const int64_t* val_start, const double* vals, const uint8_t* fmt, int offset_col0,
                       const int32_t* prior_type, const double* prior_var, char* err, int errlen) {
-    return create_impl(true, model_type, fp32, K, J, y, time, stratum, col_start, rows, val_start,
+    return create_impl(true, false, model_type, fp32, K, J, y, time, stratum, col_start, rows, val_start,
                        vals, fmt, offset_col0, prior_type, prior_var, err, errlen);
+}
+
+// The same, with B200CyclicCoordinateDescent (ccd_b200/integration) as the
+// solver: every findMode of update() is one ccdb_find_mode on the device.
+void* ref_create_b200_fused(int model_type, int fp32, int64_t K, int J, const double* y, const double* time,
+                            const int64_t* stratum, const int64_t* col_start, const int32_t* rows,
+                            const int64_t* val_start, const double* vals, const uint8_t* fmt, int offset_col0,
+                            const int32_t* prior_type, const double* prior_var, char* err, int errlen) {
+    return create_impl(true, true, model_type, fp32, K, J, y, time, stratum, col_start, rows, val_start,
+                       vals, fmt, offset_col0, prior_type, prior_var, err, errlen);
+}
+
+// ccdb_find_mode calls made by a fused solver (-1 for any other handle).
+int64_t ref_device_calls(void* hp) {
+#ifdef CCDB_B200_ADAPTER
+    auto h = static_cast<RefHandle*>(hp);
+    return h->fused ? h->fused->deviceCalls() : -1;
+#else
+    (void)hp;
+    return -1;
+#endif
 }
 
 void ref_destroy(void* hp) {
@@ -301,7 +338,12 @@ int ref_fit(void* hp, int conv_type, double tol, int max_iter, double initial_bo
             const bool offset = h->data->getHasOffsetCovariate();
             for (int j = 0; j < h->J; ++j) h->ccd->setFixedBeta(j, fixed[j] != 0 || (offset && j == 0));
         }
+#ifdef CCDB_B200_ADAPTER
+        if (h->fused) h->fused->update(a);  // update() is not virtual in the reference
+        else h->ccd->update(a);
+#else
         h->ccd->update(a);
+#endif
         for (int j = 0; j < h->J; ++j) beta_out[j] = h->ccd->getBeta(j);
         *ll_out = h->ccd->getLogLikelihood();
         *iters_out = h->ccd->getIterationCount();

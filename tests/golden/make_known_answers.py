@@ -39,7 +39,8 @@ from ccd_b200.data import (DENSE, GRADIENT, INDICATOR, INTERCEPT, MODEL_CONDITIO
                            build_columns, cox_sort_order)
 from oracle.checker import ReferenceEngine  # noqa: E402
 
-REF = os.environ.get("CYCLOPS_REFERENCE", "/root/reference")
+REF = os.environ.get("CYCLOPS_REFERENCE",
+                     os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "..", "..", "reference"))
 TESTS = os.path.join(REF, "tests", "testthat")
 
 

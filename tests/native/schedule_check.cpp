@@ -11,7 +11,11 @@
 //   * per CTA, segments in increasing level order, task ranges inside the
 //     task array; level_need[L] = CTAs with a segment on level L;
 //   * split columns: nchunks = col_chunks[j], partial slots inside n_partials,
-//     chunks of one column on distinct CTAs.
+//     chunks of one column on distinct CTAs;
+//   * the cluster sweep's per-level exchange: level_split[L] is 1 exactly when
+//     level L holds a split column, every chunk of a column carries the same
+//     slot, and the split columns of one level have distinct slots 0..n-1
+//     (n <= max_split_per_level).
 // Exit status 0 when every case passes.
 #include <algorithm>
 #include <cstdio>
@@ -107,6 +111,8 @@ void run_case(int case_id, std::mt19937_64& rng) {
     check(s.cta_seg.back() == (int64_t)s.segs.size(), "cta_seg end", case_id);
     std::map<int32_t, std::vector<std::pair<int64_t, int64_t>>> cover;
     std::map<int32_t, std::set<int>> chunk_ctas;
+    std::map<int32_t, int32_t> slot_of;                  // split column -> its slot
+    std::map<int32_t, std::map<int32_t, int32_t>> level_slots;  // level -> slot -> column
     std::vector<int32_t> need(std::max(0, s.n_levels), 0);
     for (int c = 0; c < sp.n_cta; ++c) {
         int32_t prev = -1;
@@ -133,6 +139,13 @@ void run_case(int case_id, std::mt19937_64& rng) {
                     check(t.chunk >= 0 && t.chunk < t.nchunks, "chunk index", case_id);
                     check(t.part_base >= 0 && t.part_base + t.nchunks <= s.n_partials, "partial slots", case_id);
                     check(chunk_ctas[t.col].insert(c).second, "two chunks of a column on one CTA", case_id);
+                    auto it = slot_of.find(t.col);
+                    if (it == slot_of.end()) slot_of[t.col] = t.slot;
+                    else check(it->second == t.slot, "chunks of a column with different slots", case_id);
+                    auto& ls = level_slots[sg.level];
+                    auto jt = ls.find(t.slot);
+                    if (jt == ls.end()) ls[t.slot] = t.col;
+                    else check(jt->second == t.col, "two split columns of a level share a slot", case_id);
                 }
                 cover[t.col].push_back({t.p0, t.p1});
                 kinds_seen[kind]++;
@@ -140,6 +153,15 @@ void run_case(int case_id, std::mt19937_64& rng) {
         }
     }
     for (int32_t L = 0; L < s.n_levels; ++L) check(need[L] == s.level_need[L], "level_need", case_id);
+    check((int32_t)s.level_split.size() == s.n_levels, "level_split size", case_id);
+    for (int32_t L = 0; L < s.n_levels && L < (int32_t)s.level_split.size(); ++L) {
+        const auto it = level_slots.find(L);
+        const int32_t n = (it == level_slots.end()) ? 0 : (int32_t)it->second.size();
+        check(s.level_split[L] == (n > 0 ? 1 : 0), "level_split flag", case_id);
+        check(n <= s.max_split_per_level, "max_split_per_level", case_id);
+        if (n > 0) check(it->second.rbegin()->first == n - 1 && it->second.begin()->first == 0,
+                         "slots of a level are not 0..n-1", case_id);
+    }
     for (int32_t j = 0; j < J; ++j) {
         if (fixed[j]) {
             check(cover.count(j) == 0, "task for a fixed column", case_id);
