@@ -32,6 +32,7 @@ import subprocess
 import sys
 import tempfile
 import time
+from typing import Optional
 
 import numpy as np
 
@@ -53,6 +54,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--small", action="store_true", help="a 10x smaller problem (quick checks)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the converged oracle fit that the headline line's parity fields compare with")
     ap.add_argument("--max-sweeps", type=int, default=1000,
                     help="cap on sweeps per findMode (profiling captures of one short launch)")
     ap.add_argument("--serve-requests", type=int, default=200,
@@ -99,13 +102,16 @@ def workload(rank: int, small: bool):
 
 
 def config_of(d, small: bool) -> dict:
+    """The workload, the same on both arms; what one timed step covers is the
+    line's own `step` key (a converged fit here, a sweep on the reference arm:
+    the metric is per coordinate update, and the reference's cost per sweep is
+    flat over a fit)."""
     if WORKLOAD == "cox_breslow":
         return {
             "workload": "cox_breslow" + ("_small" if small else ""), "model": "cox (Breslow ties)",
             "rows": d.K, "columns": d.J, "nnz": d.nnz, "strata": int(d.stratum.max()) + 1,
             "prior": "laplace(0.05)", "convergence": "gradient, tol 1e-6", "precision": "fp64",
-            "step": "one converged findMode from a cold start",
-            "l2": "flushed between timed steps (512 MiB device write)",
+            "start": "cold (beta = 0)",
         }
     return {
         "workload": "poisson_offset" + ("_small" if small else ""),
@@ -114,8 +120,7 @@ def config_of(d, small: bool) -> dict:
         "prior": "normal(1.0), none on offset/intercept",
         "convergence": "gradient, tol 1e-6",
         "precision": "fp64",
-        "step": "one converged findMode from a cold start",
-        "l2": "flushed between timed steps (512 MiB device write)",
+        "start": "cold (beta = 0, offset 1)",
     }
 
 
@@ -298,6 +303,76 @@ def cpu_reference_sample(d, target_s: float = 15.0):
                       f"updates, {tn:.1f} s), single thread (the reference inner loop is serial)"}
 
 
+class ConvergedReference:
+    """The same problem fitted to convergence on the host cores, beside the GPU
+    steps (threads; the GPU's timed region holds only device work): the oracle
+    restatement, bit-identical with the reference engine on every pinned case,
+    for the coefficients, log-likelihood, return flag and the cycles of each
+    findMode attempt; and the compiled reference engine, where present, for its
+    time to converge.  Single thread each, as the reference's inner loop is
+    serial."""
+
+    def __init__(self, d, conv: int, tol: float, fit_kw: Optional[dict] = None):
+        import threading
+        self.d, self.conv, self.tol, self.kw = d, conv, tol, fit_kw or {}
+        self.port = None
+        self.ref_seconds = None
+        self.ref_kind = None
+        self.error = None
+        self.threads = [threading.Thread(target=self._port, daemon=True),
+                        threading.Thread(target=self._reference, daemon=True)]
+        for t in self.threads:
+            t.start()
+
+    def _port(self):
+        from oracle import checker
+        try:
+            e = checker.RestatementEngine(self.d)
+            t0 = time.perf_counter()
+            r = e.fit(self.conv, self.tol, **self.kw)
+            r["seconds"] = time.perf_counter() - t0
+            r["attempt_sweeps"] = e.fit_attempts()
+            e.close()
+            self.port = r
+        except Exception as ex:  # reported in the line, never fatal to the bench
+            self.error = f"restatement: {ex}"
+
+    def _reference(self):
+        from oracle import checker
+        if not checker.reference_available():
+            return
+        try:
+            e = checker.ReferenceEngine(self.d)
+            t0 = time.perf_counter()
+            e.fit(self.conv, self.tol, **self.kw)
+            self.ref_seconds = time.perf_counter() - t0
+            self.ref_kind = "reference"
+            e.close()
+        except Exception as ex:
+            self.error = f"reference: {ex}"
+
+    def result(self, beta, loglik, flag, iterations, attempt_sweeps) -> dict:
+        """Errors of a GPU fit against the converged restatement."""
+        for t in self.threads:
+            t.join()
+        if self.port is None:
+            return {"error": self.error}
+        w = self.port
+        scale = max(float(np.max(np.abs(w["beta"]))), 1e-8)
+        return {
+            "oracle": "FP64 restatement of the reference (bit-identical with it on every pinned case)",
+            "max_rel_dbeta": float(np.max(np.abs(np.asarray(beta) - w["beta"]))) / scale,
+            "rel_dll": abs(loglik - w["loglik"]) / max(1.0, abs(w["loglik"])),
+            "return_flag": {"gpu": int(flag), "oracle": int(w["flag"])},
+            "iterations": {"gpu": int(iterations), "oracle": int(w["iterations"])},
+            "attempt_sweeps": {"gpu": [int(x) for x in attempt_sweeps], "oracle": w["attempt_sweeps"]},
+            "oracle_seconds": w["seconds"],
+            "within_tolerance": bool(float(np.max(np.abs(np.asarray(beta) - w["beta"]))) <= 1e-6 * scale
+                                     and abs(loglik - w["loglik"]) <= 1e-9 * max(1.0, abs(w["loglik"]))
+                                     and int(flag) == int(w["flag"])),
+        }
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
@@ -306,6 +381,12 @@ def run_reference(args, world, rank):
     eng_cls = checker.best_engine()
     kind = "reference" if eng_cls is checker.ReferenceEngine else "port"
     eng = eng_cls(d)
+    # one whole fit to convergence first (time to converge, the ILLCONDITIONED retry
+    # included), then the per-step samples: one sweep each
+    eng.set_beta(cold_beta(d))
+    t0 = time.perf_counter()
+    conv_fit = eng.fit(GRADIENT, 1e-6)
+    conv_t = time.perf_counter() - t0
     times = []
     for i in range(args.warmup + args.steps):
         eng.set_beta(cold_beta(d))
@@ -322,9 +403,14 @@ def run_reference(args, world, rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded PCG64, workload shapes of the benchmark config)",
-        "config": {**config_of(d, args.small), "step": "one sweep of the cold-start fit (bounded sample)"},
+        "config": config_of(d, args.small),
+        "step": "one sweep of the cold-start fit (a bounded sample; the cost per sweep is flat over a fit)",
+        "time_to_converge_s": conv_t,
+        "converged_fit": {"iterations": int(conv_fit["iterations"]), "return_flag": int(conv_fit["flag"]),
+                          "log_likelihood": float(conv_fit["loglik"])},
         "cpu_baseline": {"value": v, "unit": METRIC, "cores": 1, "kind": kind,
-                         "sample": "one sweep of the cold-start fit per step, single thread"},
+                         "sample": "one sweep of the cold-start fit per step, single thread; "
+                                   "time_to_converge_s is one whole fit, timed once before the steps"},
         "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -345,10 +431,11 @@ def run_ours(args, world, rank, local):
     m = native.Matrix(ctx, d)
     f = native.Fit(ctx, m, d)
     margs = native.ModeFindingArguments(convergence_type=GRADIENT, tolerance=1e-6,
-                                        max_iterations=args.max_sweeps)
+                                        max_iterations=args.max_sweeps, strategy=STRATEGIES[args.strategy])
     cold = cold_beta(d)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
 
+    parity = ConvergedReference(d, GRADIENT, 1e-6) if rank == 0 and not args.no_parity else None
     for _ in range(args.warmup):
         f.set_beta(cold)
         f.find_mode(margs)
@@ -359,6 +446,7 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     clocks.start()
     dev_t, ker_t, updates, launches, sweeps, lat = 0.0, 0.0, 0, 0, 0, []
+    attempts = 0
     for i in range(args.steps):
         flush.fill_(1)
         torch.cuda.synchronize()
@@ -371,7 +459,8 @@ def run_ours(args, world, rank, local):
         ker_t += r.kernel_seconds
         updates += r.coordinate_updates
         launches += r.kernel_launches
-        sweeps += r.iterations
+        sweeps += r.sweeps_total
+        attempts += r.attempts
         lat.append(r.device_seconds)
     torch.cuda.synchronize()
     if world > 1:
@@ -410,35 +499,56 @@ def run_ours(args, world, rank, local):
 
     if rank == 0:
         peak, peak_kind = read_peaks()
-        per_launch_bytes = (sweep_bytes(d) * sweeps + objective_bytes(d) * (sweeps + args.steps)) / args.steps
-        achieved = (sweep_bytes(d) * sweeps + objective_bytes(d) * (sweeps + args.steps)) / ker_t / 1e9
+        # every sweep that ran counts, the ILLCONDITIONED attempts' included; one
+        # sweep-kernel launch per findMode attempt, each with its initial objective
+        total_bytes = sweep_bytes(d) * sweeps + objective_bytes(d) * (sweeps + attempts)
+        per_launch_bytes = total_bytes / attempts
+        achieved = total_bytes / ker_t / 1e9
         wl = config_of(d, args.small)["workload"]
-        traffic = read_traffic(wl)  # DRAM bytes of one sweep (ncu), scaled to the launch's sweeps
+        traffic = read_traffic(wl)  # DRAM bytes of one sweep (ncu), scaled to a launch's sweeps
         if traffic is not None:
-            traffic = traffic * sweeps / args.steps
+            traffic = traffic * sweeps / attempts
+        n_levels = native.sweep_levels(d)[1]
+        attempt_sweeps = [sweeps // args.steps - r.iterations, r.iterations] if r.attempts == 2 \
+            else ([r.iterations] if r.attempts == 1 else [r.sweeps_total])
         line = {
             "metric": METRIC, "value": tot_updates / dev_max, "unit": METRIC, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dev_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded PCG64, workload shapes of the benchmark config)",
-            "config": {**config_of(d, args.small), "parallelism": f"replicas x{world}"},
+            "config": config_of(d, args.small),
+            "step": "one converged findMode from a cold start",
+            "parallelism": f"replicas x{world}",
+            "l2": "flushed between timed steps (512 MiB device write)",
             "fits_per_s": world * args.steps / dev_max,
             "fit_latency_ms": {"p50": 1e3 * float(np.percentile(lat, 50)),
                                "p99": 1e3 * float(np.percentile(lat, 99))},
             "sweeps_per_fit": sweeps / args.steps,
+            "findmode_attempts_per_fit": attempts / args.steps,
+            "dependency_levels_per_sweep": int(n_levels),
+            "level_latency_us": 1e6 * ker_t / (sweeps * n_levels),
+            "time_to_converge_s": dev_max / args.steps,
             "return_flag": last.return_flag,
             "e2e": {"value": tot_e2e / e2e_max, "unit": METRIC, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "roofline": ({"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                           "frac": achieved / peak, "peak_source": peak_kind,
                           "algorithmic_bytes_per_launch": per_launch_bytes,
-                          "kernel": "indep_sweep_kernel<POISSON> (one launch per findMode)",
+                          "kernel": ("cluster_sweep_kernel<POISSON>" if args.strategy != "grid_levels"
+                                     else "indep_sweep_kernel<POISSON>") + " (one launch per findMode attempt)",
+                          "bytes": "SURVEY 8(d) bytes of every sweep that ran plus the objective checks",
                           "traffic": traffic} if WORKLOAD == "poisson_offset" else None),
             "gpu_launches": int(tot_launch),
             "clocks": clk,
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_reference_sample(d)
+        if parity is not None:
+            line["parity"] = parity.result(last.beta, last.log_likelihood, last.return_flag, last.iterations,
+                                           attempt_sweeps)
+            if parity.ref_seconds is not None:
+                line["cpu_time_to_converge_s"] = {"value": parity.ref_seconds, "cores": 1,
+                                                  "kind": parity.ref_kind}
         print(json.dumps(line), flush=True)
     f.close()
     m.close()

@@ -296,10 +296,6 @@ void Fit::ensure_schedule(int kind) {
     sp.n_cta = ctx->n_sm * std::min(bps, 1);
     if (ctx->max_ctas > 0) sp.n_cta = std::min(sp.n_cta, ctx->max_ctas);
     // columns up to cta_max entries run on one CTA; longer ones split over CTAs
-    // (CCDB_CTA_MAX overrides, a tuning knob)
-    if (const char* cm = std::getenv("CCDB_CTA_MAX")) sp.cta_max = std::max<int64_t>(1024, std::atoll(cm));
-    if (const char* ck = std::getenv("CCDB_CHUNK")) sp.chunk = std::max<int64_t>(1024, std::atoll(ck));
-    if (const char* wm = std::getenv("CCDB_WARP_MAX")) sp.warp_max = std::max<int64_t>(32, std::atoll(wm));
     sp.warps_per_cta = indep_threads() / 32;
     std::vector<int64_t> entries(J);
     for (int j = 0; j < J; ++j) entries[j] = m->entries(j);
@@ -455,6 +451,10 @@ void Fit::find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* 
         *ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
         check_cuda(cudaMemcpyAsync(hdelta, hd.data(), sizeof(double) * J, cudaMemcpyHostToDevice, stream),
                    "bounds");
+        return;
+    }
+    if (group_engine() && a.strategy != CCDB_SWEEP_SPECULATIVE) {
+        find_mode_group_sweep(a, flag, iters, obj, ms);
         return;
     }
     if (group_engine() || use_speculative(a)) {
@@ -627,20 +627,10 @@ void Fit::apply_step(int j, double delta) {
     launches += m->entries(j) > 0 ? 1 : 0;
 }
 
-// Levels suit dense steps (every coordinate moves); speculative batches suit
-// L1 fits, where most steps are zero and a batch of gradients advances many
-// coordinates per launch.
-bool Fit::use_speculative(const ccdb_mode_args& a) const {
-    if (a.strategy == CCDB_SWEEP_LEVELS || a.strategy == CCDB_SWEEP_GRID_LEVELS) return false;
-    if (a.strategy == CCDB_SWEEP_SPECULATIVE) return true;
-    int active = 0, laplace = 0;
-    for (int j = 0; j < J; ++j) {
-        if (fixed[j]) continue;
-        ++active;
-        laplace += (ptype_h[j] == 1) ? 1 : 0;
-    }
-    return active > 0 && 2 * laplace >= active;
-}
+// The host-driven speculative batches (one round trip per batch of gradients
+// and per nonzero step) run only when asked for; every default path of the
+// independent-row models is the on-device cluster sweep.
+bool Fit::use_speculative(const ccdb_mode_args& a) const { return a.strategy == CCDB_SWEEP_SPECULATIVE; }
 
 void Fit::find_mode(const ccdb_mode_args& a, double* beta_inout, ccdb_fit_result* res) {
     if (!a.prior_type || !a.prior_var) throw Error(CCDB_ERR_INVALID, "prior arrays are required");
@@ -673,7 +663,7 @@ void Fit::find_mode(const ccdb_mode_args& a, double* beta_inout, ccdb_fit_result
     const int64_t launches0 = launches;
     check_cuda(cudaEventRecord(evc0, stream), "event");
     double bound = a.initial_bound;
-    int count = 0, flag = R_FAIL;
+    int count = 0, flag = R_FAIL, sweeps_total = 0;
     double obj = 0.0, secs = 0.0;
     int64_t updates = 0;
     for (;;) {
@@ -688,6 +678,7 @@ void Fit::find_mode(const ccdb_mode_args& a, double* beta_inout, ccdb_fit_result
         if (iters >= 0) {
             last_iterations = iters;
             updates += (int64_t)iters * active;
+            sweeps_total += iters;
         }
         ++count;
         if (beta_dirty_host) {
@@ -720,6 +711,8 @@ void Fit::find_mode(const ccdb_mode_args& a, double* beta_inout, ccdb_fit_result
         res->device_seconds = call_ms * 1e-3;
         res->kernel_seconds = secs;
         res->kernel_launches = launches - launches0;
+        res->attempts = count;
+        res->sweeps_total = sweeps_total;
     }
 }
 
@@ -1313,14 +1306,9 @@ int ccdb_batch_find_mode(ccdb_fit* f, const ccdb_batch_desc* b, const ccdb_mode_
             int32_t* keys = (int32_t*)keep(ctx->alloc(sizeof(int32_t) * (size_t)std::max<int64_t>(nnz, 1)));
             check_cuda(launch_batch_keys(m->d_rows, nnz, P.row_fold, keys, s), "batch keys");
             P.keys = keys;
-            // L2 prefetch of a later column's rows: off by default (it spends the SM's
-            // load-issue slots, which bound the column, and measured no gain)
-            const char* pf = std::getenv("CCDB_BATCH_PREFETCH");
-            P.prefetch = pf ? std::atoi(pf) : 0;
-            // CTAs per group (a cluster splits each column's rows among its CTAs);
-            // CCDB_BATCH_CLUSTER overrides
-            int C = batch_cluster_size(m, K, n_groups, ctx->n_sm);
-            if (const char* cs = std::getenv("CCDB_BATCH_CLUSTER")) C = std::atoi(cs);
+            // CTAs per group (a cluster splits each column's rows among its CTAs):
+            // the caller's choice, else the tuner's
+            int C = b->cluster ? b->cluster : batch_cluster_size(m, K, n_groups, ctx->n_sm);
             if (C < 1 || C > 16) throw Error(CCDB_ERR_INVALID, "batch cluster size must be 1..16");
             P.cluster = C;
             // per row-indexed column, where its rows cross the CTAs' row boundaries;

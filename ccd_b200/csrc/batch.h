@@ -61,7 +61,7 @@ struct BatchParams {
     // stamps (start, issued, terms, reduced, updated, end); NULL: off
     long long* trace;
     int32_t trace_sweep;
-    int32_t prefetch;          // mixed: prefetch the rows of a later column into L2 (0/1)
+    int32_t pad6;
     // mixed: per entry of the row-indexed columns, row id | fold code << 24
     // (fold code: the row's fold id, or 127 for rows in no fold)
     const int32_t* keys;

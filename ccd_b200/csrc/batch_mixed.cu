@@ -26,7 +26,6 @@
 // round trip of a later column falls on column j's critical path:
 //   * the keys (and values) of column j+4 are copied into shared memory with
 //     cp.async (completion is awaited two columns later);
-//   * the row state of column j+2 is prefetched into L2;
 //   * the coefficient, bound and XjY of column j+1 are loaded into registers;
 //   * column j's state is gathered into registers, reduced, stepped, and the
 //     updated xBeta written back from the same registers.
@@ -40,7 +39,6 @@ namespace ccdb {
 namespace {
 
 constexpr int kAhead = 4;          // column j stages column j + kAhead
-constexpr int kPf = 2;             // column j prefetches the rows of column j + kPf
 constexpr int kNBuf = kAhead + 1;  // stage buffers: columns j .. j + kAhead
 constexpr int kRing = 8;           // column metadata ring: columns j .. j + kAhead + 1
 
@@ -114,13 +112,6 @@ __global__ void __launch_bounds__(kMT, 1) batch_mixed_kernel(BatchParams P) {
                 if (m.fmt == F_SPARSE) cp_async8(&b.x[p], P.vals + m.vb + p);
             }
         };
-        auto prefetch = [&](int col) {
-            const MMeta m1 = s_meta[col & (kRing - 1)];
-            if (!stageable<SN>(m1)) return;
-            const MStage<SN>& b = st[col % kNBuf];
-            for (int p = threadIdx.x; p < m1.n; p += kMT)
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(X + (int64_t)(b.k[p] & kKeyRowMask) * G));
-        };
 
         while (__syncthreads_or(active)) {
             // sweep prologue: metadata of the first kAhead + 1 columns, stage the first kAhead
@@ -132,9 +123,6 @@ __global__ void __launch_bounds__(kMT, 1) batch_mixed_kernel(BatchParams P) {
             cp_async_commit();
             cp_async_wait_all();
             __syncthreads();
-            if (P.prefetch)
-                for (int q = 0; q < kPf; ++q)
-                    if (j0 + q < J) prefetch(j0 + q);
             // coefficient, bound, XjY and prior of the next column, one column ahead
             double nb0 = 0.0, nhd0 = 0.0, nxjy0 = 0.0;
             int npt = 0;
@@ -171,7 +159,6 @@ __global__ void __launch_bounds__(kMT, 1) batch_mixed_kernel(BatchParams P) {
                 if (threadIdx.x == 0 && j + kAhead + 1 < J) nm = I.raw(P, j + kAhead + 1);
                 if (j + kAhead < J) stage(j + kAhead);
                 cp_async_commit();
-                if (P.prefetch && j + kPf < J) prefetch(j + kPf);
                 if (tr) tr[6 * j + 1] = clock64();
 
                 // gather and FP32 terms with compensated sums

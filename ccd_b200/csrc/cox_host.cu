@@ -7,6 +7,7 @@
 
 #include "cox.h"
 #include "engine.h"
+#include "group_sweep.h"
 
 namespace ccdb {
 
@@ -137,7 +138,8 @@ void Fit::cox_release() {
     for (void* p : {(void*)cox.xbe, (void*)cox.grp, (void*)cox.rstrat, (void*)cox.denom, (void*)cox.D,
                     (void*)cox.S1, (void*)cox.S2, (void*)cox.nEv, (void*)cox.gfirst, (void*)cox.glast,
                     (void*)cox.grow, (void*)cox.tickets, (void*)cox.status, cox.tails,
-                    (void*)cox.batch_cols, (void*)cox.batch_out})
+                    (void*)cox.batch_cols, (void*)cox.batch_out, (void*)cox.sweep_cols, (void*)cox.dd,
+                    (void*)cox.ddg, cox.agg, (void*)cox.counters, (void*)cox.sweep_gh})
         ctx->release(p);
 }
 
@@ -274,6 +276,97 @@ void Fit::cox_update(int j, double delta) {
     else check_cuda(launch_grouped_update(P, j, delta, stream), "grouped update");
     ++launches;
     cox_scans();
+}
+
+// findMode (CyclicCoordinateDescent.cpp:909-1216) of the Cox and grouped
+// models as one cooperative launch: speculative gradient batches, the nonzero
+// steps, the denominator updates, the Cox scans and the convergence test all on
+// the device (group_sweep.cu).  The bounds are set by the caller.
+void Fit::find_mode_group_sweep(const ccdb_mode_args& a, int* flag, int* iters, double* obj, float* ms) {
+    std::vector<int32_t> cols;
+    int64_t max_entries = 1;
+    for (int j = 0; j < J; ++j)
+        if (!fixed[j]) {
+            cols.push_back(j);
+            max_entries = std::max<int64_t>(max_entries, m->entries(j));
+        }
+    if (cols.empty()) {  // an empty cycle: the first check sees conv = 0
+        *obj = objective(a.convergence_type);
+        *flag = (*obj != *obj) ? R_ILLCONDITIONED
+                : (a.tolerance > 0 ? R_SUCCESS : (a.max_iterations == 1 ? R_MAX_ITERATIONS : R_SUCCESS));
+        *iters = 1;
+        *ms = 0.f;
+        return;
+    }
+    int bps = 0;
+    check_cuda(group_sweep_occupancy(&bps), "occupancy");
+    if (bps < 1) throw Error(CCDB_ERR_CUDA, "the group sweep kernel does not fit on an SM");
+    int n_cta = ctx->n_sm;
+    if (ctx->max_ctas > 0) n_cta = std::min(n_cta, ctx->max_ctas);
+    if (!cox.sweep_cols) {
+        cox.sweep_cols = static_cast<int32_t*>(ctx->alloc(sizeof(int32_t) * std::max(1, J)));
+        cox.agg = ctx->alloc(sizeof(SegAgg) * 2 * ctx->n_sm);
+        cox.counters = static_cast<int64_t*>(ctx->alloc(sizeof(int64_t) * 2));
+    }
+    if (cox.dd_cap < max_entries) {
+        ctx->release(cox.dd);
+        ctx->release(cox.ddg);
+        cox.dd = static_cast<double*>(ctx->alloc(sizeof(double) * max_entries));
+        cox.ddg = static_cast<int32_t*>(ctx->alloc(sizeof(int32_t) * max_entries));
+        cox.dd_cap = max_entries;
+    }
+    check_cuda(cudaMemcpyAsync(cox.sweep_cols, cols.data(), sizeof(int32_t) * cols.size(), cudaMemcpyHostToDevice,
+                               stream), "columns");
+    if (!cox.sweep_gh) cox.sweep_gh = static_cast<double2*>(ctx->alloc(sizeof(double2) * 2 * kGroupBatchMax));
+    if (!beta_dirty_host) upload_beta();
+    DevStatus zero{};
+    zero.flag = R_FAIL;
+    check_cuda(cudaMemcpyAsync(st, &zero, sizeof(zero), cudaMemcpyHostToDevice, stream), "status");
+    check_cuda(cudaMemsetAsync(grid_bar, 0, sizeof(unsigned), stream), "barrier");
+    check_cuda(cudaMemsetAsync(cox.counters, 0, sizeof(int64_t) * 2, stream), "counters");
+    GroupSweepParams Q{};
+    Q.P = cox_params();
+    Q.cox = is_cox() ? 1 : 0;
+    Q.n_active = (int32_t)cols.size();
+    Q.cols = cox.sweep_cols;
+    Q.beta = beta;
+    Q.hdelta = hdelta;
+    Q.ptype = ptype;
+    Q.pvar = pvar;
+    Q.conv = a.convergence_type;
+    Q.max_iter = a.max_iterations;
+    Q.tol = a.tolerance;
+    Q.ll_fixed = ll_fixed;
+    Q.batch_max = std::min(kBatchMax, kGroupBatchMax);
+    Q.J = J;
+    Q.gh = cox.sweep_gh;
+    Q.dd = cox.dd;
+    Q.ddg = cox.ddg;
+    Q.red = red;
+    Q.agg = static_cast<SegAgg*>(cox.agg);
+    Q.grid_bar = grid_bar;
+    Q.st = st;
+    Q.wait_limit_ns = wait_limit_ns;
+    Q.counters = cox.counters;
+    check_cuda(cudaEventRecord(ev0, stream), "event");
+    check_cuda(launch_group_sweep(Q, n_cta, stream), "group sweep launch");
+    ++launches;
+    check_cuda(cudaEventRecord(ev1, stream), "event");
+    DevStatus out{};
+    int64_t cnt[2] = {0, 0};
+    check_cuda(cudaMemcpyAsync(&out, st, sizeof(out), cudaMemcpyDeviceToHost, stream), "status");
+    check_cuda(cudaMemcpyAsync(cnt, cox.counters, sizeof(cnt), cudaMemcpyDeviceToHost, stream), "counters");
+    check_cuda(cudaStreamSynchronize(stream), "group sweep");
+    check_cuda(cudaEventElapsedTime(ms, ev0, ev1), "elapsed");
+    if (out.error != E_NONE)
+        throw Error(CCDB_ERR_TIMEOUT, "device wait timed out (code " + std::to_string(out.error) + " at " +
+                                          std::to_string(out.error_where) + ")");
+    cox.last_updates = cnt[0];
+    cox.last_batches = cnt[1];
+    *flag = out.flag;
+    *iters = out.iterations;
+    *obj = out.objective;
+    beta_dirty_host = true;
 }
 
 }  // namespace ccdb

@@ -99,6 +99,16 @@ struct CoxDev {
     void* tails = nullptr;
     int32_t* batch_cols = nullptr;
     double2* batch_out = nullptr;
+    // the persistent sweep (group_sweep.cu): active columns, the updated
+    // column's per-entry changes, scan aggregates, counters
+    int32_t* sweep_cols = nullptr;
+    double2* sweep_gh = nullptr;
+    double* dd = nullptr;
+    int32_t* ddg = nullptr;
+    int64_t dd_cap = 0;
+    void* agg = nullptr;
+    int64_t* counters = nullptr;
+    int64_t last_updates = 0, last_batches = 0;  // of the last persistent findMode
 };
 
 int64_t cox_group_rows(const std::vector<int32_t>& pid0, const std::vector<double>& time,
@@ -202,6 +212,8 @@ struct Fit {
     void cox_objective_terms(double* out4);
     void cox_gh_batch(const int32_t* cols, int n, double2* out);
     void cox_update(int j, double delta);
+    // one findMode of the group engine in one persistent launch (group_sweep.cu)
+    void find_mode_group_sweep(const ccdb_mode_args& a, int* flag, int* iters, double* obj, float* ms);
     // mode-finding variants (modes_host.cu): the MM cycle, the KKT swindle, and
     // the MM all-coordinate (g, h) into out[J] (fixed may be nullptr)
     void find_mode_mm(const ccdb_mode_args& a, int* flag, int* iters, double* obj);

@@ -1,0 +1,458 @@
+// group_sweep.cu -- one findMode of the group engine in one persistent launch.
+//
+// The Breslow Cox model and the grouped models (conditional logistic /
+// Poisson) share rows through their risk sets or strata, so their sweep is
+// the speculative one of the per-call path, now driven by the device: the
+// gradients of a batch of consecutive coordinates are computed together
+// against one state (one CTA per column); walking them in visiting order every
+// zero step leaves the state unchanged, so each is the gradient the
+// sequential cycle (CyclicCoordinateDescent.cpp:1008-1021) would see, and the
+// first nonzero step is applied and the batch restarts after it.  Every CTA
+// takes the same decision from the same published gradients, so the control
+// flow (and every grid barrier) is uniform.
+//
+// A nonzero step of column j:
+//   * the column's rows are split over the CTAs: xBeta += delta x, e = exp,
+//     and each row's (weighted) change of e is recorded with its group;
+//   * after a barrier, the first row of each group's run adds the run's
+//     changes to the group denominator in row order, as updateXBetaImpl does
+//     (ModelSpecifics.hpp:1548-1571);
+//   * Cox: the accumulated denominators D (a segmented prefix scan within
+//     strata, computeAccumlatedDenominator, ModelSpecifics.hpp:1670-1715) and
+//     the suffix sums S1 = sum nEv/D, S2 = sum nEv/D^2 behind the O(nnz)
+//     gradient are rebuilt by a reduce-then-scan over contiguous group ranges
+//     of the CTAs: aggregates, barrier, carry-in in CTA order, barrier.
+// A column's bound (hDelta) changes with every step, zero or not; the writes
+// of a decision (bounds of the walked columns, the moved coefficient) are
+// held back by CTA 0 until the next grid barrier, after every CTA has read
+// the old values.  Convergence is tested on the device after each sweep, in
+// every CTA from the same partial sums.
+//
+// Every wait is a grid barrier bounded by wait_limit_ns (common.cuh); a wait
+// that runs out records an error, raises the abort word and all CTAs return.
+#include <cstdint>
+
+#include "common.cuh"
+#include "group_common.cuh"
+#include "group_sweep.h"
+#include "step.h"
+
+namespace ccdb {
+
+namespace {
+
+using namespace grp;
+
+struct Seg3 {
+    int f;
+    double a, b;
+};
+__device__ __forceinline__ Seg3 seg3_combine(Seg3 x, Seg3 y) {
+    return Seg3{x.f | y.f, y.f ? y.a : x.a + y.a, y.f ? y.b : x.b + y.b};
+}
+
+// Exclusive scan of one Seg3 per thread in thread order (REV: in reverse
+// thread order), fixed combination order; *total gets the block aggregate.
+template <bool REV>
+__device__ __forceinline__ Seg3 block_excl_scan3(Seg3 x, Seg3* s_w, Seg3* total) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    Seg3 inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        Seg3 y;
+        if (!REV) {
+            y.f = __shfl_up_sync(0xffffffffu, inc.f, o);
+            y.a = __shfl_up_sync(0xffffffffu, inc.a, o);
+            y.b = __shfl_up_sync(0xffffffffu, inc.b, o);
+            if (lane >= o) inc = seg3_combine(y, inc);
+        } else {
+            y.f = __shfl_down_sync(0xffffffffu, inc.f, o);
+            y.a = __shfl_down_sync(0xffffffffu, inc.a, o);
+            y.b = __shfl_down_sync(0xffffffffu, inc.b, o);
+            if (lane + o < 32) inc = seg3_combine(y, inc);
+        }
+    }
+    // exclusive within the warp: the neighbour's inclusive value
+    Seg3 ex;
+    if (!REV) {
+        ex.f = __shfl_up_sync(0xffffffffu, inc.f, 1);
+        ex.a = __shfl_up_sync(0xffffffffu, inc.a, 1);
+        ex.b = __shfl_up_sync(0xffffffffu, inc.b, 1);
+    } else {
+        ex.f = __shfl_down_sync(0xffffffffu, inc.f, 1);
+        ex.a = __shfl_down_sync(0xffffffffu, inc.a, 1);
+        ex.b = __shfl_down_sync(0xffffffffu, inc.b, 1);
+    }
+    const bool first_in_warp = REV ? (lane == 31) : (lane == 0);
+    const bool last_in_warp = REV ? (lane == 0) : (lane == 31);
+    if (last_in_warp) s_w[wid] = inc;
+    __syncthreads();
+    if (threadIdx.x == 0) {  // exclusive scan of the warp aggregates in scan order
+        Seg3 run{0, 0.0, 0.0};
+        for (int q = 0; q < kW; ++q) {
+            const int w = REV ? (kW - 1 - q) : q;
+            const Seg3 t = s_w[w];
+            s_w[w] = run;
+            run = (q == 0) ? t : seg3_combine(run, t);
+        }
+        *total = run;
+    }
+    __syncthreads();
+    const Seg3 wpre = s_w[wid];
+    const bool first_warp = REV ? (wid == kW - 1) : (wid == 0);
+    Seg3 out;
+    if (first_in_warp) out = first_warp ? Seg3{0, 0.0, 0.0} : wpre;
+    else out = first_warp ? ex : seg3_combine(wpre, ex);
+    __syncthreads();
+    return out;
+}
+
+// Thread t's contiguous share of a CTA's range [lo, hi).
+__device__ __forceinline__ void thread_share(int64_t lo, int64_t hi, int64_t& a, int64_t& b) {
+    const int64_t len = hi - lo;
+    a = lo + len * threadIdx.x / blockDim.x;
+    b = lo + len * (threadIdx.x + 1) / blockDim.x;
+}
+
+// D, S1, S2 rebuilt from the group denominators (Cox).  Three phases separated
+// by grid barriers; false when a barrier wait ran out.
+__device__ bool cox_rebuild(const GroupSweepParams& Q, unsigned& epoch, int32_t* s_fail, Seg3* s_w,
+                            Seg3* s_tot, Seg3* s_carry) {
+    const CoxParams& P = Q.P;
+    const int64_t G = gridDim.x, b = blockIdx.x;
+    const int64_t g0 = P.N * b / G, g1 = P.N * (b + 1) / G;
+    int64_t t0, t1;
+    thread_share(g0, g1, t0, t1);
+    // phase 1: aggregate of the CTA's range (prefix direction)
+    Seg3 mine{0, 0.0, 0.0};
+    for (int64_t g = t0; g < t1; ++g) {
+        const Seg3 e{P.gfirst[g], __ldcg(P.denom + g), 0.0};
+        mine = (g == t0) ? e : seg3_combine(mine, e);
+    }
+    block_excl_scan3<false>(mine, s_w, s_tot);
+    if (threadIdx.x == 0) {
+        SegAgg a{s_tot->f, 0, s_tot->a, 0.0};
+        __stcg(&Q.agg[b].f, a.f);
+        __stcg(&Q.agg[b].v0, a.v0);
+    }
+    if (!grid_barrier(Q.grid_bar, epoch, Q.wait_limit_ns, Q.st, s_fail)) return false;
+    // phase 2: carry-in from the CTAs before, D of the range; suffix aggregates
+    if (threadIdx.x == 0) {
+        Seg3 c{0, 0.0, 0.0};
+        for (int64_t q = 0; q < b; ++q) {
+            const Seg3 e{__ldcg(&Q.agg[q].f), __ldcg(&Q.agg[q].v0), 0.0};
+            c = (q == 0) ? e : seg3_combine(c, e);
+        }
+        *s_carry = c;
+    }
+    __syncthreads();
+    Seg3 pre = block_excl_scan3<false>(mine, s_w, s_tot);
+    {
+        // running value entering this thread's first group
+        Seg3 run = (b == 0) ? pre : (threadIdx.x == 0 ? *s_carry : seg3_combine(*s_carry, pre));
+        const bool has_run = (b > 0) || (threadIdx.x > 0);
+        Seg3 rs{0, 0.0, 0.0};  // suffix aggregate of the thread's share, built from the top
+        for (int64_t g = t0; g < t1; ++g) {
+            const Seg3 e{P.gfirst[g], __ldcg(P.denom + g), 0.0};
+            run = (!has_run && g == t0) ? e : seg3_combine(run, e);
+            __stcg(P.D + g, run.a);
+        }
+        for (int64_t g = t1 - 1; g >= t0; --g) {
+            const double D = __ldcg(P.D + g);
+            const double ne = P.nEv[g];
+            const Seg3 e{P.glast[g], ne / D, ne / (D * D)};
+            rs = (g == t1 - 1) ? e : seg3_combine(rs, e);
+        }
+        mine = rs;
+    }
+    block_excl_scan3<true>(mine, s_w, s_tot);
+    if (threadIdx.x == 0) {
+        __stcg(&Q.agg[G + b].f, s_tot->f);
+        __stcg(&Q.agg[G + b].v0, s_tot->a);
+        __stcg(&Q.agg[G + b].v1, s_tot->b);
+    }
+    if (!grid_barrier(Q.grid_bar, epoch, Q.wait_limit_ns, Q.st, s_fail)) return false;
+    // phase 3: carry-in from the CTAs after (suffix direction), S1 and S2 of the range
+    if (threadIdx.x == 0) {
+        Seg3 c{0, 0.0, 0.0};
+        for (int64_t q = G - 1; q > b; --q) {
+            const Seg3 e{__ldcg(&Q.agg[G + q].f), __ldcg(&Q.agg[G + q].v0), __ldcg(&Q.agg[G + q].v1)};
+            c = (q == G - 1) ? e : seg3_combine(c, e);
+        }
+        *s_carry = c;
+    }
+    __syncthreads();
+    Seg3 suf = block_excl_scan3<true>(mine, s_w, s_tot);
+    {
+        const bool last_cta = (b == G - 1);
+        Seg3 run = last_cta ? suf : (threadIdx.x == kT - 1 ? *s_carry : seg3_combine(*s_carry, suf));
+        const bool has_run = !last_cta || (threadIdx.x < kT - 1);
+        for (int64_t g = t1 - 1; g >= t0; --g) {
+            const double D = __ldcg(P.D + g);
+            const double ne = P.nEv[g];
+            const Seg3 e{P.glast[g], ne / D, ne / (D * D)};
+            run = (!has_run && g == t1 - 1) ? e : seg3_combine(run, e);
+            __stcg(P.S1 + g, run.a);
+            __stcg(P.S2 + g, run.b);
+        }
+    }
+    return grid_barrier(Q.grid_bar, epoch, Q.wait_limit_ns, Q.st, s_fail);
+}
+
+// This CTA's objective partials {LL numerator, LL denominator, gradient
+// objective, log prior} (ModelSpecifics.hpp:103-120, 605-650; JointPrior.h:121-128).
+template <bool COX>
+__device__ double4 objective_share(const GroupSweepParams& Q, double4* s_red4) {
+    const CoxParams& P = Q.P;
+    double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
+    const int64_t G = gridDim.x, b = blockIdx.x;
+    const int64_t k0 = P.K * b / G, k1 = P.K * (b + 1) / G;
+    for (int64_t k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+        const double xb = __ldcg(P.xbe + k).x;
+        const double yk = P.y[k];
+        const int yi = (int)yk;
+        if (COX) {
+            const double w = P.weighted ? P.w[k] : 1.0;
+            const double c = (yi != 1) ? 0.0 : xb;
+            acc.x += P.weighted ? c * w : c;
+            acc.z += P.weighted ? xb * yk * w : xb * yk;
+        } else {
+            acc.x += P.weighted ? (yi * xb) * P.w[k] : yi * xb;
+            acc.z += P.weighted ? xb * yk * P.w[k] : xb * yk;
+        }
+    }
+    const int64_t n0 = P.N * b / G, n1 = P.N * (b + 1) / G;
+    for (int64_t g = n0 + threadIdx.x; g < n1; g += blockDim.x)
+        acc.y += P.nEv[g] * log(__ldcg((COX ? P.D : P.denom) + g));
+    const int64_t j0 = (int64_t)Q.J * b / G, j1 = (int64_t)Q.J * (b + 1) / G;
+    for (int64_t j = j0 + threadIdx.x; j < j1; j += blockDim.x)
+        acc.w += log_prior_one(__ldcg(Q.beta + j), Q.ptype[j], Q.pvar[j]);
+    return block_sum4<kW>(acc, s_red4);
+}
+
+template <bool COX>
+__device__ bool objective_all(const GroupSweepParams& Q, unsigned& epoch, int32_t* s_fail, double4* s_red4,
+                              double& obj, double& ll, double& lp) {
+    const double4 o = objective_share<COX>(Q, s_red4);
+    if (threadIdx.x == 0) {
+        __stcg(Q.red + 2 * blockIdx.x, make_double2(o.x, o.y));
+        __stcg(Q.red + 2 * blockIdx.x + 1, make_double2(o.z, o.w));
+    }
+    if (!grid_barrier(Q.grid_bar, epoch, Q.wait_limit_ns, Q.st, s_fail)) return false;
+    double4 t = make_double4(0.0, 0.0, 0.0, 0.0);
+    for (int c = 0; c < (int)gridDim.x; ++c) {
+        const double2 u = __ldcg(Q.red + 2 * c), v = __ldcg(Q.red + 2 * c + 1);
+        t.x += u.x;
+        t.y += u.y;
+        t.z += v.x;
+        t.w += v.y;
+    }
+    ll = (t.x - t.y) + Q.ll_fixed;
+    lp = t.w;
+    obj = (Q.conv == C_GRADIENT) ? t.z : (Q.conv == C_MITTAL ? ll : ll + t.w);
+    // every CTA has read the partials before any of them writes the next ones
+    return grid_barrier(Q.grid_bar, epoch, Q.wait_limit_ns, Q.st, s_fail);
+}
+
+template <bool COX>
+__global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) {
+    __shared__ GhShared S;
+    __shared__ double4 s_red4[kW];
+    __shared__ Seg3 s_w3[kW];
+    __shared__ Seg3 s_tot, s_carry;
+    __shared__ int32_t s_fail;
+    __shared__ int32_t s_first;
+    __shared__ double s_delta, s_newbeta;
+    __shared__ double s_pend_hd[kGroupBatchMax];  // CTA 0: bounds of the last decision
+
+    const CoxParams& P = Q.P;
+    const int tid = threadIdx.x;
+    const int64_t G = gridDim.x, b = blockIdx.x;
+    unsigned epoch = 0;
+    int pend_pos = 0, pend_n = 0, pend_col = -1;  // CTA 0's writes held back to the next barrier
+    long long n_updates = 0, n_batches = 0;
+
+    // grid barrier, then CTA 0 applies the held-back writes of the last decision
+    auto barrier = [&]() -> bool {
+        if (!grid_barrier(Q.grid_bar, epoch, Q.wait_limit_ns, Q.st, &s_fail)) return false;
+        if (b == 0 && pend_n > 0) {
+            for (int i = tid; i < pend_n; i += blockDim.x) Q.hdelta[Q.cols[pend_pos + i]] = s_pend_hd[i];
+            if (tid == 0 && pend_col >= 0) Q.beta[pend_col] = s_newbeta;
+            __syncthreads();
+        }
+        pend_n = 0;
+        pend_col = -1;
+        return true;
+    };
+
+    double last, ll, lp;
+    if (!objective_all<COX>(Q, epoch, &s_fail, s_red4, last, ll, lp)) return;
+
+    int iteration = 0;
+    for (int it = 0; it < Q.max_iter; ++it) {
+        int pos = 0, batch = 32;
+        while (pos < Q.n_active) {
+            const int nb = min(batch, Q.n_active - pos);
+            // gradients of the batch, one CTA per column; the two halves of gh
+            // alternate by batch, so a CTA that is on to the next batch never
+            // overwrites values another CTA is still deciding from
+            double2* gh = Q.gh + (n_batches & 1) * kGroupBatchMax;
+            ++n_batches;
+            for (int c = (int)b; c < nb; c += (int)G) {
+                const double2 r = COX ? cox_column_gh(P, Q.cols[pos + c], S) : grouped_column_gh(P, Q.cols[pos + c], S);
+                if (tid == 0) __stcg(gh + c, r);
+            }
+            if (!barrier()) return;
+            // the decision, in every CTA from the same values: the first nonzero step
+            if (tid == 0) s_first = nb;
+            __syncthreads();
+            double hd_r[kGroupBatchMax / kT];
+#pragma unroll
+            for (int r = 0; r < kGroupBatchMax / kT; ++r) {
+                const int i = tid + r * kT;
+                hd_r[r] = 0.0;
+                if (i < nb) {
+                    const int j = Q.cols[pos + i];
+                    const double2 ghv = __ldcg(gh + i);
+                    const double b0 = __ldcg(Q.beta + j);
+                    double hd = __ldcg(Q.hdelta + j);
+                    double d = newton_prior_delta(ghv.x, ghv.y, b0, Q.ptype[j], Q.pvar[j]);
+                    d = apply_bounds(d, hd);
+                    hd_r[r] = hd;
+                    if (d != 0.0) atomicMin(&s_first, i);
+                }
+            }
+            __syncthreads();
+            const int first = s_first;
+#pragma unroll
+            for (int r = 0; r < kGroupBatchMax / kT; ++r) {
+                const int i = tid + r * kT;
+                if (i < nb && i <= first) {
+                    if (b == 0) s_pend_hd[i] = hd_r[r];
+                    if (i == first) {  // recompute the step of the moving column: same inputs, same bits
+                        const int j = Q.cols[pos + i];
+                        const double2 ghv = __ldcg(gh + i);
+                        const double b0 = __ldcg(Q.beta + j);
+                        double hd = __ldcg(Q.hdelta + j);
+                        double d = newton_prior_delta(ghv.x, ghv.y, b0, Q.ptype[j], Q.pvar[j]);
+                        d = apply_bounds(d, hd);
+                        s_delta = d;
+                        s_newbeta = b0 + d;
+                    }
+                }
+            }
+            __syncthreads();
+            if (b == 0) {
+                pend_pos = pos;
+                pend_n = (first < nb) ? first + 1 : nb;
+                pend_col = (first < nb) ? Q.cols[pos + first] : -1;
+            }
+            if (first >= nb) {  // every step of the batch was zero: the state is unchanged
+                pos += nb;
+                batch = min(2 * batch, Q.batch_max);
+                continue;
+            }
+            // ---- the nonzero step of column j: rows split over the CTAs
+            const int j = Q.cols[pos + first];
+            const double delta = s_delta;
+            ++n_updates;
+            {
+                const uint8_t f = P.fmt[j];
+                const bool has_rows = (f == F_SPARSE || f == F_INDICATOR);
+                const bool has_vals = (f == F_SPARSE || f == F_DENSE);
+                const int64_t cb = P.col_ptr[j], vb = P.val_ptr[j];
+                const int64_t n = has_rows ? (P.col_ptr[j + 1] - cb) : P.K;
+                const int64_t p0 = n * b / G, p1 = n * (b + 1) / G;
+                for (int64_t p = p0 + tid; p < p1; p += blockDim.x) {
+                    const int64_t k = has_rows ? (int64_t)__ldg(P.rows + cb + p) : p;
+                    const double x = has_vals ? __ldg(P.vals + vb + p) : 1.0;
+                    const double2 xe = __ldcg(P.xbe + k);
+                    const double xb = xe.x + delta * x;
+                    const double en = exp(xb);
+                    __stcg(P.xbe + k, make_double2(xb, en));
+                    double dd;
+                    if (COX && P.weighted) {
+                        const double w = P.w[k];
+                        dd = w * en - w * xe.y;
+                    } else {
+                        dd = en - xe.y;
+                    }
+                    __stcg(Q.dd + p, dd);
+                    __stcg(Q.ddg + p, P.grp[k]);
+                }
+                if (!barrier()) return;
+                // the first row of each group's run adds the run's changes in row order;
+                // rows dropped by a zero weight (group N) may sit inside a run
+                for (int64_t p = p0 + tid; p < p1; p += blockDim.x) {
+                    const int32_t g = __ldcg(Q.ddg + p);
+                    if (g == P.N) continue;
+                    int64_t q = p - 1;
+                    while (q >= 0 && __ldcg(Q.ddg + q) == P.N) --q;
+                    if (q >= 0 && __ldcg(Q.ddg + q) == g) continue;
+                    double d = __ldcg(P.denom + g);
+                    for (q = p; q < n; ++q) {
+                        const int32_t gq = __ldcg(Q.ddg + q);
+                        if (gq == P.N) continue;
+                        if (gq != g) break;
+                        d = d + __ldcg(Q.dd + q);
+                    }
+                    __stcg(P.denom + g, d);
+                }
+                if (!barrier()) return;
+            }
+            if (COX && !cox_rebuild(Q, epoch, &s_fail, s_w3, &s_tot, &s_carry)) return;
+            pos += first + 1;
+            batch = 32;
+        }
+        // the sweep is complete: held-back writes land, then the objective
+        if (!barrier()) return;
+        double cur;
+        if (!objective_all<COX>(Q, epoch, &s_fail, s_red4, cur, ll, lp)) return;
+        iteration = it + 1;
+        double conv;
+        bool ill = false;
+        if (cur != cur) {
+            conv = 0.0;
+            ill = true;
+        } else {
+            conv = fabs(cur - last) / (fabs(cur) + 1.0);
+        }
+        last = cur;
+        int done = 0, flag = R_SUCCESS;
+        if (Q.tol > 0 && conv < Q.tol) {
+            flag = ill ? R_ILLCONDITIONED : R_SUCCESS;
+            done = 1;
+        } else if (iteration == Q.max_iter) {
+            flag = R_MAX_ITERATIONS;
+            done = 1;
+        }
+        if (b == 0 && tid == 0) {
+            Q.st->iterations = iteration;
+            Q.st->objective = cur;
+            Q.st->loglik = ll;
+            Q.st->log_prior = lp;
+            if (done) Q.st->flag = flag;
+        }
+        if (done) break;
+    }
+    if (b == 0 && tid == 0 && Q.counters) {
+        Q.counters[0] = n_updates;
+        Q.counters[1] = n_batches;
+    }
+}
+
+}  // namespace
+
+int group_sweep_threads() { return kT; }
+
+cudaError_t group_sweep_occupancy(int* blocks_per_sm) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, group_sweep_kernel<true>, kT, 0);
+}
+
+cudaError_t launch_group_sweep(const GroupSweepParams& Q, int n_cta, cudaStream_t stream) {
+    void* args[] = {(void*)&Q};
+    const void* fn = Q.cox ? (const void*)group_sweep_kernel<true> : (const void*)group_sweep_kernel<false>;
+    return cudaLaunchCooperativeKernel(fn, dim3(n_cta), dim3(kT), args, 0, stream);
+}
+
+}  // namespace ccdb

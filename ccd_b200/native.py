@@ -51,7 +51,7 @@ class _ModeArgs(C.Structure):
 
 class _BatchDesc(C.Structure):
     _fields_ = [("n_instances", C.c_int32), ("row_fold", C.c_void_p), ("holdout", C.c_void_p),
-                ("variance", C.c_void_p), ("group", C.c_int32)]
+                ("variance", C.c_void_p), ("group", C.c_int32), ("cluster", C.c_int32)]
 
 
 class _BatchResult(C.Structure):
@@ -65,7 +65,8 @@ class _FitResult(C.Structure):
     _fields_ = [("return_flag", C.c_int32), ("iterations", C.c_int32),
                 ("log_likelihood", C.c_double), ("objective", C.c_double),
                 ("coordinate_updates", C.c_int64), ("device_seconds", C.c_double),
-                ("kernel_seconds", C.c_double), ("kernel_launches", C.c_int64)]
+                ("kernel_seconds", C.c_double), ("kernel_launches", C.c_int64),
+                ("attempts", C.c_int32), ("sweeps_total", C.c_int32)]
 
 
 @dataclass
@@ -94,6 +95,8 @@ class FitResult:
     device_seconds: float
     kernel_seconds: float = 0.0
     kernel_launches: int = 0
+    attempts: int = 1       # findMode runs (the ILLCONDITIONED retry adds some)
+    sweeps_total: int = 0   # cycles over all of them
 
 
 _lib = None
@@ -369,9 +372,10 @@ class Fit:
 
     # --- the cross-validation grid: many instances in one launch
     def batch_find_mode(self, variance, holdout=None, row_fold=None,
-                        args: Optional[ModeFindingArguments] = None, group: int = 0):
+                        args: Optional[ModeFindingArguments] = None, group: int = 0, cluster: int = 0):
         """Fit len(variance) instances (fold held out, prior variance) together.
-        ``group``: lockstep group size of a mixed-precision fit (0: the engine's choice).
+        ``group``: lockstep group size of a mixed-precision fit, ``cluster``: its CTAs
+        per group (0: the engine's choice).
         Returns (beta[n, J], list of per-instance dicts, device seconds)."""
         args = args or ModeFindingArguments()
         keep = []
@@ -380,7 +384,7 @@ class Fit:
         n = var.shape[0]
         hold = None if holdout is None else _c(holdout, np.int32)
         fold = None if row_fold is None else _c(row_fold, np.int32)
-        bd = _BatchDesc(n, _p(fold), _p(hold), _p(var), int(group))
+        bd = _BatchDesc(n, _p(fold), _p(hold), _p(var), int(group), int(cluster))
         beta = np.zeros((n, self.d.J))
         res = (_BatchResult * n)()
         secs = C.c_double()
@@ -446,7 +450,7 @@ class Fit:
         out = b if b is not None else self.get_beta()
         return FitResult(out, res.return_flag, res.iterations, res.log_likelihood, res.objective,
                          res.coordinate_updates, res.device_seconds, res.kernel_seconds,
-                         res.kernel_launches)
+                         res.kernel_launches, res.attempts, res.sweeps_total)
 
 
 def fit_model(ctx: Context, d: CyclopsData, args: Optional[ModeFindingArguments] = None,
@@ -466,7 +470,7 @@ def fit_model(ctx: Context, d: CyclopsData, args: Optional[ModeFindingArguments]
                                 C.byref(ma), _p(beta), C.byref(res)))
     return FitResult(beta, res.return_flag, res.iterations, res.log_likelihood, res.objective,
                      res.coordinate_updates, res.device_seconds, res.kernel_seconds,
-                     res.kernel_launches)
+                     res.kernel_launches, res.attempts, res.sweeps_total)
 
 
 def validate_matrix(d: CyclopsData) -> None:

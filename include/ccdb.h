@@ -174,11 +174,13 @@ typedef struct {
     int32_t max_bound_count;   /* default 5 */
     int32_t per_coordinate;    /* 0: on-device mode finding (default); 1: host loop over
                                   the per-coordinate calls above (the reference's call pattern) */
-    int32_t strategy;          /* on-device sweep strategy for logistic/Poisson:
-                                  CCDB_SWEEP_AUTO, _LEVELS (fused persistent kernel over
-                                  dependency levels) or _SPECULATIVE (batched gradients,
-                                  restart after each nonzero step); other models always
-                                  use speculative batches */
+    int32_t strategy;          /* sweep strategy.  Logistic/Poisson: CCDB_SWEEP_AUTO and
+                                  _LEVELS run the cluster sweep (one launch per findMode over
+                                  dependency levels), _GRID_LEVELS the grid-wide level sweep,
+                                  _SPECULATIVE host-driven batches of gradients that restart
+                                  after each nonzero step.  Cox and conditional models: one
+                                  persistent launch per findMode of device-driven speculative
+                                  batches, or with _SPECULATIVE the host-driven batches */
     int32_t algorithm;         /* AlgorithmType (Types.h:149-153): CCDB_ALGORITHM_CCD (0,
                                   default) or CCDB_ALGORITHM_MM (findMode's MM cycle,
                                   CyclicCoordinateDescent.cpp:974-1001; conditional logistic,
@@ -210,6 +212,8 @@ typedef struct {
                                    the copy of beta back to the host */
     double kernel_seconds;      /* span of the fused sweep launches alone */
     int64_t kernel_launches;    /* engine kernels launched by the call */
+    int32_t attempts;           /* findMode runs: 1, plus one per ILLCONDITIONED retry */
+    int32_t sweeps_total;       /* cycles over every attempt (iterations counts the last) */
 } ccdb_fit_result;
 
 /* Run CyclicCoordinateDescent::update (.cpp:586-615): findMode, with the
@@ -234,6 +238,8 @@ typedef struct {
     const double* variance;  /* n_instances: prior variance of the regularised columns */
     int32_t group;           /* CCDB_PRECISION_MIXED fits: instances stepped in lockstep per CTA
                                 (1, 2 or 4); 0 lets the engine choose.  Ignored for FP64 fits. */
+    int32_t cluster;         /* CCDB_PRECISION_MIXED fits: CTAs per group, each owning a range of
+                                rows (1..16); 0 lets the engine choose.  Ignored for FP64 fits. */
 } ccdb_batch_desc;
 
 typedef struct {

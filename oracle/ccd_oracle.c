@@ -28,6 +28,7 @@ enum { F_DENSE = 0, F_SPARSE = 1, F_INDICATOR = 2, F_INTERCEPT = 3 };
 enum { C_GRADIENT = 0, C_LANGE = 1, C_MITTAL = 2 };
 enum { R_SUCCESS = 0, R_MAX_ITERATIONS = 2, R_ILLCONDITIONED = 3 };
 
+#define ORC_MAX_ATTEMPTS 16
 #define ORC_PI 3.14159265358979323851280895940618620443274267017841339111328125
 
 /* Test hook: a copy of the arithmetic with exp moved by one unit in the last
@@ -86,6 +87,9 @@ typedef struct {
     double* w; /* CV weights or NULL */
     int valid_weights, xb_known, suff_known, touched_y;
     int last_flag, last_iter;
+    /* cycles of each findMode attempt of the last orc_fit (the ILLCONDITIONED
+     * retry of CyclicCoordinateDescent::update, CCD.cpp:598-614) */
+    int n_attempts, attempt_sweeps[ORC_MAX_ATTEMPTS];
 } Orc;
 
 static int is_indep(const Orc* o) { return o->model == MT_LOGISTIC || o->model == MT_POISSON; }
@@ -1018,6 +1022,7 @@ int orc_fit(void* hp, int conv_type, double tol, int max_iter, double initial_bo
         for (int j = 0; j < o->J; ++j) o->fix[j] = (fixed[j] != 0) || (o->offset_col0 && j == 0);
     o->bound = initial_bound;
     int count = 0;
+    o->n_attempts = 0;
     for (;;) {
         const char* msg = NULL;
         /* update: kktSwindle when asked and a Laplace prior supports it (CCD.cpp:598-603) */
@@ -1030,6 +1035,7 @@ int orc_fit(void* hp, int conv_type, double tol, int max_iter, double initial_bo
             return -1;
         }
         ++count;
+        if (o->n_attempts < ORC_MAX_ATTEMPTS) o->attempt_sweeps[o->n_attempts++] = o->last_iter;
         if (o->last_flag == R_ILLCONDITIONED && count < max_bound_count) {
             o->bound /= 10.0;
             for (int j = o->offset_col0 ? 1 : 0; j < o->J; ++j) o->beta[j] = 0.0;
@@ -1045,6 +1051,12 @@ int orc_fit(void* hp, int conv_type, double tol, int max_iter, double initial_bo
     *iters_out = o->last_iter;
     *flag_out = o->last_flag;
     return 0;
+}
+
+int orc_fit_attempts(void* hp, int* sweeps, int max_n) {
+    const Orc* o = (const Orc*)hp;
+    for (int i = 0; i < o->n_attempts && i < max_n; ++i) sweeps[i] = o->attempt_sweeps[i];
+    return o->n_attempts;
 }
 
 int orc_grad_hess(void* hp, int j, double* g, double* h) {

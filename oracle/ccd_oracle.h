@@ -29,6 +29,9 @@ int orc_set_beta(void* h, const double* beta);
 int orc_fit(void* h, int conv_type, double tol, int max_iter, double initial_bound,
             int max_bound_count, int algorithm, int use_kkt, const uint8_t* fixed, double* beta_out,
             double* ll_out, int* iters_out, int* flag_out, char* err, int errlen);
+/* Cycles of each findMode attempt of the last orc_fit (the ILLCONDITIONED
+ * retry runs several); returns the number of attempts, writes at most max_n. */
+int orc_fit_attempts(void* h, int* sweeps, int max_n);
 int orc_grad_hess(void* h, int j, double* g, double* hs);
 int orc_update_beta(void* h, int j, double delta);
 int orc_loglik(void* h, double* ll);

@@ -320,6 +320,15 @@ class RestatementEngine(_Engine):
     prefix = "orc_"
     libpath = PORT_LIB
 
+    def fit_attempts(self):
+        """Cycles of each findMode attempt of the last fit (the ILLCONDITIONED
+        retry of CyclicCoordinateDescent::update runs several)."""
+        fn = self.lib().orc_fit_attempts
+        fn.argtypes = [_P, _P, C.c_int]
+        buf = np.zeros(16, np.int32)
+        n = fn(self.h, _ptr(buf), 16)
+        return [int(x) for x in buf[:min(n, 16)]]
+
     @classmethod
     def set_exp_perturbation(cls, one_in: int, salt: int = 0):
         """Move exp by one ulp on 2 in `one_in` arguments (0: off), for every

@@ -36,16 +36,15 @@ def _rel(b, want):
     (MODEL_LOGISTIC, dict(seed=71, K=600, P=20, formats=("sparse", "dense", "indicator")), MITTAL),
     (MODEL_POISSON, dict(seed=72, K=600, P=20, offset=True, prior=PRIOR_NORMAL), MITTAL),
 ])
-def test_mixed_batch_matches_fp64_oracle(gpu_ctx, oracle_engine, monkeypatch, model, kw, conv, group, cluster):
+def test_mixed_batch_matches_fp64_oracle(gpu_ctx, oracle_engine, model, kw, conv, group, cluster):
     """cluster: CTAs per group, each owning a row range of every column."""
-    monkeypatch.setenv("CCDB_BATCH_CLUSTER", str(cluster))
     d = synthetic.small(model, **kw)
     fold = synthetic.cv_folds(d.K, n_folds=5, seed=4)
     hold, var = synthetic.cv_grid(n_folds=5, n_vars=3, lower=0.01, upper=10.0)
     m = native.Matrix(gpu_ctx, d)
     f = native.Fit(gpu_ctx, m, d, precision=native.PRECISION_MIXED)
     args = native.ModeFindingArguments(convergence_type=conv, tolerance=1e-10, max_iterations=2000)
-    beta, res, _ = f.batch_find_mode(var, hold, fold, args, group=group)
+    beta, res, _ = f.batch_find_mode(var, hold, fold, args, group=group, cluster=cluster)
     worst = 0.0
     for i in range(len(var)):
         di = d.with_prior(int(d.prior_type[-1]), float(var[i]))
@@ -64,18 +63,17 @@ def test_mixed_batch_matches_fp64_oracle(gpu_ctx, oracle_engine, monkeypatch, mo
 
 
 @pytest.mark.parametrize("cluster", [1, 4])
-def test_mixed_instance_alone_equals_in_group(gpu_ctx, monkeypatch, cluster):
+def test_mixed_instance_alone_equals_in_group(gpu_ctx, cluster):
     """An instance's arithmetic does not depend on its group mates: alone (its
     group padded) it gives bit-identical coefficients."""
-    monkeypatch.setenv("CCDB_BATCH_CLUSTER", str(cluster))
     d = synthetic.small(MODEL_LOGISTIC, seed=73, K=700, P=25)
     fold = synthetic.cv_folds(d.K, n_folds=4, seed=2)
     hold, var = synthetic.cv_grid(n_folds=4, n_vars=3, lower=0.05, upper=5.0)
     m = native.Matrix(gpu_ctx, d)
     f = native.Fit(gpu_ctx, m, d, precision=native.PRECISION_MIXED)
-    b_all, r_all, _ = f.batch_find_mode(var, hold, fold, group=4)
+    b_all, r_all, _ = f.batch_find_mode(var, hold, fold, group=4, cluster=cluster)
     for i in (0, 5, 11):
-        b1, r1, _ = f.batch_find_mode(var[i:i + 1], hold[i:i + 1], fold, group=4)
+        b1, r1, _ = f.batch_find_mode(var[i:i + 1], hold[i:i + 1], fold, group=4, cluster=cluster)
         assert np.array_equal(b1[0], b_all[i])
         assert r1[0]["iterations"] == r_all[i]["iterations"]
         assert r1[0]["loglik"] == r_all[i]["loglik"]

@@ -50,14 +50,18 @@ def test_cox_gradient_hessian(gpu_ctx, oracle_engine, kw):
 
 @pytest.mark.parametrize("kw", CASES)
 @pytest.mark.parametrize("conv", [GRADIENT, MITTAL, LANGE])
-@pytest.mark.parametrize("per_coordinate", [False, True])
-def test_cox_find_mode(gpu_ctx, oracle_engine, kw, conv, per_coordinate):
+@pytest.mark.parametrize("mode", ["device", "host_batches", "per_coordinate"])
+def test_cox_find_mode(gpu_ctx, oracle_engine, kw, conv, mode):
+    """device: one persistent launch per findMode (group_sweep.cu); host_batches:
+    the host-driven speculative batches; per_coordinate: the reference's call
+    pattern, one round trip per coordinate."""
     d = synthetic.small(MODEL_COX, **kw)
     want = oracle_engine(d).fit(conv, 1e-6)
     m = native.Matrix(gpu_ctx, d)
     f = native.Fit(gpu_ctx, m, d)
-    got = f.find_mode(native.ModeFindingArguments(convergence_type=conv,
-                                                  per_coordinate=per_coordinate))
+    got = f.find_mode(native.ModeFindingArguments(
+        convergence_type=conv, per_coordinate=(mode == "per_coordinate"),
+        strategy=native.SWEEP_SPECULATIVE if mode == "host_batches" else native.SWEEP_AUTO))
     assert got.return_flag == want["flag"]
     assert got.iterations == want["iterations"]
     assert rel_beta(got.beta, want["beta"]) <= BETA_TOL
@@ -87,3 +91,25 @@ def test_cox_deterministic(gpu_ctx):
     r2 = native.fit_model(gpu_ctx, d)
     assert np.array_equal(r1.beta, r2.beta)
     assert r1.log_likelihood == r2.log_likelihood
+
+
+@pytest.mark.parametrize("prior,var", [(PRIOR_LAPLACE, 0.05), (PRIOR_NORMAL, 1.0)])
+def test_cox_device_sweep_on_many_ctas(gpu_ctx, oracle_engine, prior, var):
+    """A problem large enough that the persistent sweep's row updates, group
+    runs and scans spread over every CTA: 60,000 rows in 150 strata of uneven
+    size, daily ties, 300 indicator columns; the device sweep against the
+    oracle and against the host-driven batches."""
+    d = synthetic.small(MODEL_COX, seed=12, K=60_000, P=300, density=0.004, n_strata=150, tie_days=4,
+                        formats=("indicator",), prior=prior, variance=var)
+    want = oracle_engine(d).fit(GRADIENT, 1e-6)
+    m = native.Matrix(gpu_ctx, d)
+    f = native.Fit(gpu_ctx, m, d)
+    got = f.find_mode(native.ModeFindingArguments(convergence_type=GRADIENT), beta=np.zeros(d.J))
+    host = f.find_mode(native.ModeFindingArguments(convergence_type=GRADIENT, strategy=native.SWEEP_SPECULATIVE),
+                       beta=np.zeros(d.J))
+    for r in (got, host):
+        assert r.return_flag == want["flag"]
+        assert r.iterations == want["iterations"]
+        assert rel_beta(r.beta, want["beta"]) <= BETA_TOL
+        assert abs(r.log_likelihood - want["loglik"]) <= LL_TOL * abs(want["loglik"])
+    assert got.kernel_launches < host.kernel_launches

@@ -46,10 +46,12 @@ def test_grouped_gradient_hessian(gpu_ctx, oracle_engine, model, kw):
 
 @pytest.mark.parametrize("model,kw", CASES)
 @pytest.mark.parametrize("conv", [GRADIENT, MITTAL, LANGE])
-def test_grouped_find_mode(gpu_ctx, oracle_engine, model, kw, conv):
+@pytest.mark.parametrize("strategy", [native.SWEEP_AUTO, native.SWEEP_SPECULATIVE])
+def test_grouped_find_mode(gpu_ctx, oracle_engine, model, kw, conv, strategy):
+    """AUTO: one persistent launch per findMode; SPECULATIVE: host-driven batches."""
     d = synthetic.small(model, **kw)
     want = oracle_engine(d).fit(conv, 1e-6)
-    got = native.fit_model(gpu_ctx, d, native.ModeFindingArguments(convergence_type=conv))
+    got = native.fit_model(gpu_ctx, d, native.ModeFindingArguments(convergence_type=conv, strategy=strategy))
     assert got.return_flag == want["flag"]
     assert got.iterations == want["iterations"]
     assert rel_beta(got.beta, want["beta"]) <= BETA_TOL
@@ -68,3 +70,15 @@ def test_clr_weighted(gpu_ctx, oracle_engine):
     got = f.find_mode()
     assert got.iterations == want["iterations"]
     assert rel_beta(got.beta, want["beta"]) <= BETA_TOL
+
+
+def test_clr_device_sweep_on_many_ctas(gpu_ctx, oracle_engine):
+    """20,000 matched sets (~130,000 rows), 400 indicator columns: the persistent
+    sweep's row updates and stratum runs spread over every CTA."""
+    d = synthetic.conditional_logistic(seed=13, n_sets=20_000, P=400)
+    want = oracle_engine(d).fit(GRADIENT, 1e-6)
+    got = native.fit_model(gpu_ctx, d, native.ModeFindingArguments(convergence_type=GRADIENT))
+    assert got.return_flag == want["flag"]
+    assert got.iterations == want["iterations"]
+    assert rel_beta(got.beta, want["beta"]) <= BETA_TOL
+    assert abs(got.log_likelihood - want["loglik"]) <= LL_TOL * abs(want["loglik"])

@@ -52,13 +52,14 @@ def test_per_coordinate_gradient_hessian(gpu_ctx, oracle_engine, model, kw):
 
 @pytest.mark.parametrize("model,kw", CASES)
 @pytest.mark.parametrize("conv", [GRADIENT, MITTAL, LANGE])
-@pytest.mark.parametrize("mode", ["levels", "speculative", "per_coordinate"])
+@pytest.mark.parametrize("mode", ["levels", "grid_levels", "speculative", "per_coordinate"])
 def test_find_mode_matches_oracle(gpu_ctx, oracle_engine, model, kw, conv, mode):
     d = synthetic.small(model, **kw)
     want = oracle_engine(d).fit(conv, 1e-6)
     m = native.Matrix(gpu_ctx, d)
     f = native.Fit(gpu_ctx, m, d)
-    strategy = {"levels": native.SWEEP_LEVELS, "speculative": native.SWEEP_SPECULATIVE}.get(mode, 0)
+    strategy = {"levels": native.SWEEP_LEVELS, "grid_levels": native.SWEEP_GRID_LEVELS,
+                "speculative": native.SWEEP_SPECULATIVE}.get(mode, 0)
     got = f.find_mode(native.ModeFindingArguments(convergence_type=conv, strategy=strategy,
                                                   per_coordinate=(mode == "per_coordinate")))
     assert got.return_flag == want["flag"]
@@ -67,7 +68,7 @@ def test_find_mode_matches_oracle(gpu_ctx, oracle_engine, model, kw, conv, mode)
     assert abs(got.log_likelihood - want["loglik"]) <= LL_TOL * abs(want["loglik"])
 
 
-@pytest.mark.parametrize("strategy", [1, 2])
+@pytest.mark.parametrize("strategy", [1, 2, 3])
 def test_logistic_l1_benchmark_problem(gpu_ctx, oracle_engine, strategy):
     """10,000 x 1,000 L1 logistic, MITTAL 1e-6, the reference's CPU-runnable case."""
     d = synthetic.logistic_l1(seed=1)
@@ -106,15 +107,16 @@ def test_fused_is_deterministic(gpu_ctx):
     (MODEL_POISSON, dict(offset=True, prior=PRIOR_NORMAL)),
     (MODEL_LOGISTIC, dict()),
 ])
-def test_split_columns_beyond_the_stage(gpu_ctx, oracle_engine, model, kw):
+@pytest.mark.parametrize("strategy", [1, 3])
+def test_split_columns_beyond_the_stage(gpu_ctx, oracle_engine, model, kw, strategy):
     """700,000 rows: the intercept splits over every CTA in chunks longer than a
     CTA stages, so its gradient takes the streaming path -- on the first
     dependency level, where the staged column metadata must be published to all
-    threads before the level starts."""
+    threads before the level starts (both level sweeps)."""
     d = synthetic.small(model, seed=5, K=700_000, P=3, density=0.001, formats=("indicator",), **kw)
     m = native.Matrix(gpu_ctx, d)
     f = native.Fit(gpu_ctx, m, d)
-    r = f.find_mode(native.ModeFindingArguments(convergence_type=GRADIENT, strategy=native.SWEEP_LEVELS))
+    r = f.find_mode(native.ModeFindingArguments(convergence_type=GRADIENT, strategy=strategy))
     want = oracle_engine(d).fit(GRADIENT, 1e-6)
     assert r.return_flag == want["flag"] and r.iterations == want["iterations"]
     assert rel_beta(r.beta, want["beta"]) <= BETA_TOL

@@ -45,20 +45,19 @@ def test_grid_sweep_wait_runs_out_then_recovers(gpu_ctx, oracle_engine):
     assert _rel(r.beta, want["beta"]) <= 1e-6
 
 
-def test_batch_cluster_exchange_wait_runs_out_then_recovers(gpu_ctx, monkeypatch):
-    monkeypatch.setenv("CCDB_BATCH_CLUSTER", "2")
+def test_batch_cluster_exchange_wait_runs_out_then_recovers(gpu_ctx):
     d = synthetic.small(MODEL_LOGISTIC, seed=81, K=900, P=30)
     fold = synthetic.cv_folds(d.K, n_folds=4, seed=3)
     hold, var = synthetic.cv_grid(n_folds=4, n_vars=2, lower=0.05, upper=5.0)
     m = native.Matrix(gpu_ctx, d)
     f = native.Fit(gpu_ctx, m, d, precision=native.PRECISION_MIXED)
-    b_want, r_want, _ = f.batch_find_mode(var, hold, fold, group=2)
+    b_want, r_want, _ = f.batch_find_mode(var, hold, fold, group=2, cluster=2)
     f.set_wait_limit(1)
     with pytest.raises(native.CcdbError) as ex:
-        f.batch_find_mode(var, hold, fold, group=2)
+        f.batch_find_mode(var, hold, fold, group=2, cluster=2)
     assert ex.value.code == native.ERR_TIMEOUT
     f.set_wait_limit(0)
-    b, r, _ = f.batch_find_mode(var, hold, fold, group=2)
+    b, r, _ = f.batch_find_mode(var, hold, fold, group=2, cluster=2)
     assert np.array_equal(b, b_want)
     assert [x["iterations"] for x in r] == [x["iterations"] for x in r_want]
     assert all(x["flag"] == 0 for x in r)
