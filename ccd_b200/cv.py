@@ -408,6 +408,72 @@ def grid_search(fit, row_fold, n_folds: int, lower: float = 0.01, upper: float =
     return out
 
 
+class ShardedFit:
+    """The batched calls of a fit, spread over the ranks of a torch.distributed
+    process group: one process per GPU, each with its own context, its own
+    copy of the matrix in its GPU's memory and its own fit (`fit`), all over
+    the same data.  Instance i of a call runs on rank i mod world (round
+    robin, so every rank gets a share of each variance, the weak priors being
+    the longest fits); after the local launch the ranks exchange their
+    (instance, coefficients, result) lists once (all_gather_object, a host
+    gather: no collective on the data path), so every rank returns the whole
+    call's results in instance order and the drivers above run unchanged, in
+    step, on every rank.  device_seconds is the slowest rank's.
+
+    grid_search / auto_search take a ShardedFit wherever they take a fit."""
+
+    def __init__(self, fit, group=None):
+        import torch.distributed as dist
+        self.fit = fit
+        self.d = fit.d
+        self.group = group
+        self.rank = dist.get_rank(group)
+        self.world = dist.get_world_size(group)
+
+    @property
+    def precision(self):
+        return getattr(self.fit, "precision", 0)
+
+    def _shard(self, n: int) -> np.ndarray:
+        return np.arange(self.rank, n, self.world)
+
+    def _gather(self, n: int, mine, beta, res, secs):
+        import torch.distributed as dist
+        parts = [None] * self.world
+        dist.all_gather_object(parts, (np.asarray(mine).tolist(), np.asarray(beta), list(res), float(secs)),
+                               group=self.group)
+        out_b = np.zeros((n, self.d.J))
+        out_r: list = [None] * n
+        for idx, b, r, _ in parts:
+            for q, i in enumerate(idx):
+                out_b[i] = b[q]
+                out_r[i] = r[q]
+        return out_b, out_r, max(p[3] for p in parts)
+
+    def batch_find_mode(self, variance, holdout=None, row_fold=None, args=None, group: int = 0,
+                        cluster: int = 0):
+        var = np.asarray(variance, dtype=np.float64)
+        n = var.shape[0]
+        mine = self._shard(n)
+        if len(mine):
+            hold = None if holdout is None else np.asarray(holdout)[mine]
+            beta, res, secs = self.fit.batch_find_mode(var[mine], hold, row_fold, args, group=group,
+                                                       cluster=cluster)
+        else:
+            beta, res, secs = np.zeros((0, self.d.J)), [], 0.0
+        return self._gather(n, mine, beta, res, secs)
+
+    def fold_instances(self, variances, holdout, row_fold, args=None):
+        var = np.asarray(variances, dtype=np.float64)
+        n = var.shape[0]
+        mine = self._shard(n)
+        if len(mine):
+            beta, res, secs = self.fit.fold_instances(var[mine], np.asarray(holdout)[mine], row_fold, args)
+        else:
+            beta, res, secs = np.zeros((0, self.d.J)), [], 0.0
+        return self._gather(n, mine, beta, res, secs)
+
+
 def refit_at(ctx, matrix, d: CyclopsData, variance, args=None):
     """resetForOptimal: all rows weighted 1, the selected variance parameters
     (a scalar: the first; a sequence: one per parameter, CVResult.variances),
