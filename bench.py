@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--small", action="store_true", help="a 10x smaller problem (quick checks)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="headline only: skip the other configurations' measurements nested in the line")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the converged oracle fit that the headline line's parity fields compare with")
     ap.add_argument("--max-sweeps", type=int, default=1000,
@@ -61,7 +63,7 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=200,
                     help="serve: requests in the replayed stream")
     ap.add_argument("--serve-slots", type=int, default=8, help="serve: concurrent fits")
-    ap.add_argument("--workload", choices=["poisson_offset", "cv_grid", "cox_breslow", "serve",
+    ap.add_argument("--workload", choices=["poisson_offset", "logistic_l1", "cv_grid", "cox_breslow", "serve",
                                            "kkt_l1", "mm_clr", "fisher_l1"],
                     default="poisson_offset",
                     help="poisson_offset: plain fits (default); cv_grid: 10 folds x 20 Laplace "
@@ -416,7 +418,7 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args, world, rank, local):
+def run_ours(args, world, rank, local, collect=False):
     import torch
     if world > 1:
         import datetime
@@ -435,7 +437,8 @@ def run_ours(args, world, rank, local):
     cold = cold_beta(d)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
 
-    parity = ConvergedReference(d, GRADIENT, 1e-6) if rank == 0 and not args.no_parity else None
+    parity = (ConvergedReference(d, GRADIENT, 1e-6)
+              if rank == 0 and not args.no_parity and WORKLOAD == "poisson_offset" else None)
     for _ in range(args.warmup):
         f.set_beta(cold)
         f.find_mode(margs)
@@ -549,12 +552,191 @@ def run_ours(args, world, rank, local):
             if parity.ref_seconds is not None:
                 line["cpu_time_to_converge_s"] = {"value": parity.ref_seconds, "cores": 1,
                                                   "kind": parity.ref_kind}
-        print(json.dumps(line), flush=True)
     f.close()
     m.close()
     ctx.close()
+    if rank == 0 and collect:
+        return line
+    if rank == 0:
+        if world == 1 and WORKLOAD == "poisson_offset" and not args.no_extras:
+            del flush
+            line["workloads"] = run_extras(args, local)
+        print(json.dumps(line), flush=True)
     if world > 1:
         tdist.destroy_process_group()
+
+
+def run_logistic_l1(args, world, rank, local, collect=False):
+    """The CPU-runnable configuration: L1 logistic regression, 10,000 rows x
+    1,000 indicator covariates at density 0.01 plus an intercept, Laplace
+    variance 0.1, FP64, relative log-likelihood change (MITTAL) 1e-6, cold
+    start.  A step is one converged fit; the reference engine's converged fit
+    of the same problem is timed on the host (single thread, repeated for a
+    stable figure) and the oracle's coefficients give the parity fields."""
+    import torch
+    from ccd_b200 import native
+    from ccd_b200.data import MITTAL
+    from oracle import checker
+    if rank != 0:
+        return None
+    d = synthetic.logistic_l1(seed=1)
+    ctx = native.Context(local)
+    m = native.Matrix(ctx, d)
+    f = native.Fit(ctx, m, d)
+    margs = native.ModeFindingArguments(convergence_type=MITTAL, tolerance=1e-6, max_iterations=args.max_sweeps,
+                                        strategy=STRATEGIES[args.strategy])
+    cold = cold_beta(d)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    for _ in range(args.warmup):
+        f.set_beta(cold)
+        f.find_mode(margs)
+    clocks = Clocks(local)
+    torch.cuda.synchronize()
+    clocks.start()
+    dev_t = ker_t = 0.0
+    sweeps = attempts = launches = 0
+    for _ in range(args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        f.set_beta(cold)
+        r = f.find_mode(margs)
+        dev_t += r.device_seconds
+        ker_t += r.kernel_seconds
+        sweeps += r.sweeps_total
+        attempts += r.attempts
+        launches += r.kernel_launches
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    e2e_t = 0.0
+    for _ in range(args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        e2e_t += native.fit_model(ctx, d, margs).device_seconds
+    h2d = sum(a.nbytes for a in (d.y, d.col_start, d.rows, d.val_start, d.vals, d.fmt))
+    f.close()
+    m.close()
+    ctx.close()
+    # the reference engine, whole converged fits, single thread
+    eng_cls = checker.best_engine()
+    kind = "reference" if eng_cls is checker.ReferenceEngine else "port"
+    eng = eng_cls(d)
+    eng.fit(MITTAL, 1e-6)
+    reps, t_ref = 0, 0.0
+    while t_ref < 2.0 and reps < 200:
+        eng.set_beta(cold)
+        t0 = time.perf_counter()
+        ref_fit = eng.fit(MITTAL, 1e-6)
+        t_ref += time.perf_counter() - t0
+        reps += 1
+    eng.close()
+    port = checker.RestatementEngine(d)
+    want = port.fit(MITTAL, 1e-6)
+    port.close()
+    active = active_columns(d)
+    peak, peak_kind = read_peaks()
+    total_bytes = sweep_bytes(d) * sweeps + objective_bytes(d) * (sweeps + attempts)
+    scale = max(float(np.max(np.abs(want["beta"]))), 1e-8)
+    line = {
+        "metric": METRIC, "value": sweeps * active / dev_t, "unit": METRIC, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * dev_t / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded PCG64)",
+        "config": {"workload": "logistic_l1", "model": "logistic", "rows": d.K, "columns": d.J, "nnz": d.nnz,
+                   "prior": "laplace(0.1), none on the intercept", "convergence": "mittal (relative LL), tol 1e-6",
+                   "precision": "fp64", "start": "cold (beta = 0)"},
+        "step": "one converged findMode from a cold start",
+        "time_to_converge_s": dev_t / args.steps,
+        "sweeps_per_fit": sweeps / args.steps,
+        "e2e": {"value": sweeps * active / e2e_t, "unit": METRIC, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d.J * 8)},
+        "roofline": {"bound": "hbm", "achieved": total_bytes / ker_t / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": total_bytes / ker_t / 1e9 / peak, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": total_bytes / attempts,
+                     "kernel": "cluster_sweep_kernel<LOGISTIC>", "traffic": None,
+                     "note": "1.1e5 entries per sweep: latency-bound, L2-resident"},
+        "cpu_baseline": {"value": ref_fit["iterations"] * active * reps / t_ref, "unit": METRIC, "cores": 1,
+                         "kind": kind, "time_to_converge_s": t_ref / reps,
+                         "sample": f"{reps} whole converged fits, single thread"},
+        "parity": {"oracle": "FP64 restatement of the reference",
+                   "max_rel_dbeta": float(np.max(np.abs(r.beta - want["beta"]))) / scale,
+                   "rel_dll": abs(r.log_likelihood - want["loglik"]) / max(1.0, abs(want["loglik"])),
+                   "iterations": {"gpu": int(r.iterations), "oracle": int(want["iterations"])},
+                   "return_flag": {"gpu": int(r.return_flag), "oracle": int(want["flag"])}},
+        "gpu_launches": int(launches), "clocks": clk,
+    }
+    if collect:
+        return line
+    print(json.dumps(line), flush=True)
+
+
+def run_logistic_l1_reference(args, world, rank):
+    """The reference engine on the CPU-runnable configuration: one whole
+    converged fit per step (a few milliseconds), single thread."""
+    if rank != 0:
+        return
+    from ccd_b200.data import MITTAL
+    from oracle import checker
+    d = synthetic.logistic_l1(seed=1)
+    eng_cls = checker.best_engine()
+    kind = "reference" if eng_cls is checker.ReferenceEngine else "port"
+    eng = eng_cls(d)
+    times, sweeps = [], 0
+    for i in range(args.warmup + args.steps):
+        eng.set_beta(cold_beta(d))
+        t0 = time.perf_counter()
+        r = eng.fit(MITTAL, 1e-6)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+            sweeps += r["iterations"]
+    eng.close()
+    total = float(np.sum(times))
+    v = sweeps * active_columns(d) / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded PCG64)",
+        "config": {"workload": "logistic_l1", "model": "logistic", "rows": d.K, "columns": d.J, "nnz": d.nnz,
+                   "prior": "laplace(0.1), none on the intercept", "convergence": "mittal (relative LL), tol 1e-6",
+                   "precision": "fp64", "start": "cold (beta = 0)"},
+        "step": "one converged findMode from a cold start",
+        "time_to_converge_s": total / args.steps,
+        "cpu_baseline": {"value": v, "unit": METRIC, "cores": 1, "kind": kind,
+                         "sample": "one whole converged fit per step, single thread"},
+        "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_extras(args, local) -> dict:
+    """The other configurations, measured after the headline in the same run
+    and nested in its line: the CPU-runnable L1 logistic fit, the Breslow Cox
+    fit, the cross-validation grid and the served stream.  Each runs its own
+    workload with a few warm-up and timed steps (bounded so the whole bench
+    stays within minutes); a failure is recorded, not raised."""
+    import copy
+    global WORKLOAD
+    out = {}
+    plans = [
+        ("logistic_l1", run_logistic_l1, dict(steps=max(3, min(args.steps, 20)), warmup=max(3, args.warmup))),
+        ("cox_breslow", run_ours, dict(steps=1, warmup=1, no_cpu_baseline=args.no_cpu_baseline)),
+        ("cv_grid", run_cv, dict(steps=1, warmup=1, plain_sample=2, fp64_check=2)),
+        ("serve", run_serve, dict(steps=1, warmup=1, serve_requests=200)),
+    ]
+    for name, fn, over in plans:
+        a = copy.copy(args)
+        for k, v in over.items():
+            setattr(a, k, v)
+        a.workload = name
+        WORKLOAD = name
+        t0 = time.perf_counter()
+        try:
+            out[name] = fn(a, 1, 0, local, collect=True)
+        except Exception as ex:  # recorded in the line
+            out[name] = {"error": f"{type(ex).__name__}: {str(ex)[:300]}"}
+        out[name]["bench_seconds"] = time.perf_counter() - t0
+    WORKLOAD = "poisson_offset"
+    return out
 
 
 def cv_workload(small: bool, columns: int = 20_000):
@@ -578,7 +760,7 @@ def cv_bytes(d, res) -> float:
     return idx + per
 
 
-def run_cv(args, world, rank, local):
+def run_cv(args, world, rank, local, collect=False):
     import torch
     import torch.distributed as tdist
     if world > 1:  # instances shard over the ranks; no data-path collective
@@ -694,6 +876,11 @@ def run_cv(args, world, rank, local):
         "gpu_launches": args.steps,
         "clocks": clk,
     }
+    f.close()
+    m.close()
+    ctx.close()
+    if collect:
+        return line
     print(json.dumps(line), flush=True)
     if world > 1:
         tdist.barrier()
@@ -796,7 +983,7 @@ def cv_cpu_sample(d, fold, hold, var, res):
 SERVE_RANGES = dict(rate=50.0, K_range=(1e3, 1e5), J_range=(1e2, 1e4), density_range=(0.001, 0.02))
 
 
-def run_serve(args, world, rank, local):
+def run_serve(args, world, rank, local, collect=False):
     """The served stream: Poisson(50/s) arrivals of independent logistic /
     conditional logistic / Cox fits, replayed in real time into the server."""
     import torch
@@ -849,6 +1036,8 @@ def run_serve(args, world, rank, local):
         "e2e": {"value": s["p50_s"], "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "roofline": None, "cpu_baseline": cpu, "gpu_launches": None, "clocks": clk,
     }
+    if collect:
+        return line
     print(json.dumps(line), flush=True)
 
 
@@ -1221,6 +1410,8 @@ def main():
         run_cv_reference(args, world, rank)
     elif args.impl == "reference" and args.workload == "serve":
         run_serve_reference(args, world, rank)
+    elif args.impl == "reference" and args.workload == "logistic_l1":
+        run_logistic_l1_reference(args, world, rank)
     elif args.impl == "reference":
         run_reference(args, world, rank)
     elif args.workload in VARIANTS:
@@ -1229,6 +1420,8 @@ def main():
         run_cv(args, world, rank, local)
     elif args.workload == "serve":
         run_serve(args, world, rank, local)
+    elif args.workload == "logistic_l1":
+        run_logistic_l1(args, world, rank, local)
     else:
         run_ours(args, world, rank, local)
 

@@ -16,7 +16,12 @@
 // streams, or different host threads on one device) race on it.  The host
 // needs the array's device address, which it obtains once per device with
 // cudaGetSymbolAddress; the first call on each device does that set-up (no
-// allocation), so make that first call before any stream capture begins.
+// allocation) and also loads both models' kernels on that device (with lazy
+// module loading a kernel's first launch would otherwise load it then), so
+// one call of either model on a device, made before any stream capture
+// begins, prepares every later call there.  The address is kept for the life
+// of the process: resetting the device (cudaDeviceReset) after that first
+// call is not supported.
 #include <cstdint>
 #include <mutex>
 #include <string>
@@ -129,6 +134,11 @@ extern "C" int ccdb_column_gradient_hessian_noalloc(int32_t model_type, int32_t 
             void* p = nullptr;
             if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p)
                 return fail(CCDB_ERR_CUDA, "noalloc gradient: cannot resolve the scratch address");
+            cudaFuncAttributes fa;
+            if (cudaFuncGetAttributes(&fa, noalloc_partial_kernel<M_LOGISTIC>) != cudaSuccess ||
+                cudaFuncGetAttributes(&fa, noalloc_partial_kernel<M_POISSON>) != cudaSuccess ||
+                cudaFuncGetAttributes(&fa, noalloc_finish_kernel) != cudaSuccess)
+                return fail(CCDB_ERR_CUDA, "noalloc gradient: cannot load the kernels");
             g_scratch_addr[dev] = static_cast<double2*>(p);
         }
         scratch = g_scratch_addr[dev];

@@ -290,8 +290,10 @@ int ccdb_batch_find_mode(ccdb_fit* f, const ccdb_batch_desc* batch, const ccdb_m
  * library holds that array until the process exits.  All calls share it and
  * it keeps the last call's contents (each call overwrites the slots it
  * reads); calls whose kernels overlap on the GPU race on it.  The first call
- * on each device looks up the array's device address (no allocation): make
- * it before any stream capture. */
+ * on each device looks up the array's device address and loads this entry
+ * point's kernels there (no allocation): make one call on a device before any
+ * stream capture, and do not reset the device (cudaDeviceReset) afterwards,
+ * since the address is kept for the life of the process. */
 int ccdb_column_gradient_hessian_noalloc(int32_t model_type, int32_t fmt, int64_t n_entries,
                                          const int32_t* rows, const double* vals,
                                          const double* row_state, double xjy, double* out,

@@ -22,16 +22,23 @@ pytestmark = pytest.mark.gpu
 GH_TOL = 1e-10
 
 
+@pytest.mark.parametrize("weighted", [False, True])
 @pytest.mark.parametrize("model,kw", [
     (MODEL_LOGISTIC, dict(seed=90, K=700, P=12)),
     (MODEL_POISSON, dict(seed=91, K=500, P=9, formats=("sparse", "dense", "indicator"))),
 ])
-def test_noalloc_matches_regular_entry_point(gpu_ctx, model, kw):
+def test_noalloc_matches_regular_entry_point(gpu_ctx, model, kw, weighted):
+    """weighted: random non-negative row weights (zeros included), the
+    cross-validation case, against the regular entry point on a weighted fit."""
     import torch
     d = synthetic.small(model, **kw)
     m = native.Matrix(gpu_ctx, d)
     f = native.Fit(gpu_ctx, m, d)
-    beta = np.random.default_rng(5).normal(0, 0.2, size=d.J)
+    rng = np.random.default_rng(5)
+    w = np.where(rng.random(d.K) < 0.2, 0.0, rng.uniform(0.2, 2.0, d.K)) if weighted else np.ones(d.K)
+    if weighted:
+        f.set_weights(w)
+    beta = rng.normal(0, 0.2, size=d.J)
     f.set_beta(beta)
     want = np.array([f.compute_gradient_and_hessian(j) for j in range(d.J)])
 
@@ -39,7 +46,8 @@ def test_noalloc_matches_regular_entry_point(gpu_ctx, model, kw):
     xb = torch.tensor(f.get_xbeta(), dtype=torch.float64, device="cuda")
     e = torch.exp(xb)
     denom = (1.0 + e) if model == MODEL_LOGISTIC else e.clone()
-    state = torch.stack([xb, e, denom, torch.ones_like(xb)], dim=1).contiguous()
+    state = torch.stack([xb, e, denom, torch.tensor(w, dtype=torch.float64, device="cuda")],
+                        dim=1).contiguous()
     out = torch.zeros(2, dtype=torch.float64, device="cuda")
     stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     lib = native.lib()
@@ -52,10 +60,10 @@ def test_noalloc_matches_regular_entry_point(gpu_ctx, model, kw):
         vals_t = torch.tensor(v, dtype=torch.float64, device="cuda") if len(v) else None
         if fmt in (DENSE, INTERCEPT):
             x = v if fmt == DENSE else np.ones(d.K)
-            xjy = float(np.sum(x * d.y))
+            xjy = float(np.sum(x * d.y * w))
         else:
             x = v if fmt == SPARSE else np.ones(len(r))
-            xjy = float(np.sum(x * d.y[r]))
+            xjy = float(np.sum(x * d.y[r] * w[r]))
         for call in range(2):  # two calls in a row share (and overwrite) the scratch
             out.zero_()
             rc = lib.ccdb_column_gradient_hessian_noalloc(
