@@ -408,6 +408,7 @@ void Fit::find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* 
                "bounds");
     if (a.algorithm == CCDB_ALGORITHM_MM) {
         auto t0 = std::chrono::steady_clock::now();
+        nz_known = false;  // the MM cycle moves every coordinate at once
         find_mode_mm(a, flag, iters, obj);
         *ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
         return;
@@ -425,7 +426,10 @@ void Fit::find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* 
                 gradient_hessian(j, &g, &h);
                 double delta = newton_prior_delta(g, h, beta_h[j], ptype_h[j], pvar_h[j]);
                 delta = apply_bounds(delta, hd[j]);
-                if (delta != 0.0) update_xbeta(j, delta);
+                if (delta != 0.0) {
+                    update_xbeta(j, delta);
+                    ++nz_steps;
+                }
             }
             ++iteration;
             const double cur = objective(a.convergence_type);
@@ -529,6 +533,8 @@ void Fit::find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* 
     *flag = out.flag;
     *iters = out.iterations;
     *obj = out.objective;
+    if (kind == kSchedCluster) nz_steps += (int64_t)out.nonzero_steps;
+    else nz_known = false;  // the grid-wide sweep does not count them
     beta_dirty_host = true;
 }
 
@@ -564,6 +570,7 @@ void Fit::find_mode_batched(const ccdb_mode_args& a, double bound, int* flag, in
                 if (delta != 0.0) {
                     beta_h[j] += delta;
                     apply_step(j, delta);
+                    ++nz_steps;
                     advanced = i + 1;
                     break;
                 }
@@ -661,6 +668,8 @@ void Fit::find_mode(const ccdb_mode_args& a, double* beta_inout, ccdb_fit_result
     int active = 0;
     for (int j = 0; j < J; ++j) active += fixed[j] ? 0 : 1;
     const int64_t launches0 = launches;
+    nz_steps = 0;
+    nz_known = true;
     check_cuda(cudaEventRecord(evc0, stream), "event");
     double bound = a.initial_bound;
     int count = 0, flag = R_FAIL, sweeps_total = 0;
@@ -713,6 +722,7 @@ void Fit::find_mode(const ccdb_mode_args& a, double* beta_inout, ccdb_fit_result
         res->kernel_launches = launches - launches0;
         res->attempts = count;
         res->sweeps_total = sweeps_total;
+        res->nonzero_steps = nz_known ? nz_steps : -1;
     }
 }
 

@@ -363,6 +363,7 @@ void Fit::find_mode_group_sweep(const ccdb_mode_args& a, int* flag, int* iters, 
                                           std::to_string(out.error_where) + ")");
     cox.last_updates = cnt[0];
     cox.last_batches = cnt[1];
+    nz_steps += cnt[0];
     *flag = out.flag;
     *iters = out.iterations;
     *obj = out.objective;

@@ -151,6 +151,8 @@ struct Fit {
     int64_t launches = 0;                        // engine kernels launched so far
     double last_call_seconds = 0.0;              // device time of the last fisher_information passes
     int last_iterations = 0;                     // getIterationCount: the last findMode's cycles
+    int64_t nz_steps = 0;                        // nonzero coordinate steps of the current find_mode
+    bool nz_known = true;                        // every path of the call counted them
     std::unique_ptr<DevSchedule> sched;
     CoxDev cox;
 

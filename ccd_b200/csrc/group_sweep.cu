@@ -435,9 +435,12 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
         }
         if (done) break;
     }
-    if (b == 0 && tid == 0 && Q.counters) {
-        Q.counters[0] = n_updates;
-        Q.counters[1] = n_batches;
+    if (b == 0 && tid == 0) {
+        if (Q.counters) {
+            Q.counters[0] = n_updates;
+            Q.counters[1] = n_batches;
+        }
+        Q.st->nonzero_steps = (unsigned long long)n_updates;
     }
 }
 

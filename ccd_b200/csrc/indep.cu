@@ -743,6 +743,7 @@ __global__ void __launch_bounds__(kThreads, 1) cluster_sweep_kernel(IndepParams 
     const unsigned C = gridDim.x, rank = cl_rank();
     const int64_t seg0 = P.cta_seg[rank], seg1 = P.cta_seg[rank + 1];
     int rb = 0;
+    unsigned long long moved = 0;  // nonzero steps written by this thread
 
     // the objective of the current state, combined in rank order in every CTA
     auto objective_all = [&](double& ll) -> double4 {
@@ -843,7 +844,10 @@ __global__ void __launch_bounds__(kThreads, 1) cluster_sweep_kernel(IndepParams 
                     const double2 s = cta_sum2(make_double2(g, h), s_red2, rb);
                     double hd;
                     const double d = meta_step(m, t.p1, s.x, s.y, hd);
-                    if (tid == 0) meta_write(P, t.col, m, d, hd);
+                    if (tid == 0) {
+                        meta_write(P, t.col, m, d, hd);
+                        if (d != 0.0) ++moved;
+                    }
                     if (d != 0.0) {
                         if (staged) staged_update_smem(P, sc, s_gath, tid, d);
                         else update_dispatch(P, t.col, f, t.p0, t.p1, tid, blockDim.x, d);
@@ -872,7 +876,10 @@ __global__ void __launch_bounds__(kThreads, 1) cluster_sweep_kernel(IndepParams 
                         const double2 s = warp_sum2(make_double2(g, h));
                         double hd;
                         const double d = meta_step(m, t.p1, s.x, s.y, hd);
-                        if (lane == 0) meta_write(P, t.col, m, d, hd);
+                        if (lane == 0) {
+                            meta_write(P, t.col, m, d, hd);
+                            if (d != 0.0) ++moved;
+                        }
                         if (d != 0.0) {
                             if (staged) staged_update_smem(P, sw, s_gath, tid, d);
                             else update_dispatch(P, t.col, f, t.p0, t.p1, lane, 32, d);
@@ -914,7 +921,10 @@ __global__ void __launch_bounds__(kThreads, 1) cluster_sweep_kernel(IndepParams 
                         m.hd = s_stash[q].y;
                         double hd;
                         const double d = meta_step(m, 1, s.x, s.y, hd);  // split columns are never empty
-                        if (t.chunk == 0 && tid == 0) meta_write(P, t.col, m, d, hd);
+                        if (t.chunk == 0 && tid == 0) {
+                            meta_write(P, t.col, m, d, hd);
+                            if (d != 0.0) ++moved;
+                        }
                         if (d != 0.0) {
                             const uint8_t f = (uint8_t)m.fmt;
                             if (q == sg.n_chunk - 1 && stageable<kE>(t, blockDim.x)) {
@@ -964,6 +974,7 @@ __global__ void __launch_bounds__(kThreads, 1) cluster_sweep_kernel(IndepParams 
         if (done) break;  // the same decision in every CTA: no barrier is left open
         cl_arrive();      // s_obj is read; the next sweep's first wait completes this barrier
     }
+    if (moved) atomicAdd(&P.st->nonzero_steps, moved);
 }
 
 // ---------------------------------------------------------------- per-coordinate kernels

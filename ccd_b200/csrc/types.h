@@ -48,6 +48,8 @@ struct DevStatus {
     double last_objective;
     double loglik;
     double log_prior;
+    unsigned long long nonzero_steps;  // coordinate steps that moved a coefficient (device sweeps)
+    unsigned long long pad2;
 };
 
 }  // namespace ccdb

@@ -66,7 +66,7 @@ class _FitResult(C.Structure):
                 ("log_likelihood", C.c_double), ("objective", C.c_double),
                 ("coordinate_updates", C.c_int64), ("device_seconds", C.c_double),
                 ("kernel_seconds", C.c_double), ("kernel_launches", C.c_int64),
-                ("attempts", C.c_int32), ("sweeps_total", C.c_int32)]
+                ("attempts", C.c_int32), ("sweeps_total", C.c_int32), ("nonzero_steps", C.c_int64)]
 
 
 @dataclass
@@ -97,6 +97,7 @@ class FitResult:
     kernel_launches: int = 0
     attempts: int = 1       # findMode runs (the ILLCONDITIONED retry adds some)
     sweeps_total: int = 0   # cycles over all of them
+    nonzero_steps: int = -1  # steps that moved a coefficient (-1: not counted)
 
 
 _lib = None
@@ -450,7 +451,7 @@ class Fit:
         out = b if b is not None else self.get_beta()
         return FitResult(out, res.return_flag, res.iterations, res.log_likelihood, res.objective,
                          res.coordinate_updates, res.device_seconds, res.kernel_seconds,
-                         res.kernel_launches, res.attempts, res.sweeps_total)
+                         res.kernel_launches, res.attempts, res.sweeps_total, res.nonzero_steps)
 
 
 def fit_model(ctx: Context, d: CyclopsData, args: Optional[ModeFindingArguments] = None,
@@ -470,7 +471,7 @@ def fit_model(ctx: Context, d: CyclopsData, args: Optional[ModeFindingArguments]
                                 C.byref(ma), _p(beta), C.byref(res)))
     return FitResult(beta, res.return_flag, res.iterations, res.log_likelihood, res.objective,
                      res.coordinate_updates, res.device_seconds, res.kernel_seconds,
-                     res.kernel_launches, res.attempts, res.sweeps_total)
+                     res.kernel_launches, res.attempts, res.sweeps_total, res.nonzero_steps)
 
 
 def validate_matrix(d: CyclopsData) -> None:

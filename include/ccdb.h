@@ -214,6 +214,8 @@ typedef struct {
     int64_t kernel_launches;    /* engine kernels launched by the call */
     int32_t attempts;           /* findMode runs: 1, plus one per ILLCONDITIONED retry */
     int32_t sweeps_total;       /* cycles over every attempt (iterations counts the last) */
+    int64_t nonzero_steps;      /* coordinate steps that moved a coefficient, every attempt;
+                                   -1 where the sweep used does not count them */
 } ccdb_fit_result;
 
 /* Run CyclicCoordinateDescent::update (.cpp:586-615): findMode, with the
