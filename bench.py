@@ -588,6 +588,21 @@ def run_ours(args, world, rank, local, collect=False):
             if parity.ref_seconds is not None:
                 line["cpu_time_to_converge_s"] = {"value": parity.ref_seconds, "cores": 1,
                                                   "kind": parity.ref_kind}
+    if rank == 0 and WORKLOAD == "cox_breslow":
+        # the same fit in mixed precision beside FP64, and its error against the FP64 fit
+        fm = native.Fit(ctx, m, d, precision=native.PRECISION_MIXED)
+        fm.set_beta(cold)
+        fm.find_mode(margs)  # warm-up
+        fm.set_beta(cold)
+        rm = fm.find_mode(margs)
+        fm.close()
+        scale = max(float(np.max(np.abs(last.beta))), 1e-8)
+        line["mixed_precision"] = {
+            "ms_per_fit": 1e3 * rm.device_seconds, "iterations": int(rm.iterations),
+            "return_flag": int(rm.return_flag), "coordinate_updates_per_s": rm.coordinate_updates / rm.device_seconds,
+            "max_rel_dbeta_vs_fp64": float(np.max(np.abs(rm.beta - last.beta))) / scale,
+            "rel_dll_vs_fp64": abs(rm.log_likelihood - last.log_likelihood) / max(1.0, abs(last.log_likelihood)),
+            "arithmetic": "FP32 exp and per-entry terms (TwoSum), FP64 risk-set sums, reductions, step"}
     f.close()
     m.close()
     ctx.close()

@@ -900,7 +900,7 @@ int ccdb_fit_create(ccdb_context* ctx, const ccdb_matrix* m, const ccdb_fit_desc
             throw Error(CCDB_ERR_INVALID, "Cox fits need survival times");
         if (d->precision != CCDB_PRECISION_FP64 &&
             !(d->precision == CCDB_PRECISION_MIXED &&
-              (d->model_type == M_LOGISTIC || d->model_type == M_POISSON)))
+              (d->model_type == M_LOGISTIC || d->model_type == M_POISSON || d->model_type == M_COX)))
             throw Error(CCDB_ERR_UNSUPPORTED, "precision not supported for this model");
         check_cuda(cudaSetDevice(ctx->device), "cudaSetDevice");
         std::unique_ptr<ccdb_fit> f(new ccdb_fit());
@@ -960,10 +960,11 @@ int ccdb_fit_destroy(ccdb_fit* f) {
     return guard([&] { delete f; });
 }
 
-// Mixed precision is implemented by the batched engine; the single-fit calls
-// compute in FP64 only and refuse a mixed fit rather than ignore its setting.
+// Mixed precision of logistic and Poisson fits is implemented by the batched
+// engine; their single-fit calls compute in FP64 only and refuse a mixed fit
+// rather than ignore its setting.  Cox fits take it in every call.
 static void require_fp64(const ccdb_fit* f) {
-    if (f->precision != CCDB_PRECISION_FP64)
+    if (f->precision != CCDB_PRECISION_FP64 && f->model != M_COX)
         throw Error(CCDB_ERR_UNSUPPORTED, "mixed precision serves batched fits (ccdb_batch_find_mode) only");
 }
 

@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(kT) cox_update_kernel(CoxParams P, int j, doub
             const double x = has_vals ? __ldg(P.vals + vb + p) : 1.0;
             const double2 xe = P.xbe[k];
             const double xb = xe.x + delta * x;
-            const double en = exp(xb);
+            const double en = row_exp(xb, P.mixed);
             P.xbe[k] = make_double2(xb, en);
             grp = P.grp[k];
             if (P.weighted) {
@@ -112,7 +112,7 @@ __global__ void cox_exp_kernel(CoxParams P) {
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P.K;
          k += (int64_t)gridDim.x * blockDim.x) {
         const double xb = P.xbe[k].x;
-        P.xbe[k] = make_double2(xb, exp(xb));
+        P.xbe[k] = make_double2(xb, row_exp(xb, P.mixed));
     }
 }
 

@@ -25,7 +25,7 @@ struct CoxParams {
     const int32_t* grp;    // group of each row (N: dropped by a zero weight)
     const int32_t* rstrat; // stratum index of each row
     int32_t weighted;
-    int32_t pad0;
+    int32_t mixed;  // Cox, CCDB_PRECISION_MIXED: FP32 exp and per-entry gradient terms
     // groups (N + 1 slots; slot N absorbs dropped rows and reads as zero)
     double* denom;
     double* D;

@@ -71,6 +71,7 @@ CoxParams Fit::cox_params() const {
     P.grp = cox.grp;
     P.rstrat = cox.rstrat;
     P.weighted = weighted ? 1 : 0;
+    P.mixed = (is_cox() && precision == CCDB_PRECISION_MIXED) ? 1 : 0;
     P.denom = cox.denom;
     P.D = cox.D;
     P.S1 = cox.S1;

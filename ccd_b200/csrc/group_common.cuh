@@ -53,6 +53,21 @@ __device__ __forceinline__ Seg2 block_seg_scan(Seg2 x, Seg2* s_w, Seg2* agg) {
     return x;
 }
 
+// exp of a row's xBeta: FP64, or in the mixed precision of the Cox engine
+// FP32 (expf of the rounded xBeta), kept in the FP64 row state.
+__device__ __forceinline__ double row_exp(double xb, int mixed) {
+    return mixed ? (double)expf((float)xb) : exp(xb);
+}
+
+// Knuth's TwoSum: s + c carries the running FP32 sum with the rounding error
+// of every addition kept in c.
+__device__ __forceinline__ void two_sum_f(float& s, float& c, float v) {
+    const float t = s + v;
+    const float bp = t - s;
+    c += (s - (t - bp)) + (v - bp);
+    s = t;
+}
+
 // Shared memory of one CTA computing column gradients.
 struct GhShared {
     Seg2 w[kW], w2[kW];
@@ -77,11 +92,13 @@ __device__ __forceinline__ double2 cox_column_gh(const CoxParams& P, int j, GhSh
     const int64_t cb = P.col_ptr[j], vb = P.val_ptr[j];
     const int64_t n = has_rows ? (P.col_ptr[j + 1] - cb) : P.K;
     double g = 0.0, h2 = 0.0, hq = 0.0;
+    float gs = 0.f, gc = 0.f, hs = 0.f, hc = 0.f;  // mixed: FP32 TwoSum partials of g and h2
     double carry = 0.0;
     int32_t carry_key = -1;
     for (int64_t base = 0; base < n; base += kT) {
         const int64_t p = base + threadIdx.x;
         double n1 = 0.0, n2 = 0.0, s1 = 0.0, s2 = 0.0;
+        float n1f = 0.f, n2f = 0.f;
         int32_t key = 0x7fffffff;  // past the end: a segment of its own
         if (p < n) {
             const int64_t k = has_rows ? (int64_t)__ldg(P.rows + cb + p) : p;
@@ -89,9 +106,17 @@ __device__ __forceinline__ double2 cox_column_gh(const CoxParams& P, int j, GhSh
             const int32_t grp = P.grp[k];
             const double2 xe = __ldcg(P.xbe + k);
             const double w = P.w[k];
-            // incrementNumeratorForGradientImpl (ModelSpecifics.hpp:1433-1449)
-            n1 = P.weighted ? w * (xe.y * x) : xe.y * x;
-            if (!ind) n2 = P.weighted ? w * (xe.y * x * x) : xe.y * x * x;
+            if (P.mixed) {  // the per-entry terms in FP32
+                const float xf = (float)x, ef = (float)xe.y;
+                n1f = P.weighted ? (float)w * (ef * xf) : ef * xf;
+                if (!ind) n2f = n1f * xf;
+                n1 = (double)n1f;
+                n2 = (double)n2f;
+            } else {
+                // incrementNumeratorForGradientImpl (ModelSpecifics.hpp:1433-1449)
+                n1 = P.weighted ? w * (xe.y * x) : xe.y * x;
+                if (!ind) n2 = P.weighted ? w * (xe.y * x * x) : xe.y * x * x;
+            }
             key = P.rstrat[k];
             s1 = __ldcg(P.S1 + grp);  // S1[N] = S2[N] = 0 for dropped rows
             s2 = __ldcg(P.S2 + grp);
@@ -105,9 +130,15 @@ __device__ __forceinline__ double2 cox_column_gh(const CoxParams& P, int j, GhSh
         const double A_incl = r.v;
         const double A_excl = A_incl - n1;
         if (p < n) {
-            g += n1 * s1;
-            h2 += n2 * s1;
-            hq += s2 * (A_incl * A_incl - A_excl * A_excl);
+            if (P.mixed) {
+                const float s1f = (float)s1;
+                two_sum_f(gs, gc, n1f * s1f);
+                two_sum_f(hs, hc, n2f * s1f);
+            } else {
+                g += n1 * s1;
+                h2 += n2 * s1;
+            }
+            hq += s2 * (A_incl * A_incl - A_excl * A_excl);  // risk-set sums: FP64
         }
         // carry: the value of the last element of this tile
         if (threadIdx.x == kT - 1) {
@@ -118,6 +149,10 @@ __device__ __forceinline__ double2 cox_column_gh(const CoxParams& P, int j, GhSh
         carry = S.last;
         carry_key = S.last_key;
         __syncthreads();
+    }
+    if (P.mixed) {
+        g = (double)gs + (double)gc;
+        h2 = (double)hs + (double)hc;
     }
     double2 v = warp_sum2(make_double2(g, h2));
     double q = hq;

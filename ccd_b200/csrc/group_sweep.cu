@@ -368,7 +368,7 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
                     const double x = has_vals ? __ldg(P.vals + vb + p) : 1.0;
                     const double2 xe = __ldcg(P.xbe + k);
                     const double xb = xe.x + delta * x;
-                    const double en = exp(xb);
+                    const double en = row_exp(xb, P.mixed);
                     __stcg(P.xbe + k, make_double2(xb, en));
                     double dd;
                     if (COX && P.weighted) {

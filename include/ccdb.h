@@ -40,9 +40,11 @@ extern "C" {
 #define CCDB_ERR_TIMEOUT (-5)     /* a bounded device-side wait ran out */
 
 #define CCDB_PRECISION_FP64 0  /* all arithmetic in double, as the reference's RealType=double */
-#define CCDB_PRECISION_MIXED 1 /* batched fits only: FP64 xBeta and step; exp, ratios and
-                                  per-entry gradient/Hessian terms in FP32 with compensated
-                                  sums; FP64 cross-thread reductions and log-likelihoods */
+#define CCDB_PRECISION_MIXED 1 /* FP64 xBeta and step; exp, ratios and per-entry
+                                  gradient/Hessian terms in FP32 with compensated sums; FP64
+                                  cross-thread reductions, Cox risk-set sums and
+                                  log-likelihoods.  Logistic/Poisson: batched fits only
+                                  (ccdb_batch_find_mode); Cox: every call */
 
 typedef struct ccdb_context ccdb_context;
 typedef struct ccdb_matrix ccdb_matrix;

@@ -113,3 +113,23 @@ def test_cox_device_sweep_on_many_ctas(gpu_ctx, oracle_engine, prior, var):
         assert rel_beta(r.beta, want["beta"]) <= BETA_TOL
         assert abs(r.log_likelihood - want["loglik"]) <= LL_TOL * abs(want["loglik"])
     assert got.kernel_launches < host.kernel_launches
+
+
+@pytest.mark.parametrize("kw", [CASES[0], CASES[3], CASES[4]])
+def test_cox_mixed_precision_against_fp64_oracle(gpu_ctx, oracle_engine, kw):
+    """CCDB_PRECISION_MIXED Cox: FP32 exp and per-entry gradient terms with
+    compensated sums; FP64 risk-set sums, reductions, step and log-likelihood.
+    Fitted to 1e-10 so that the comparison measures the arithmetic rather than
+    where each run stopped: coefficients within 1e-6 of their scale of the
+    FP64 oracle, log-likelihood within 1e-8."""
+    d = synthetic.small(MODEL_COX, **kw)
+    want = oracle_engine(d).fit(GRADIENT, 1e-10, 2000)
+    m = native.Matrix(gpu_ctx, d)
+    f = native.Fit(gpu_ctx, m, d, precision=native.PRECISION_MIXED)
+    got = f.find_mode(native.ModeFindingArguments(convergence_type=GRADIENT, tolerance=1e-10,
+                                                  max_iterations=2000))
+    assert got.return_flag == want["flag"] == 0
+    err = rel_beta(got.beta, want["beta"])
+    print(f"mixed Cox: max relative coefficient error {err:.2e}")
+    assert err <= 1e-6
+    assert abs(got.log_likelihood - want["loglik"]) <= 1e-8 * abs(want["loglik"])
