@@ -254,17 +254,21 @@ int Fit::sweep_kind(const ccdb_mode_args& a) const {
 }
 
 void Fit::ensure_schedule(int kind) {
-    if (sched && sched->fixed == fixed && sched->kind == kind) return;
-    release_schedule();
+    int C = 0;  // the cluster sweep's size: the largest resident, within the context's CTA share
     if (kind == kSchedCluster) {
         if (ctx->sweep_cluster < 0) {
             int c = 0;
             check_cuda(cluster_sweep_max_size(model, &c), "cluster occupancy");
             ctx->sweep_cluster = c;
         }
-        int C = ctx->sweep_cluster;
+        C = ctx->sweep_cluster;
         if (C < 1) throw Error(CCDB_ERR_CUDA, "the cluster sweep kernel cannot be resident");
         while (ctx->max_ctas > 0 && C > ctx->max_ctas && C > 1) C /= 2;
+    }
+    if (sched && sched->fixed == fixed && sched->kind == kind && (kind != kSchedCluster || sched->cluster == C))
+        return;
+    release_schedule();
+    if (kind == kSchedCluster) {
         ScheduleParams sp;
         sp.n_cta = C;
         sp.warps_per_cta = indep_threads() / 32;
@@ -493,10 +497,16 @@ void Fit::find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* 
     P.max_iter = a.max_iterations;
     // CCDB_TRACE_FILE=<path>: dump per-segment timestamps of the first sweep
     // together with the schedule (profiling aid; off by default)
-    const char* trace_path = (kind == kSchedGrid) ? std::getenv("CCDB_TRACE_FILE") : nullptr;
+    const char* trace_path = std::getenv("CCDB_TRACE_FILE");
     unsigned long long* d_trace = nullptr;
     const size_t n_seg = sched->host.segs.size();
-    if (trace_path) {
+    if (trace_path && kind == kSchedCluster) {
+        // the cluster sweep: 4 timestamps per level and CTA of the first sweep
+        const size_t n = 4 * (size_t)sched->host.n_levels * sched->cluster;
+        d_trace = static_cast<unsigned long long*>(ctx->alloc(sizeof(unsigned long long) * n));
+        check_cuda(cudaMemsetAsync(d_trace, 0, sizeof(unsigned long long) * n, stream), "trace");
+        P.trace = d_trace;
+    } else if (trace_path) {
         d_trace = static_cast<unsigned long long*>(ctx->alloc(sizeof(unsigned long long) * 5 * n_seg));
         check_cuda(cudaMemsetAsync(d_trace, 0, sizeof(unsigned long long) * 5 * n_seg, stream), "trace");
         P.trace = d_trace;
@@ -511,6 +521,23 @@ void Fit::find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* 
     check_cuda(cudaMemcpyAsync(&out, st, sizeof(out), cudaMemcpyDeviceToHost, stream), "status");
     check_cuda(cudaStreamSynchronize(stream), "sweep");
     check_cuda(cudaEventElapsedTime(ms, ev0, ev1), "elapsed");
+    if (d_trace && kind == kSchedCluster) {
+        const size_t n = 4 * (size_t)sched->host.n_levels * sched->cluster;
+        std::vector<unsigned long long> tr(n);
+        check_cuda(cudaMemcpy(tr.data(), d_trace, sizeof(unsigned long long) * n, cudaMemcpyDeviceToHost),
+                   "trace copy");
+        ctx->release(d_trace);
+        d_trace = nullptr;
+        if (FILE* fh = std::fopen(trace_path, "wb")) {
+            // header: levels, CTAs; then the level of every column, the split flags, the stamps
+            const int64_t hdr[2] = {sched->host.n_levels, sched->cluster};
+            std::fwrite(hdr, sizeof(int64_t), 2, fh);
+            std::fwrite(sched->host.level_of.data(), sizeof(int32_t), sched->host.level_of.size(), fh);
+            std::fwrite(sched->host.level_split.data(), 1, sched->host.level_split.size(), fh);
+            std::fwrite(tr.data(), sizeof(unsigned long long), n, fh);
+            std::fclose(fh);
+        }
+    }
     if (d_trace) {
         std::vector<unsigned long long> tr(5 * n_seg);
         check_cuda(cudaMemcpy(tr.data(), d_trace, sizeof(unsigned long long) * 5 * n_seg,

@@ -303,14 +303,17 @@ __device__ __forceinline__ bool xch_sum(const Inst<G>& I, double (&v)[2], ColXch
     phase_bits ^= 1u << slot;
     const unsigned a = smem_addr(&x.bar[slot]);
     const unsigned long long t0 = xch_now();
+    const unsigned hint_ns = (unsigned)(limit_ns < 20000ull ? (limit_ns > 0 ? limit_ns : 1ull) : 20000ull);
     bool raised = false;
     for (;;) {
         unsigned done;
+        // try_wait may suspend the thread in hardware; the hint bounds each
+        // suspension so that the loop sees the time and the bound
         asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3;\n"
             " selp.u32 %0, 1, 0, p;\n}\n"
             : "=r"(done)
-            : "r"(a), "r"(parity)
+            : "r"(a), "r"(parity), "r"(hint_ns)
             : "memory");
         if (done) break;
         const unsigned long long dt = xch_now() - t0;

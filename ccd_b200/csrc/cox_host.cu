@@ -204,6 +204,10 @@ void Fit::cox_apply_weights() {
                "grow");
     check_cuda(cudaMemsetAsync(cox.S1 + N, 0, sizeof(double), stream), "S1N");
     check_cuda(cudaMemsetAsync(cox.S2 + N, 0, sizeof(double), stream), "S2N");
+    // slot N gathers the rows a zero weight drops; like the reference's denomPid[N]
+    // it holds 0, which the MM bound reads (0 * e / 0 for such a row, as there)
+    check_cuda(cudaMemsetAsync(cox.denom + N, 0, sizeof(double), stream), "denomN");
+    check_cuda(cudaMemsetAsync(cox.D + N, 0, sizeof(double), stream), "DN");
     check_cuda(launch_xjy(m->d_col_ptr, m->d_rows, m->d_val_ptr, m->d_vals, m->d_fmt, y,
                           weighted ? w : nullptr, K, J, xjy, stream),
                "xjy");

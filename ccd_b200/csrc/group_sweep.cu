@@ -114,6 +114,40 @@ __device__ __forceinline__ void thread_share(int64_t lo, int64_t hi, int64_t& a,
     b = lo + len * (threadIdx.x + 1) / blockDim.x;
 }
 
+// Up to kCh consecutive groups of a thread's share are loaded before they are
+// combined, so a thread has kCh independent loads in flight instead of one
+// dependent load per group.
+constexpr int kCh = 4;
+
+// The forward (prefix) elements {gfirst, denominator} of groups [g, g + n).
+__device__ __forceinline__ void load_fwd(const CoxParams& P, int64_t g, int n, int (&f)[kCh], double (&v)[kCh]) {
+#pragma unroll
+    for (int i = 0; i < kCh; ++i)
+        if (i < n) {
+            f[i] = P.gfirst[g + i];
+            v[i] = __ldcg(P.denom + g + i);
+        }
+}
+
+// The suffix elements {glast, nEv/D, nEv/D^2} of groups [g, g + n).
+__device__ __forceinline__ void load_rev(const CoxParams& P, int64_t g, int n, int (&f)[kCh], double (&a)[kCh],
+                                         double (&c)[kCh]) {
+    double D[kCh], ne[kCh];
+#pragma unroll
+    for (int i = 0; i < kCh; ++i)
+        if (i < n) {
+            f[i] = P.glast[g + i];
+            D[i] = __ldcg(P.D + g + i);
+            ne[i] = P.nEv[g + i];
+        }
+#pragma unroll
+    for (int i = 0; i < kCh; ++i)
+        if (i < n) {
+            a[i] = ne[i] / D[i];
+            c[i] = ne[i] / (D[i] * D[i]);
+        }
+}
+
 // D, S1, S2 rebuilt from the group denominators (Cox).  Three phases separated
 // by grid barriers; false when a barrier wait ran out.
 __device__ bool cox_rebuild(const GroupSweepParams& Q, unsigned& epoch, int32_t* s_fail, Seg3* s_w,
@@ -123,17 +157,24 @@ __device__ bool cox_rebuild(const GroupSweepParams& Q, unsigned& epoch, int32_t*
     const int64_t g0 = P.N * b / G, g1 = P.N * (b + 1) / G;
     int64_t t0, t1;
     thread_share(g0, g1, t0, t1);
+    int fl[kCh];
+    double va[kCh], vb[kCh];
     // phase 1: aggregate of the CTA's range (prefix direction)
     Seg3 mine{0, 0.0, 0.0};
-    for (int64_t g = t0; g < t1; ++g) {
-        const Seg3 e{P.gfirst[g], __ldcg(P.denom + g), 0.0};
-        mine = (g == t0) ? e : seg3_combine(mine, e);
+    for (int64_t g = t0; g < t1; g += kCh) {
+        const int n = (int)(int)(t1 - g < kCh ? t1 - g : kCh);
+        load_fwd(P, g, n, fl, va);
+#pragma unroll
+        for (int i = 0; i < kCh; ++i)
+            if (i < n) {
+                const Seg3 e{fl[i], va[i], 0.0};
+                mine = (g + i == t0) ? e : seg3_combine(mine, e);
+            }
     }
     block_excl_scan3<false>(mine, s_w, s_tot);
     if (threadIdx.x == 0) {
-        SegAgg a{s_tot->f, 0, s_tot->a, 0.0};
-        __stcg(&Q.agg[b].f, a.f);
-        __stcg(&Q.agg[b].v0, a.v0);
+        __stcg(&Q.agg[b].f, s_tot->f);
+        __stcg(&Q.agg[b].v0, s_tot->a);
     }
     if (!grid_barrier(Q.grid_bar, epoch, Q.wait_limit_ns, Q.st, s_fail)) return false;
     // phase 2: carry-in from the CTAs before, D of the range; suffix aggregates
@@ -151,17 +192,28 @@ __device__ bool cox_rebuild(const GroupSweepParams& Q, unsigned& epoch, int32_t*
         // running value entering this thread's first group
         Seg3 run = (b == 0) ? pre : (threadIdx.x == 0 ? *s_carry : seg3_combine(*s_carry, pre));
         const bool has_run = (b > 0) || (threadIdx.x > 0);
-        Seg3 rs{0, 0.0, 0.0};  // suffix aggregate of the thread's share, built from the top
-        for (int64_t g = t0; g < t1; ++g) {
-            const Seg3 e{P.gfirst[g], __ldcg(P.denom + g), 0.0};
-            run = (!has_run && g == t0) ? e : seg3_combine(run, e);
-            __stcg(P.D + g, run.a);
+        for (int64_t g = t0; g < t1; g += kCh) {
+            const int n = (int)(int)(t1 - g < kCh ? t1 - g : kCh);
+            load_fwd(P, g, n, fl, va);
+#pragma unroll
+            for (int i = 0; i < kCh; ++i)
+                if (i < n) {
+                    const Seg3 e{fl[i], va[i], 0.0};
+                    run = (!has_run && g + i == t0) ? e : seg3_combine(run, e);
+                    __stcg(P.D + g + i, run.a);
+                }
         }
-        for (int64_t g = t1 - 1; g >= t0; --g) {
-            const double D = __ldcg(P.D + g);
-            const double ne = P.nEv[g];
-            const Seg3 e{P.glast[g], ne / D, ne / (D * D)};
-            rs = (g == t1 - 1) ? e : seg3_combine(rs, e);
+        Seg3 rs{0, 0.0, 0.0};  // suffix aggregate of the thread's share, built from the top
+        for (int64_t hi = t1; hi > t0; hi -= kCh) {
+            const int64_t g = (hi - kCh > t0 ? hi - kCh : t0);
+            const int n = (int)(hi - g);
+            load_rev(P, g, n, fl, va, vb);
+#pragma unroll
+            for (int i = kCh - 1; i >= 0; --i)
+                if (i < n) {
+                    const Seg3 e{fl[i], va[i], vb[i]};
+                    rs = (g + i == t1 - 1) ? e : seg3_combine(rs, e);
+                }
         }
         mine = rs;
     }
@@ -187,13 +239,18 @@ __device__ bool cox_rebuild(const GroupSweepParams& Q, unsigned& epoch, int32_t*
         const bool last_cta = (b == G - 1);
         Seg3 run = last_cta ? suf : (threadIdx.x == kT - 1 ? *s_carry : seg3_combine(*s_carry, suf));
         const bool has_run = !last_cta || (threadIdx.x < kT - 1);
-        for (int64_t g = t1 - 1; g >= t0; --g) {
-            const double D = __ldcg(P.D + g);
-            const double ne = P.nEv[g];
-            const Seg3 e{P.glast[g], ne / D, ne / (D * D)};
-            run = (!has_run && g == t1 - 1) ? e : seg3_combine(run, e);
-            __stcg(P.S1 + g, run.a);
-            __stcg(P.S2 + g, run.b);
+        for (int64_t hi = t1; hi > t0; hi -= kCh) {
+            const int64_t g = (hi - kCh > t0 ? hi - kCh : t0);
+            const int n = (int)(hi - g);
+            load_rev(P, g, n, fl, va, vb);
+#pragma unroll
+            for (int i = kCh - 1; i >= 0; --i)
+                if (i < n) {
+                    const Seg3 e{fl[i], va[i], vb[i]};
+                    run = (!has_run && g + i == t1 - 1) ? e : seg3_combine(run, e);
+                    __stcg(P.S1 + g + i, run.a);
+                    __stcg(P.S2 + g + i, run.b);
+                }
         }
     }
     return grid_barrier(Q.grid_bar, epoch, Q.wait_limit_ns, Q.st, s_fail);

@@ -732,7 +732,7 @@ template <int MODEL>
 __global__ void __launch_bounds__(kThreads, 1) cluster_sweep_kernel(IndepParams P) {
     __shared__ double4 s_red4[kWarps];
     __shared__ double2 s_red2[2][kWarps];
-    __shared__ double2 s_split[kMaxSplit][kMaxClusterSweep];  // [slot][rank] chunk partials
+    __shared__ double2 s_split[kMaxSplit][kMaxClusterSweep];  // [slot][chunk] chunk partials
     __shared__ double2 s_obj[kMaxClusterSweep][2];             // [rank] objective terms
     __shared__ double2 s_stash[kMaxSplit];  // {beta, hDelta} of this CTA's chunks, read in phase A
     __shared__ ColMeta s_meta[kWarps + 1];
@@ -774,7 +774,10 @@ __global__ void __launch_bounds__(kThreads, 1) cluster_sweep_kernel(IndepParams 
 
     for (int it = 0; it < P.max_iter; ++it) {
         int64_t si = seg0;
+        // optional timestamps of the first sweep: per level and CTA, entry, opened, phase A done, released
+        unsigned long long* tr = (P.trace && it == 0 && tid == 0) ? P.trace + 4 * (size_t)rank : nullptr;
         for (int L = 0; L < P.n_levels; ++L) {
+            if (tr) tr[(size_t)L * 4 * C] = global_ns();
             Seg sg{};
             const bool mine = si < seg1 && P.segs[si].level == L;
             if (mine) sg = P.segs[si];
@@ -823,6 +826,7 @@ __global__ void __launch_bounds__(kThreads, 1) cluster_sweep_kernel(IndepParams 
                 }
             }
             cl_wait();  // the previous level (or the objective) is complete in every CTA
+            if (tr) tr[(size_t)L * 4 * C + 1] = global_ns();
             if (mine) {
                 __syncthreads();  // s_meta, s_wstage of this level
                 // ---- CTA tasks
@@ -902,9 +906,12 @@ __global__ void __launch_bounds__(kThreads, 1) cluster_sweep_kernel(IndepParams 
                     }
                     const double2 s = cta_sum2(make_double2(g, h), s_red2, rb);
                     if (tid == 0) s_stash[q] = make_double2(m.beta, m.hd);
-                    if (tid < (int)C) st_peer_d2(&s_split[t.slot][rank], tid, s);
+                    // slot [column's exchange slot][chunk index]: every chunk's CTA adds the
+                    // partials in chunk order, whichever ranks the chunks sit on
+                    if (tid < (int)C) st_peer_d2(&s_split[t.slot][t.chunk], tid, s);
                 }
             }
+            if (tr) tr[(size_t)L * 4 * C + 2] = global_ns();
             if (P.level_split[L]) {
                 cl_arrive();
                 cl_wait();  // every chunk's partial has arrived
@@ -940,6 +947,7 @@ __global__ void __launch_bounds__(kThreads, 1) cluster_sweep_kernel(IndepParams 
                 }
             }
             cl_arrive();  // this CTA's updates of level L are released to the cluster
+            if (tr) tr[(size_t)L * 4 * C + 3] = global_ns();
             if (mine) ++si;
         }
         cl_wait();  // every level of the sweep is complete
