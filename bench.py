@@ -831,7 +831,16 @@ def run_cv(args, world, rank, local, collect=False):
     f = native.Fit(ctx, m, d, precision=prec)
     margs = native.ModeFindingArguments(convergence_type=GRADIENT, tolerance=1e-6,
                                         max_iterations=args.max_sweeps)
-    grid = lambda fit: fit.batch_find_mode(var, hold, fold, margs, group=args.group)
+    tuned = None
+    group, cluster = args.group, 0
+    if mixed and not args.group:
+        # the launch shape from one measured sweep per candidate (ccd_b200.tune), outside the timing
+        from ccd_b200 import tune
+        ch = tune.tune_batch(f, var, hold, fold, margs)
+        group, cluster = ch.group, ch.cluster
+        tuned = {"group": group, "cluster": cluster, "cached": ch.cached,
+                 "one_sweep_seconds": {f"G{g}C{c}": v for (g, c), v in sorted(ch.seconds.items())}}
+    grid = lambda fit: fit.batch_find_mode(var, hold, fold, margs, group=group, cluster=cluster)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
     for _ in range(args.warmup):
         grid(f)
@@ -912,6 +921,7 @@ def run_cv(args, world, rank, local, collect=False):
         "dtype": "f32/f64 (f32 exp, ratios, per-entry terms; f64 state, reductions, step)" if mixed else "f64",
         "data": "synthetic (seeded PCG64, workload shapes of the benchmark config)",
         "config": cv_config(args, d, len(var), world),
+        "launch_shape": tuned or {"group": group, "cluster": cluster or "engine's choice"},
         "e2e": {"value": world * len(var) * args.steps / e2e_t, "unit": "fits/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "plain_fits_per_s": plain_n / plain_t if plain_n else None,
