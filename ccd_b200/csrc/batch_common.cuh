@@ -303,19 +303,19 @@ __device__ __forceinline__ bool xch_sum(const Inst<G>& I, double (&v)[2], ColXch
     phase_bits ^= 1u << slot;
     const unsigned a = smem_addr(&x.bar[slot]);
     const unsigned long long t0 = xch_now();
-    const unsigned hint_ns = (unsigned)(limit_ns < 20000ull ? (limit_ns > 0 ? limit_ns : 1ull) : 20000ull);
     bool raised = false;
-    for (;;) {
+    for (unsigned n = 0;; ++n) {
         unsigned done;
-        // try_wait may suspend the thread in hardware; the hint bounds each
-        // suspension so that the loop sees the time and the bound
+        // test_wait returns at once (try_wait may suspend the thread in hardware
+        // until the phase completes, which would hide the bound from this loop)
         asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3;\n"
+            "{\n .reg .pred p;\n mbarrier.test_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
             " selp.u32 %0, 1, 0, p;\n}\n"
             : "=r"(done)
-            : "r"(a), "r"(parity), "r"(hint_ns)
+            : "r"(a), "r"(parity)
             : "memory");
         if (done) break;
+        if (n > 8) __nanosleep(32);
         const unsigned long long dt = xch_now() - t0;
         if (!raised && dt > limit_ns) {
             atomicExch(abort, 1);

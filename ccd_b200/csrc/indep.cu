@@ -685,6 +685,44 @@ __device__ __forceinline__ void st_peer_d2(const void* p, unsigned rank, double2
     asm volatile("st.shared::cluster.v2.f64 [%0], {%1, %2};" ::"r"(ra), "d"(v.x), "d"(v.y) : "memory");
 }
 
+// Look-ahead staging of the cluster sweep: a segment's task records (at most
+// kSegTaskCap of them; longer segments read them from global memory) are copied
+// into shared memory with cp.async while the previous level runs, and their
+// columns' metadata is prefetched into L1 before the barrier that opens them.
+constexpr int kSegTaskCap = 128;
+constexpr size_t kClusterSmem = kGatherSmem + 2 * kSegTaskCap * sizeof(Task);
+
+__device__ __forceinline__ int seg_tasks(const Seg& sg) { return sg.n_chunk + sg.n_cta + sg.n_warp; }
+
+__device__ __forceinline__ void copy_tasks(const IndepParams& P, const Seg& sg, Task* dst, int tid) {
+    const int n = seg_tasks(sg);
+    if (n > kSegTaskCap) return;
+    const char* src = reinterpret_cast<const char*>(P.tasks + sg.t0);
+    char* d = reinterpret_cast<char*>(dst);
+    for (int c = tid; c < 2 * n; c += blockDim.x) {  // 16-byte pieces of 32-byte records
+        const unsigned a = (unsigned)__cvta_generic_to_shared(d + 16 * c);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(a), "l"(src + 16 * c) : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all_tasks() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+__device__ __forceinline__ void prefetch_meta(const IndepParams& P, const Seg& sg, const Task* T, int tid) {
+    const int n = seg_tasks(sg);
+    for (int q = tid; q < n; q += blockDim.x) {
+        const int j = T[q].col;
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(P.col_ptr + j));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(P.val_ptr + j));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(P.fmt + j));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(P.xjy + j));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(P.pvar + j));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(P.ptype + j));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(P.beta + j));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(P.hdelta + j));
+    }
+}
+
 // CTA-wide sum of (g, h) with a fixed combination order, returned to every
 // thread with identical bits: warp butterflies, one barrier, then every warp
 // combines the kWarps per-warp sums by the same half-warp butterfly.
@@ -737,7 +775,12 @@ __global__ void __launch_bounds__(kThreads, 1) cluster_sweep_kernel(IndepParams 
     __shared__ double2 s_stash[kMaxSplit];  // {beta, hDelta} of this CTA's chunks, read in phase A
     __shared__ ColMeta s_meta[kWarps + 1];
     __shared__ Staged<kEw> s_wstage[kThreads];
+    // look-ahead: the task records of this CTA's next segment are copied here
+    // (cp.async) while the current level runs, and the metadata they point to is
+    // prefetched into L1 before the level's barrier
     extern __shared__ __align__(16) double2 s_gath[];
+    Task (*s_tasks)[kSegTaskCap] = reinterpret_cast<Task (*)[kSegTaskCap]>(
+        reinterpret_cast<char*>(s_gath) + kGatherSmem);  // after the gather slots, in dynamic memory
 
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const unsigned C = gridDim.x, rank = cl_rank();
@@ -776,12 +819,25 @@ __global__ void __launch_bounds__(kThreads, 1) cluster_sweep_kernel(IndepParams 
         int64_t si = seg0;
         // optional timestamps of the first sweep: per level and CTA, entry, opened, phase A done, released
         unsigned long long* tr = (P.trace && it == 0 && tid == 0) ? P.trace + 4 * (size_t)rank : nullptr;
+        // this CTA's current (cseg) and next segments; cseg's tasks sit in s_tasks[tb]
+        Seg cseg{}, nxt{};
+        cseg.level = nxt.level = -1;
+        int tb = 0;
+        if (si < seg1) {
+            cseg = P.segs[si];
+            copy_tasks(P, cseg, s_tasks[tb], tid);
+        }
+        if (si + 1 < seg1) nxt = P.segs[si + 1];
         for (int L = 0; L < P.n_levels; ++L) {
             if (tr) tr[(size_t)L * 4 * C] = global_ns();
+            const bool mine = (cseg.level == L);
             Seg sg{};
-            const bool mine = si < seg1 && P.segs[si].level == L;
-            if (mine) sg = P.segs[si];
-            const Task* T = P.tasks + sg.t0;
+            if (mine) {
+                sg = cseg;
+                cp_async_wait_all_tasks();
+                __syncthreads();  // every thread's part of the task copy has landed
+            }
+            const Task* T = (mine && seg_tasks(sg) <= kSegTaskCap) ? s_tasks[tb] : P.tasks + sg.t0;
             const int n_cl = sg.n_chunk + sg.n_cta;
             const int qw0 = n_cl, qw1 = qw0 + sg.n_warp;
 
@@ -829,6 +885,7 @@ __global__ void __launch_bounds__(kThreads, 1) cluster_sweep_kernel(IndepParams 
             if (tr) tr[(size_t)L * 4 * C + 1] = global_ns();
             if (mine) {
                 __syncthreads();  // s_meta, s_wstage of this level
+                if (nxt.level >= 0) copy_tasks(P, nxt, s_tasks[tb ^ 1], tid);
                 // ---- CTA tasks
                 for (int q = sg.n_chunk; q < n_cl; ++q) {
                     const Task t = T[q];
@@ -911,6 +968,11 @@ __global__ void __launch_bounds__(kThreads, 1) cluster_sweep_kernel(IndepParams 
                     if (tid < (int)C) st_peer_d2(&s_split[t.slot][t.chunk], tid, s);
                 }
             }
+            if (mine && nxt.level >= 0) {
+                cp_async_wait_all_tasks();
+                __syncthreads();
+                prefetch_meta(P, nxt, seg_tasks(nxt) <= kSegTaskCap ? s_tasks[tb ^ 1] : P.tasks + nxt.t0, tid);
+            }
             if (tr) tr[(size_t)L * 4 * C + 2] = global_ns();
             if (P.level_split[L]) {
                 cl_arrive();
@@ -948,7 +1010,13 @@ __global__ void __launch_bounds__(kThreads, 1) cluster_sweep_kernel(IndepParams 
             }
             cl_arrive();  // this CTA's updates of level L are released to the cluster
             if (tr) tr[(size_t)L * 4 * C + 3] = global_ns();
-            if (mine) ++si;
+            if (mine) {
+                ++si;
+                cseg = nxt;
+                tb ^= 1;
+                nxt.level = -1;
+                if (si + 1 < seg1) nxt = P.segs[si + 1];
+            }
         }
         cl_wait();  // every level of the sweep is complete
         double ll;
@@ -1158,7 +1226,7 @@ cudaError_t launch_indep_sweep(const IndepParams& P, int n_cta, cudaStream_t str
 template <int MODEL>
 static cudaError_t cluster_attrs() {
     cudaError_t e = cudaFuncSetAttribute(cluster_sweep_kernel<MODEL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kGatherSmem);
+                                         (int)kClusterSmem);
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(cluster_sweep_kernel<MODEL>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
 }
@@ -1168,7 +1236,7 @@ static cudaError_t cluster_config(int C, cudaStream_t stream, cudaLaunchConfig_t
     cfg = cudaLaunchConfig_t{};
     cfg.gridDim = dim3(C);
     cfg.blockDim = dim3(kThreads);
-    cfg.dynamicSmemBytes = kGatherSmem;
+    cfg.dynamicSmemBytes = kClusterSmem;
     cfg.stream = stream;
     at[0].id = cudaLaunchAttributeClusterDimension;
     at[0].val.clusterDim.x = C;
