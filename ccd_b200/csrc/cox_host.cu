@@ -1,6 +1,8 @@
 // cox_host.cu -- host side of the Breslow Cox engine: risk-set grouping,
 // per-group tables, and the per-coordinate calls on the device.
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -353,6 +355,16 @@ void Fit::find_mode_group_sweep(const ccdb_mode_args& a, int* flag, int* iters, 
     Q.st = st;
     Q.wait_limit_ns = wait_limit_ns;
     Q.counters = cox.counters;
+    // CCDB_TRACE_FILE=<path>: timestamps of the first 4,096 nonzero steps (profiling aid; off by default)
+    const char* trace_path = std::getenv("CCDB_TRACE_FILE");
+    unsigned long long* d_trace = nullptr;
+    const int trace_steps = 4096;
+    if (trace_path) {
+        d_trace = static_cast<unsigned long long*>(ctx->alloc(sizeof(unsigned long long) * 6 * trace_steps));
+        check_cuda(cudaMemsetAsync(d_trace, 0, sizeof(unsigned long long) * 6 * trace_steps, stream), "trace");
+        Q.trace = d_trace;
+        Q.trace_steps = trace_steps;
+    }
     check_cuda(cudaEventRecord(ev0, stream), "event");
     check_cuda(launch_group_sweep(Q, n_cta, stream), "group sweep launch");
     ++launches;
@@ -363,6 +375,16 @@ void Fit::find_mode_group_sweep(const ccdb_mode_args& a, int* flag, int* iters, 
     check_cuda(cudaMemcpyAsync(cnt, cox.counters, sizeof(cnt), cudaMemcpyDeviceToHost, stream), "counters");
     check_cuda(cudaStreamSynchronize(stream), "group sweep");
     check_cuda(cudaEventElapsedTime(ms, ev0, ev1), "elapsed");
+    if (d_trace) {
+        std::vector<unsigned long long> tr(6 * (size_t)trace_steps);
+        check_cuda(cudaMemcpy(tr.data(), d_trace, sizeof(unsigned long long) * tr.size(), cudaMemcpyDeviceToHost),
+                   "trace copy");
+        ctx->release(d_trace);
+        if (FILE* fh = std::fopen(trace_path, "wb")) {
+            std::fwrite(tr.data(), sizeof(unsigned long long), tr.size(), fh);
+            std::fclose(fh);
+        }
+    }
     if (out.error != E_NONE)
         throw Error(CCDB_ERR_TIMEOUT, "device wait timed out (code " + std::to_string(out.error) + " at " +
                                           std::to_string(out.error_where) + ")");

@@ -328,6 +328,8 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
     unsigned epoch = 0;
     int pend_pos = 0, pend_n = 0, pend_col = -1;  // CTA 0's writes held back to the next barrier
     long long n_updates = 0, n_batches = 0;
+    unsigned long long* trc = (Q.trace && Q.trace_steps > 0 && b == 0 && tid == 0) ? Q.trace : nullptr;
+    int trn = Q.trace_steps;
 
     // grid barrier, then CTA 0 applies the held-back writes of the last decision
     auto barrier = [&]() -> bool {
@@ -350,6 +352,9 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
         int pos = 0, batch = 32;
         while (pos < Q.n_active) {
             const int nb = min(batch, Q.n_active - pos);
+            // optional timestamps of the first nonzero steps (CTA 0): batch start, decided,
+            // rows updated, denominators updated, rebuilt, next
+            if (trc) trc[0] = global_ns();
             // gradients of the batch, one CTA per column; the two halves of gh
             // alternate by batch, so a CTA that is on to the next batch never
             // overwrites values another CTA is still deciding from
@@ -360,6 +365,7 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
                 if (tid == 0) __stcg(gh + c, r);
             }
             if (!barrier()) return;
+            if (trc) trc[1] = global_ns();
             // the decision, in every CTA from the same values: the first nonzero step
             if (tid == 0) s_first = nb;
             __syncthreads();
@@ -438,6 +444,7 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
                     __stcg(Q.ddg + p, P.grp[k]);
                 }
                 if (!barrier()) return;
+                if (trc) trc[2] = global_ns();
                 // the first row of each group's run adds the run's changes in row order;
                 // rows dropped by a zero weight (group N) may sit inside a run
                 for (int64_t p = p0 + tid; p < p1; p += blockDim.x) {
@@ -456,9 +463,16 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
                     __stcg(P.denom + g, d);
                 }
                 if (!barrier()) return;
+                if (trc) trc[3] = global_ns();
             }
             if (COX && !cox_rebuild(Q, epoch, &s_fail, s_w3, &s_tot, &s_carry)) return;
+            if (trc) trc[4] = global_ns();
             pos += first + 1;
+            if (trc) {
+                trc[5] = global_ns();
+                trc += 6;
+                if (--trn <= 0) trc = nullptr;
+            }
             batch = 32;
         }
         // the sweep is complete: held-back writes land, then the objective

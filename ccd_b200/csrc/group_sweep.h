@@ -44,6 +44,11 @@ struct GroupSweepParams {
     DevStatus* st;
     long long wait_limit_ns;
     int64_t* counters;      // [0]: nonzero steps, [1]: gradient batches (whole launch)
+    // optional timestamps of the first trace_steps nonzero steps (profiling aid): per
+    // step, the start of its batch, decided, rows updated, denominators, rebuilt, done
+    unsigned long long* trace;
+    int32_t trace_steps;
+    int32_t pad;
 };
 
 cudaError_t group_sweep_occupancy(int* blocks_per_sm);
