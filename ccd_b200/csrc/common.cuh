@@ -120,11 +120,11 @@ __device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned& epoch,
     __syncthreads();
     if (threadIdx.x == 0) {
         ++epoch;
-        __threadfence();
-        atomicAdd(counter, 1u);
+        // the CTA's writes, ordered before this thread's by the barrier above, are
+        // released with the arrival; the waits' acquire loads order every later read
+        red_release_gpu_add(counter, 1u);
         const bool ok = wait_geq(counter, epoch * gridDim.x, limit, st, E_WAIT_GRID, -1);
         *s_fail = ok ? 0 : 1;
-        __threadfence();
     }
     __syncthreads();
     return *s_fail == 0;

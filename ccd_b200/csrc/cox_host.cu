@@ -360,8 +360,8 @@ void Fit::find_mode_group_sweep(const ccdb_mode_args& a, int* flag, int* iters, 
     unsigned long long* d_trace = nullptr;
     const int trace_steps = 4096;
     if (trace_path) {
-        d_trace = static_cast<unsigned long long*>(ctx->alloc(sizeof(unsigned long long) * 6 * trace_steps));
-        check_cuda(cudaMemsetAsync(d_trace, 0, sizeof(unsigned long long) * 6 * trace_steps, stream), "trace");
+        d_trace = static_cast<unsigned long long*>(ctx->alloc(sizeof(unsigned long long) * kTraceStamps * trace_steps));
+        check_cuda(cudaMemsetAsync(d_trace, 0, sizeof(unsigned long long) * kTraceStamps * trace_steps, stream), "trace");
         Q.trace = d_trace;
         Q.trace_steps = trace_steps;
     }
@@ -376,7 +376,7 @@ void Fit::find_mode_group_sweep(const ccdb_mode_args& a, int* flag, int* iters, 
     check_cuda(cudaStreamSynchronize(stream), "group sweep");
     check_cuda(cudaEventElapsedTime(ms, ev0, ev1), "elapsed");
     if (d_trace) {
-        std::vector<unsigned long long> tr(6 * (size_t)trace_steps);
+        std::vector<unsigned long long> tr(kTraceStamps * (size_t)trace_steps);
         check_cuda(cudaMemcpy(tr.data(), d_trace, sizeof(unsigned long long) * tr.size(), cudaMemcpyDeviceToHost),
                    "trace copy");
         ctx->release(d_trace);

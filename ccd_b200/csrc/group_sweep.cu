@@ -43,13 +43,6 @@ namespace {
 
 using namespace grp;
 
-struct Seg3 {
-    int f;
-    double a, b;
-};
-__device__ __forceinline__ Seg3 seg3_combine(Seg3 x, Seg3 y) {
-    return Seg3{x.f | y.f, y.f ? y.a : x.a + y.a, y.f ? y.b : x.b + y.b};
-}
 
 // Exclusive scan of one Seg3 per thread in thread order (REV: in reverse
 // thread order), fixed combination order; *total gets the block aggregate.
@@ -87,15 +80,23 @@ __device__ __forceinline__ Seg3 block_excl_scan3(Seg3 x, Seg3* s_w, Seg3* total)
     const bool last_in_warp = REV ? (lane == 0) : (lane == 31);
     if (last_in_warp) s_w[wid] = inc;
     __syncthreads();
-    if (threadIdx.x == 0) {  // exclusive scan of the warp aggregates in scan order
-        Seg3 run{0, 0.0, 0.0};
-        for (int q = 0; q < kW; ++q) {
-            const int w = REV ? (kW - 1 - q) : q;
-            const Seg3 t = s_w[w];
-            s_w[w] = run;
-            run = (q == 0) ? t : seg3_combine(run, t);
+    if (wid == 0) {  // warp 0: exclusive scan of the warp aggregates in scan order
+        const int w = REV ? (kW - 1 - lane) : lane;  // lane q holds the q-th warp in scan order
+        Seg3 a = (lane < kW) ? s_w[w] : Seg3{0, 0.0, 0.0};
+#pragma unroll
+        for (int o = 1; o < kW; o <<= 1) {
+            Seg3 y;
+            y.f = __shfl_up_sync(0xffffffffu, a.f, o);
+            y.a = __shfl_up_sync(0xffffffffu, a.a, o);
+            y.b = __shfl_up_sync(0xffffffffu, a.b, o);
+            if (lane >= o) a = seg3_combine(y, a);
         }
-        *total = run;
+        Seg3 e;
+        e.f = __shfl_up_sync(0xffffffffu, a.f, 1);
+        e.a = __shfl_up_sync(0xffffffffu, a.a, 1);
+        e.b = __shfl_up_sync(0xffffffffu, a.b, 1);
+        if (lane < kW) s_w[w] = (lane == 0) ? Seg3{0, 0.0, 0.0} : e;
+        if (lane == kW - 1) *total = a;
     }
     __syncthreads();
     const Seg3 wpre = s_w[wid];
@@ -105,6 +106,41 @@ __device__ __forceinline__ Seg3 block_excl_scan3(Seg3 x, Seg3* s_w, Seg3* total)
     else out = first_warp ? ex : seg3_combine(wpre, ex);
     __syncthreads();
     return out;
+}
+
+// The CTA aggregates agg[q], q in [lo, hi), combined in ascending q (REV:
+// descending q, the suffix direction) by one warp: each lane combines a
+// contiguous run of them in scan order, its loads issued together, then the
+// lanes' results are combined in lane order by a tree (lane l takes lane
+// l + o, o = 1, 2, 4, ...).  Valid in lane 0.  The empty range gives {0, 0, 0}.
+template <bool REV>
+__device__ __forceinline__ Seg3 warp_agg_combine(const SegAgg* agg, int64_t lo, int64_t hi, bool two) {
+    const int lane = threadIdx.x & 31;
+    const int64_t n = hi - lo;
+    const int64_t m = (n + 31) / 32;
+    const int64_t s0 = lane * m, s1 = (s0 + m < n) ? s0 + m : n;
+    Seg3 run{0, 0.0, 0.0};
+    for (int64_t s = s0; s < s1; s += 4) {
+        Seg3 e[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (s + i < s1) {
+                const int64_t q = REV ? (hi - 1 - (s + i)) : (lo + s + i);
+                e[i] = Seg3{__ldcg(&agg[q].f), __ldcg(&agg[q].v0), two ? __ldcg(&agg[q].v1) : 0.0};
+            }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (s + i < s1) run = (s + i == s0) ? e[i] : seg3_combine(run, e[i]);
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        Seg3 y;
+        y.f = __shfl_down_sync(0xffffffffu, run.f, o);
+        y.a = __shfl_down_sync(0xffffffffu, run.a, o);
+        y.b = __shfl_down_sync(0xffffffffu, run.b, o);
+        if ((lane & (2 * o - 1)) == 0 && lane + o < 32) run = seg3_combine(run, y);
+    }
+    return run;
 }
 
 // Thread t's contiguous share of a CTA's range [lo, hi).
@@ -118,6 +154,12 @@ __device__ __forceinline__ void thread_share(int64_t lo, int64_t hi, int64_t& a,
 // combined, so a thread has kCh independent loads in flight instead of one
 // dependent load per group.
 constexpr int kCh = 4;
+
+// A nonzero step's column of at most kSoloMax entries is applied by one CTA
+// (rows, then group denominators, between block barriers), with the entries'
+// changes staged in shared memory.
+constexpr int kSoloPer = 4;
+constexpr int kSoloMax = 2 * kT * kSoloPer;
 
 // The forward (prefix) elements {gfirst, denominator} of groups [g, g + n).
 __device__ __forceinline__ void load_fwd(const CoxParams& P, int64_t g, int n, int (&f)[kCh], double (&v)[kCh]) {
@@ -151,7 +193,7 @@ __device__ __forceinline__ void load_rev(const CoxParams& P, int64_t g, int n, i
 // D, S1, S2 rebuilt from the group denominators (Cox).  Three phases separated
 // by grid barriers; false when a barrier wait ran out.
 __device__ bool cox_rebuild(const GroupSweepParams& Q, unsigned& epoch, int32_t* s_fail, Seg3* s_w,
-                            Seg3* s_tot, Seg3* s_carry) {
+                            Seg3* s_tot, Seg3* s_carry, unsigned long long* trc) {
     const CoxParams& P = Q.P;
     const int64_t G = gridDim.x, b = blockIdx.x;
     const int64_t g0 = P.N * b / G, g1 = P.N * (b + 1) / G;
@@ -177,14 +219,11 @@ __device__ bool cox_rebuild(const GroupSweepParams& Q, unsigned& epoch, int32_t*
         __stcg(&Q.agg[b].v0, s_tot->a);
     }
     if (!grid_barrier(Q.grid_bar, epoch, Q.wait_limit_ns, Q.st, s_fail)) return false;
+    if (trc) trc[4] = global_ns();
     // phase 2: carry-in from the CTAs before, D of the range; suffix aggregates
-    if (threadIdx.x == 0) {
-        Seg3 c{0, 0.0, 0.0};
-        for (int64_t q = 0; q < b; ++q) {
-            const Seg3 e{__ldcg(&Q.agg[q].f), __ldcg(&Q.agg[q].v0), 0.0};
-            c = (q == 0) ? e : seg3_combine(c, e);
-        }
-        *s_carry = c;
+    if (threadIdx.x < 32) {
+        const Seg3 c = warp_agg_combine<false>(Q.agg, 0, b, false);
+        if (threadIdx.x == 0) *s_carry = c;
     }
     __syncthreads();
     Seg3 pre = block_excl_scan3<false>(mine, s_w, s_tot);
@@ -224,14 +263,11 @@ __device__ bool cox_rebuild(const GroupSweepParams& Q, unsigned& epoch, int32_t*
         __stcg(&Q.agg[G + b].v1, s_tot->b);
     }
     if (!grid_barrier(Q.grid_bar, epoch, Q.wait_limit_ns, Q.st, s_fail)) return false;
+    if (trc) trc[5] = global_ns();
     // phase 3: carry-in from the CTAs after (suffix direction), S1 and S2 of the range
-    if (threadIdx.x == 0) {
-        Seg3 c{0, 0.0, 0.0};
-        for (int64_t q = G - 1; q > b; --q) {
-            const Seg3 e{__ldcg(&Q.agg[G + q].f), __ldcg(&Q.agg[G + q].v0), __ldcg(&Q.agg[G + q].v1)};
-            c = (q == G - 1) ? e : seg3_combine(c, e);
-        }
-        *s_carry = c;
+    if (threadIdx.x < 32) {
+        const Seg3 c = warp_agg_combine<true>(Q.agg + G, b + 1, G, true);
+        if (threadIdx.x == 0) *s_carry = c;
     }
     __syncthreads();
     Seg3 suf = block_excl_scan3<true>(mine, s_w, s_tot);
@@ -321,6 +357,8 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
     __shared__ int32_t s_first;
     __shared__ double s_delta, s_newbeta;
     __shared__ double s_pend_hd[kGroupBatchMax];  // CTA 0: bounds of the last decision
+    __shared__ double s_dd[kSoloMax];             // CTA 0: changes of a short column's entries
+    __shared__ int32_t s_ddg[kSoloMax];
 
     const CoxParams& P = Q.P;
     const int tid = threadIdx.x;
@@ -353,7 +391,7 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
         while (pos < Q.n_active) {
             const int nb = min(batch, Q.n_active - pos);
             // optional timestamps of the first nonzero steps (CTA 0): batch start, decided,
-            // rows updated, denominators updated, rebuilt, next
+            // rows updated, denominators updated, rebuild phases 1 and 2 done, rebuilt, next
             if (trc) trc[0] = global_ns();
             // gradients of the batch, one CTA per column; the two halves of gh
             // alternate by batch, so a CTA that is on to the next batch never
@@ -415,7 +453,7 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
                 batch = min(2 * batch, Q.batch_max);
                 continue;
             }
-            // ---- the nonzero step of column j: rows split over the CTAs
+            // ---- the nonzero step of column j: the rows, then the group denominators
             const int j = Q.cols[pos + first];
             const double delta = s_delta;
             ++n_updates;
@@ -425,52 +463,130 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
                 const bool has_vals = (f == F_SPARSE || f == F_DENSE);
                 const int64_t cb = P.col_ptr[j], vb = P.val_ptr[j];
                 const int64_t n = has_rows ? (P.col_ptr[j + 1] - cb) : P.K;
-                const int64_t p0 = n * b / G, p1 = n * (b + 1) / G;
-                for (int64_t p = p0 + tid; p < p1; p += blockDim.x) {
-                    const int64_t k = has_rows ? (int64_t)__ldg(P.rows + cb + p) : p;
-                    const double x = has_vals ? __ldg(P.vals + vb + p) : 1.0;
-                    const double2 xe = __ldcg(P.xbe + k);
+                // entry p: xBeta += delta x, e = exp, the (weighted) change of e and the group recorded
+                auto update_entry = [&](int64_t p, int64_t k, double x, double2 xe, double w, int32_t g) {
                     const double xb = xe.x + delta * x;
                     const double en = row_exp(xb, P.mixed);
                     __stcg(P.xbe + k, make_double2(xb, en));
-                    double dd;
-                    if (COX && P.weighted) {
-                        const double w = P.w[k];
-                        dd = w * en - w * xe.y;
-                    } else {
-                        dd = en - xe.y;
-                    }
+                    const double dd = (COX && P.weighted) ? w * en - w * xe.y : en - xe.y;
                     __stcg(Q.dd + p, dd);
-                    __stcg(Q.ddg + p, P.grp[k]);
-                }
-                if (!barrier()) return;
-                if (trc) trc[2] = global_ns();
+                    __stcg(Q.ddg + p, g);
+                };
                 // the first row of each group's run adds the run's changes in row order;
                 // rows dropped by a zero weight (group N) may sit inside a run
-                for (int64_t p = p0 + tid; p < p1; p += blockDim.x) {
-                    const int32_t g = __ldcg(Q.ddg + p);
-                    if (g == P.N) continue;
-                    int64_t q = p - 1;
-                    while (q >= 0 && __ldcg(Q.ddg + q) == P.N) --q;
-                    if (q >= 0 && __ldcg(Q.ddg + q) == g) continue;
-                    double d = __ldcg(P.denom + g);
-                    for (q = p; q < n; ++q) {
-                        const int32_t gq = __ldcg(Q.ddg + q);
-                        if (gq == P.N) continue;
-                        if (gq != g) break;
-                        d = d + __ldcg(Q.dd + q);
+                auto add_runs = [&](int64_t p0, int64_t p1) {
+                    for (int64_t p = p0 + tid; p < p1; p += blockDim.x) {
+                        const int32_t g = __ldcg(Q.ddg + p);
+                        if (g == P.N) continue;
+                        int64_t q = p - 1;
+                        while (q >= 0 && __ldcg(Q.ddg + q) == P.N) --q;
+                        if (q >= 0 && __ldcg(Q.ddg + q) == g) continue;
+                        double d = __ldcg(P.denom + g);
+                        for (q = p; q < n; ++q) {
+                            const int32_t gq = __ldcg(Q.ddg + q);
+                            if (gq == P.N) continue;
+                            if (gq != g) break;
+                            d = d + __ldcg(Q.dd + q);
+                        }
+                        __stcg(P.denom + g, d);
                     }
-                    __stcg(P.denom + g, d);
+                };
+                if (n <= (int64_t)kSoloMax) {
+                    // a short column: CTA 0 alone, its changes staged in shared memory, and
+                    // one grid barrier; kSoloPer entries per thread a round, their loads
+                    // issued together
+                    if (b == 0) {
+#pragma unroll 1
+                        for (int64_t r0 = 0; r0 < n; r0 += (int64_t)kT * kSoloPer) {
+                            int64_t kk[kSoloPer];
+                            double xv[kSoloPer];
+#pragma unroll
+                            for (int i = 0; i < kSoloPer; ++i) {
+                                const int64_t p = r0 + tid + (int64_t)i * kT;
+                                kk[i] = -1;
+                                xv[i] = 1.0;
+                                if (p < n) {
+                                    kk[i] = has_rows ? (int64_t)__ldg(P.rows + cb + p) : p;
+                                    if (has_vals) xv[i] = __ldg(P.vals + vb + p);
+                                }
+                            }
+                            double2 xe[kSoloPer];
+                            double wv[kSoloPer];
+                            int32_t gv[kSoloPer];
+#pragma unroll
+                            for (int i = 0; i < kSoloPer; ++i)
+                                if (kk[i] >= 0) {
+                                    xe[i] = __ldcg(P.xbe + kk[i]);
+                                    wv[i] = (COX && P.weighted) ? P.w[kk[i]] : 1.0;
+                                    gv[i] = P.grp[kk[i]];
+                                }
+#pragma unroll
+                            for (int i = 0; i < kSoloPer; ++i)
+                                if (kk[i] >= 0) {
+                                    const int64_t p = r0 + tid + (int64_t)i * kT;
+                                    const double xb = xe[i].x + delta * xv[i];
+                                    const double en = row_exp(xb, P.mixed);
+                                    __stcg(P.xbe + kk[i], make_double2(xb, en));
+                                    s_dd[p] = (COX && P.weighted) ? wv[i] * en - wv[i] * xe[i].y : en - xe[i].y;
+                                    s_ddg[p] = gv[i];
+                                }
+                        }
+                        __syncthreads();  // every entry's change is staged
+                        // run heads: the first entry of each group's run (dropped rows, group
+                        // N, may sit inside a run); their denominators are loaded together
+                        constexpr int R = kSoloMax / kT;
+                        int32_t hg[R];
+                        double hd0[R];
+#pragma unroll
+                        for (int i = 0; i < R; ++i) {
+                            const int p = tid + i * kT;
+                            hg[i] = -1;
+                            if (p < n) {
+                                const int32_t g = s_ddg[p];
+                                int q = p - 1;
+                                while (q >= 0 && s_ddg[q] == P.N) --q;
+                                if (g != P.N && (q < 0 || s_ddg[q] != g)) hg[i] = g;
+                            }
+                        }
+#pragma unroll
+                        for (int i = 0; i < R; ++i)
+                            if (hg[i] >= 0) hd0[i] = __ldcg(P.denom + hg[i]);
+#pragma unroll
+                        for (int i = 0; i < R; ++i)
+                            if (hg[i] >= 0) {
+                                double d = hd0[i];  // the run's changes added in row order
+                                for (int q = tid + i * kT; q < n; ++q) {
+                                    const int32_t gq = s_ddg[q];
+                                    if (gq == P.N) continue;
+                                    if (gq != hg[i]) break;
+                                    d = d + s_dd[q];
+                                }
+                                __stcg(P.denom + hg[i], d);
+                            }
+                    }
+                    if (!barrier()) return;
+                    if (trc) trc[2] = trc[3] = global_ns();
+                } else {
+                    // rows split over the CTAs
+                    const int64_t p0 = n * b / G, p1 = n * (b + 1) / G;
+                    for (int64_t p = p0 + tid; p < p1; p += blockDim.x) {
+                        const int64_t k = has_rows ? (int64_t)__ldg(P.rows + cb + p) : p;
+                        const double x = has_vals ? __ldg(P.vals + vb + p) : 1.0;
+                        update_entry(p, k, x, __ldcg(P.xbe + k), (COX && P.weighted) ? P.w[k] : 1.0, P.grp[k]);
+                    }
+                    if (!barrier()) return;
+                    if (trc) trc[2] = global_ns();
+                    add_runs(p0, p1);
+                    if (!barrier()) return;
+                    if (trc) trc[3] = global_ns();
                 }
-                if (!barrier()) return;
-                if (trc) trc[3] = global_ns();
             }
-            if (COX && !cox_rebuild(Q, epoch, &s_fail, s_w3, &s_tot, &s_carry)) return;
-            if (trc) trc[4] = global_ns();
+            if (COX && !cox_rebuild(Q, epoch, &s_fail, s_w3, &s_tot, &s_carry, trc)) return;
+            if (trc) trc[6] = global_ns();
             pos += first + 1;
             if (trc) {
-                trc[5] = global_ns();
-                trc += 6;
+                trc[7] = global_ns();
+                trc += kTraceStamps;
                 if (--trn <= 0) trc = nullptr;
             }
             batch = 32;

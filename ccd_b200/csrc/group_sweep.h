@@ -12,6 +12,7 @@
 namespace ccdb {
 
 constexpr int kGroupBatchMax = 1024;  // columns per speculative gradient batch
+constexpr int kTraceStamps = 8;       // timestamps per traced nonzero step
 
 // Aggregate of one CTA's share of a segmented scan (one or two channels).
 struct SegAgg {
@@ -45,7 +46,8 @@ struct GroupSweepParams {
     long long wait_limit_ns;
     int64_t* counters;      // [0]: nonzero steps, [1]: gradient batches (whole launch)
     // optional timestamps of the first trace_steps nonzero steps (profiling aid): per
-    // step, the start of its batch, decided, rows updated, denominators, rebuilt, done
+    // step (kTraceStamps), the start of its batch, decided, rows updated, denominators,
+    // rebuild phases 1 and 2 done, rebuilt, done
     unsigned long long* trace;
     int32_t trace_steps;
     int32_t pad;

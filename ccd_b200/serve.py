@@ -10,11 +10,13 @@ on the device.  A fit runs exactly as it would alone (same engine, same
 kernels, same arithmetic: its result does not depend on its neighbours); the
 server only decides when it starts.
 
-Each slot's context limits its persistent sweep grids to its share of the SMs
-(SM count / slots), so the slots' sweep kernels can all be resident at once
-and run side by side; logistic and Poisson fits use the dependency-level sweep
-(one persistent launch per findMode), grouped models (conditional logistic,
-Cox) their own engines.
+Each slot's context limits its sweep kernels to its share of the SMs (SM
+count / slots CTAs), so the slots' kernels can all be resident at once and run
+side by side.  Every model runs a whole findMode attempt in one launch:
+logistic and Poisson fits the cluster sweep over dependency levels (a thread
+block cluster of at most that many CTAs), grouped models (conditional
+logistic, Cox) the persistent group sweep (a cooperative grid of at most that
+many CTAs).
 
 The reference has no serving layer; this loop drives the same C ABI entry
 point a single fit uses (ccdb_fit_model: upload, findMode, coefficients back).
