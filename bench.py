@@ -80,7 +80,7 @@ def parse():
                     help="cv_grid: covariate columns (fewer for short profiling captures)")
     ap.add_argument("--fp64-check", type=int, default=4,
                     help="cv_grid, mixed: instances also fitted by the FP64 engine to report the error")
-    ap.add_argument("--strategy", choices=["auto", "levels", "speculative", "grid_levels"], default="auto",
+    ap.add_argument("--strategy", choices=["auto", "levels", "speculative", "grid_levels", "resident"], default="auto",
                     help="sweep strategy of the independent-row engine (CCDB_SWEEP_*)")
     ap.add_argument("--trace", default=None,
                     help="write a per-level timestamp trace of the last timed findMode's first "
@@ -702,7 +702,9 @@ def run_logistic_l1(args, world, rank, local, collect=False):
         "roofline": {"bound": "hbm", "achieved": total_bytes / ker_t / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": total_bytes / ker_t / 1e9 / peak, "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": total_bytes / attempts,
-                     "kernel": "cluster_sweep_kernel<LOGISTIC>", "traffic": None,
+                     "kernel": ("resident_sweep_kernel<LOGISTIC> (one CTA, row state in shared memory)"
+                                if args.strategy in ("auto", "resident") else
+                                f"{args.strategy} sweep of the independent-row engine"), "traffic": None,
                      "note": "1.1e5 entries per sweep: latency-bound, L2-resident"},
         "cpu_baseline": {"value": ref_fit["iterations"] * active * reps / t_ref, "unit": METRIC, "cores": 1,
                          "kind": kind, "time_to_converge_s": t_ref / reps,
@@ -1111,8 +1113,8 @@ def serve_config(args, stream) -> dict:
             "density": "uniform 0.001..0.02", "prior": "Laplace, variance 0.1",
             "slots": args.serve_slots, "hbm_budget_bytes": 150e9,
             "step": "replay of the whole stream; latency = completion - arrival",
-            "strategy": "logistic: dependency-level sweeps on the slot's share of the SMs; "
-                        "grouped models: their engines"}
+            "strategy": "logistic: the resident sweep (one CTA) when the rows fit it, else the "
+                        "cluster sweep on the slot's share of the SMs; grouped models: the group sweep"}
 
 
 def _serve_cpu_latencies(stream, n: int):
@@ -1190,7 +1192,7 @@ def run_serve_reference(args, world, rank):
 
 # ------------------------------------------------------------------ variants
 VARIANTS = ("kkt_l1", "mm_clr", "fisher_l1")
-STRATEGIES = {"auto": 0, "levels": 1, "speculative": 2, "grid_levels": 3}
+STRATEGIES = {"auto": 0, "levels": 1, "speculative": 2, "grid_levels": 3, "resident": 4}
 
 
 def variant_problem(name: str):

@@ -22,6 +22,7 @@
 #include "batch.h"
 #include "csr_host.h"
 #include "engine.h"
+#include "resident.h"
 
 namespace ccdb {
 
@@ -103,7 +104,8 @@ void Matrix::ensure_csr(cudaStream_t s) {
 Fit::~Fit() {
     for (void* p : {(void*)row, (void*)y, (void*)beta, (void*)hdelta, (void*)xjy, (void*)ptype,
                     (void*)pvar, (void*)st, (void*)grid_bar, (void*)red, (void*)xb_tmp, (void*)w,
-                    (void*)gh_parts, (void*)gh_out, (void*)d_batch_cols, (void*)d_batch_out})
+                    (void*)gh_parts, (void*)gh_out, (void*)d_batch_cols, (void*)d_batch_out,
+                    (void*)d_res_recs})
         ctx->release(p);
     release_schedule();
     if (group_engine()) cox_release();
@@ -465,6 +467,10 @@ void Fit::find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* 
         find_mode_group_sweep(a, flag, iters, obj, ms);
         return;
     }
+    if (use_resident(a)) {
+        find_mode_resident(a, flag, iters, obj, ms);
+        return;
+    }
     if (group_engine() || use_speculative(a)) {
         auto t0 = std::chrono::steady_clock::now();
         find_mode_batched(a, bound, flag, iters, obj);
@@ -665,6 +671,83 @@ void Fit::apply_step(int j, double delta) {
 // and per nonzero step) run only when asked for; every default path of the
 // independent-row models is the on-device cluster sweep.
 bool Fit::use_speculative(const ccdb_mode_args& a) const { return a.strategy == CCDB_SWEEP_SPECULATIVE; }
+
+// The resident sweep serves independent-row fits whose row state fits one
+// CTA's shared memory: chosen by CCDB_SWEEP_AUTO, required by
+// CCDB_SWEEP_RESIDENT (an error when the fit is too large for it).
+bool Fit::use_resident(const ccdb_mode_args& a) {
+    if (group_engine()) return false;
+    if (a.strategy != CCDB_SWEEP_AUTO && a.strategy != CCDB_SWEEP_RESIDENT) return false;
+    if (ctx->resident_rows < 0) {
+        int64_t r = 0;
+        check_cuda(resident_max_rows(model, &r), "resident capacity");
+        ctx->resident_rows = r;
+    }
+    if (K <= ctx->resident_rows) return true;
+    if (a.strategy == CCDB_SWEEP_RESIDENT)
+        throw Error(CCDB_ERR_UNSUPPORTED, "the fit has more rows than the resident sweep holds (" +
+                                              std::to_string(ctx->resident_rows) + ")");
+    return false;
+}
+
+void Fit::find_mode_resident(const ccdb_mode_args& a, int* flag, int* iters, double* obj, float* ms) {
+    std::vector<int32_t> cols;
+    for (int j = 0; j < J; ++j)
+        if (!fixed[j]) cols.push_back(j);
+    if (cols.empty()) {  // an empty cycle: the first check sees conv = 0
+        *obj = objective(a.convergence_type);
+        *flag = (*obj != *obj) ? R_ILLCONDITIONED
+                : (a.tolerance > 0 ? R_SUCCESS : (a.max_iterations == 1 ? R_MAX_ITERATIONS : R_SUCCESS));
+        *iters = 1;
+        *ms = 0.f;
+        return;
+    }
+    // the column records in visiting order
+    std::vector<ResCol> recs(cols.size());
+    for (size_t q = 0; q < cols.size(); ++q) {
+        const int j = cols[q];
+        const uint8_t f = m->fmt[j];
+        const bool has_rows = (f == F_SPARSE || f == F_INDICATOR);
+        ResCol& r = recs[q];
+        r.j = j;
+        r.flags = (has_rows ? 1 : 0) | ((f == F_SPARSE || f == F_DENSE) ? 2 : 0) |
+                  ((f == F_INDICATOR || f == F_INTERCEPT) ? 4 : 0);
+        r.n = has_rows ? m->col_start[j + 1] - m->col_start[j] : K;
+        r.cb = m->col_start[j];
+        r.vb = m->val_start[j];
+    }
+    if (d_res_cap < (int32_t)recs.size()) {
+        ctx->release(d_res_recs);
+        d_res_recs = static_cast<ResCol*>(ctx->alloc(sizeof(ResCol) * recs.size()));
+        d_res_cap = (int32_t)recs.size();
+    }
+    check_cuda(cudaMemcpyAsync(d_res_recs, recs.data(), sizeof(ResCol) * recs.size(), cudaMemcpyHostToDevice,
+                               stream), "column records");
+    DevStatus zero{};
+    zero.flag = R_FAIL;
+    check_cuda(cudaMemcpyAsync(st, &zero, sizeof(zero), cudaMemcpyHostToDevice, stream), "status");
+    ResidentParams R{};
+    R.P = params();
+    R.P.conv = a.convergence_type;
+    R.P.tol = a.tolerance;
+    R.P.max_iter = a.max_iterations;
+    R.recs = d_res_recs;
+    R.n_active = (int32_t)recs.size();
+    R.weighted = weighted ? 1 : 0;
+    check_cuda(cudaEventRecord(ev0, stream), "event");
+    check_cuda(launch_resident_sweep(R, stream), "resident sweep launch");
+    ++launches;
+    check_cuda(cudaEventRecord(ev1, stream), "event");
+    DevStatus out{};
+    check_cuda(cudaMemcpyAsync(&out, st, sizeof(out), cudaMemcpyDeviceToHost, stream), "status");
+    check_cuda(cudaStreamSynchronize(stream), "resident sweep");
+    check_cuda(cudaEventElapsedTime(ms, ev0, ev1), "elapsed");
+    *flag = out.flag;
+    *iters = out.iterations;
+    *obj = out.objective;
+    nz_steps += (int64_t)out.nonzero_steps;
+    beta_dirty_host = true;
+}
 
 void Fit::find_mode(const ccdb_mode_args& a, double* beta_inout, ccdb_fit_result* res) {
     if (!a.prior_type || !a.prior_var) throw Error(CCDB_ERR_INVALID, "prior arrays are required");

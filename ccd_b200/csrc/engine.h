@@ -16,6 +16,7 @@
 #include "../../include/ccdb.h"
 #include "cox.h"
 #include "indep.h"
+#include "resident.h"
 #include "schedule.h"
 #include "step.h"
 
@@ -35,6 +36,7 @@ struct Context {
     int n_sm = 0;
     int max_ctas = 0;  // persistent sweep grids: at most this many CTAs (0: n_sm)
     int sweep_cluster = -1;  // largest resident cluster of the cluster sweep (-1: not queried)
+    int64_t resident_rows = -1;  // most rows of a shared-memory resident sweep (-1: not queried)
     size_t budget = 0;
     size_t in_use = 0;
     cudaStream_t stream = nullptr;
@@ -198,6 +200,11 @@ struct Fit {
     void gh_batch(const int32_t* cols, int n, double2* out);
     void apply_step(int j, double delta);
     bool use_speculative(const ccdb_mode_args& a) const;
+    // the single-CTA sweep with the row state in shared memory (resident.cu)
+    bool use_resident(const ccdb_mode_args& a);
+    void find_mode_resident(const ccdb_mode_args& a, int* flag, int* iters, double* obj, float* ms);
+    ResCol* d_res_recs = nullptr;  // its active columns' records in visiting order
+    int32_t d_res_cap = 0;
     int32_t* d_batch_cols = nullptr;  // independent-row models
     double2* d_batch_out = nullptr;
     bool is_cox() const { return model == M_COX; }

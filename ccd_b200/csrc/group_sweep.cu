@@ -155,11 +155,19 @@ __device__ __forceinline__ void thread_share(int64_t lo, int64_t hi, int64_t& a,
 // dependent load per group.
 constexpr int kCh = 4;
 
-// A nonzero step's column of at most kSoloMax entries is applied by one CTA
-// (rows, then group denominators, between block barriers), with the entries'
-// changes staged in shared memory.
-constexpr int kSoloPer = 4;
-constexpr int kSoloMax = 2 * kT * kSoloPer;
+
+// Hint the cache lines of elements [a, b) of an array into L1: a thread's
+// share of a phase is contiguous, so its lines are all requested at once and
+// the phase's loads hit L1 instead of waiting on L2 a chunk at a time.  The
+// arrays are read with plain loads after a grid barrier, whose acquire orders
+// them after every CTA's writes.
+template <typename T>
+__device__ __forceinline__ void prefetch_l1(const T* p, int64_t a, int64_t b) {
+    if (a >= b) return;
+    const uintptr_t lo = reinterpret_cast<uintptr_t>(p + a) & ~(uintptr_t)127;
+    const uintptr_t hi = reinterpret_cast<uintptr_t>(p + b);
+    for (uintptr_t q = lo; q < hi; q += 128) asm volatile("prefetch.global.L1 [%0];" ::"l"(q));
+}
 
 // The forward (prefix) elements {gfirst, denominator} of groups [g, g + n).
 __device__ __forceinline__ void load_fwd(const CoxParams& P, int64_t g, int n, int (&f)[kCh], double (&v)[kCh]) {
@@ -167,7 +175,7 @@ __device__ __forceinline__ void load_fwd(const CoxParams& P, int64_t g, int n, i
     for (int i = 0; i < kCh; ++i)
         if (i < n) {
             f[i] = P.gfirst[g + i];
-            v[i] = __ldcg(P.denom + g + i);
+            v[i] = P.denom[g + i];
         }
 }
 
@@ -179,7 +187,7 @@ __device__ __forceinline__ void load_rev(const CoxParams& P, int64_t g, int n, i
     for (int i = 0; i < kCh; ++i)
         if (i < n) {
             f[i] = P.glast[g + i];
-            D[i] = __ldcg(P.D + g + i);
+            D[i] = P.D[g + i];
             ne[i] = P.nEv[g + i];
         }
 #pragma unroll
@@ -202,6 +210,8 @@ __device__ bool cox_rebuild(const GroupSweepParams& Q, unsigned& epoch, int32_t*
     int fl[kCh];
     double va[kCh], vb[kCh];
     // phase 1: aggregate of the CTA's range (prefix direction)
+    prefetch_l1(P.gfirst, t0, t1);
+    prefetch_l1(P.denom, t0, t1);
     Seg3 mine{0, 0.0, 0.0};
     for (int64_t g = t0; g < t1; g += kCh) {
         const int n = (int)(int)(t1 - g < kCh ? t1 - g : kCh);
@@ -231,27 +241,31 @@ __device__ bool cox_rebuild(const GroupSweepParams& Q, unsigned& epoch, int32_t*
         // running value entering this thread's first group
         Seg3 run = (b == 0) ? pre : (threadIdx.x == 0 ? *s_carry : seg3_combine(*s_carry, pre));
         const bool has_run = (b > 0) || (threadIdx.x > 0);
+        prefetch_l1(P.glast, t0, t1);
+        prefetch_l1(P.nEv, t0, t1);
+        // the suffix aggregate of the share from the D just computed: the element of
+        // group g is the highest of [t0, g], so it is combined in front
+        Seg3 rs{0, 0.0, 0.0};
         for (int64_t g = t0; g < t1; g += kCh) {
             const int n = (int)(int)(t1 - g < kCh ? t1 - g : kCh);
             load_fwd(P, g, n, fl, va);
+            int fr[kCh];
+            double ne[kCh];
+#pragma unroll
+            for (int i = 0; i < kCh; ++i)
+                if (i < n) {
+                    fr[i] = P.glast[g + i];
+                    ne[i] = P.nEv[g + i];
+                }
 #pragma unroll
             for (int i = 0; i < kCh; ++i)
                 if (i < n) {
                     const Seg3 e{fl[i], va[i], 0.0};
                     run = (!has_run && g + i == t0) ? e : seg3_combine(run, e);
                     __stcg(P.D + g + i, run.a);
-                }
-        }
-        Seg3 rs{0, 0.0, 0.0};  // suffix aggregate of the thread's share, built from the top
-        for (int64_t hi = t1; hi > t0; hi -= kCh) {
-            const int64_t g = (hi - kCh > t0 ? hi - kCh : t0);
-            const int n = (int)(hi - g);
-            load_rev(P, g, n, fl, va, vb);
-#pragma unroll
-            for (int i = kCh - 1; i >= 0; --i)
-                if (i < n) {
-                    const Seg3 e{fl[i], va[i], vb[i]};
-                    rs = (g + i == t1 - 1) ? e : seg3_combine(rs, e);
+                    const double D = run.a;
+                    const Seg3 r{fr[i], ne[i] / D, ne[i] / (D * D)};
+                    rs = (g + i == t0) ? r : seg3_combine(r, rs);
                 }
         }
         mine = rs;
@@ -265,6 +279,7 @@ __device__ bool cox_rebuild(const GroupSweepParams& Q, unsigned& epoch, int32_t*
     if (!grid_barrier(Q.grid_bar, epoch, Q.wait_limit_ns, Q.st, s_fail)) return false;
     if (trc) trc[5] = global_ns();
     // phase 3: carry-in from the CTAs after (suffix direction), S1 and S2 of the range
+    prefetch_l1(P.D, t0, t1);
     if (threadIdx.x < 32) {
         const Seg3 c = warp_agg_combine<true>(Q.agg + G, b + 1, G, true);
         if (threadIdx.x == 0) *s_carry = c;
@@ -357,8 +372,6 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
     __shared__ int32_t s_first;
     __shared__ double s_delta, s_newbeta;
     __shared__ double s_pend_hd[kGroupBatchMax];  // CTA 0: bounds of the last decision
-    __shared__ double s_dd[kSoloMax];             // CTA 0: changes of a short column's entries
-    __shared__ int32_t s_ddg[kSoloMax];
 
     const CoxParams& P = Q.P;
     const int tid = threadIdx.x;
@@ -491,95 +504,18 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
                         __stcg(P.denom + g, d);
                     }
                 };
-                if (n <= (int64_t)kSoloMax) {
-                    // a short column: CTA 0 alone, its changes staged in shared memory, and
-                    // one grid barrier; kSoloPer entries per thread a round, their loads
-                    // issued together
-                    if (b == 0) {
-#pragma unroll 1
-                        for (int64_t r0 = 0; r0 < n; r0 += (int64_t)kT * kSoloPer) {
-                            int64_t kk[kSoloPer];
-                            double xv[kSoloPer];
-#pragma unroll
-                            for (int i = 0; i < kSoloPer; ++i) {
-                                const int64_t p = r0 + tid + (int64_t)i * kT;
-                                kk[i] = -1;
-                                xv[i] = 1.0;
-                                if (p < n) {
-                                    kk[i] = has_rows ? (int64_t)__ldg(P.rows + cb + p) : p;
-                                    if (has_vals) xv[i] = __ldg(P.vals + vb + p);
-                                }
-                            }
-                            double2 xe[kSoloPer];
-                            double wv[kSoloPer];
-                            int32_t gv[kSoloPer];
-#pragma unroll
-                            for (int i = 0; i < kSoloPer; ++i)
-                                if (kk[i] >= 0) {
-                                    xe[i] = __ldcg(P.xbe + kk[i]);
-                                    wv[i] = (COX && P.weighted) ? P.w[kk[i]] : 1.0;
-                                    gv[i] = P.grp[kk[i]];
-                                }
-#pragma unroll
-                            for (int i = 0; i < kSoloPer; ++i)
-                                if (kk[i] >= 0) {
-                                    const int64_t p = r0 + tid + (int64_t)i * kT;
-                                    const double xb = xe[i].x + delta * xv[i];
-                                    const double en = row_exp(xb, P.mixed);
-                                    __stcg(P.xbe + kk[i], make_double2(xb, en));
-                                    s_dd[p] = (COX && P.weighted) ? wv[i] * en - wv[i] * xe[i].y : en - xe[i].y;
-                                    s_ddg[p] = gv[i];
-                                }
-                        }
-                        __syncthreads();  // every entry's change is staged
-                        // run heads: the first entry of each group's run (dropped rows, group
-                        // N, may sit inside a run); their denominators are loaded together
-                        constexpr int R = kSoloMax / kT;
-                        int32_t hg[R];
-                        double hd0[R];
-#pragma unroll
-                        for (int i = 0; i < R; ++i) {
-                            const int p = tid + i * kT;
-                            hg[i] = -1;
-                            if (p < n) {
-                                const int32_t g = s_ddg[p];
-                                int q = p - 1;
-                                while (q >= 0 && s_ddg[q] == P.N) --q;
-                                if (g != P.N && (q < 0 || s_ddg[q] != g)) hg[i] = g;
-                            }
-                        }
-#pragma unroll
-                        for (int i = 0; i < R; ++i)
-                            if (hg[i] >= 0) hd0[i] = __ldcg(P.denom + hg[i]);
-#pragma unroll
-                        for (int i = 0; i < R; ++i)
-                            if (hg[i] >= 0) {
-                                double d = hd0[i];  // the run's changes added in row order
-                                for (int q = tid + i * kT; q < n; ++q) {
-                                    const int32_t gq = s_ddg[q];
-                                    if (gq == P.N) continue;
-                                    if (gq != hg[i]) break;
-                                    d = d + s_dd[q];
-                                }
-                                __stcg(P.denom + hg[i], d);
-                            }
-                    }
-                    if (!barrier()) return;
-                    if (trc) trc[2] = trc[3] = global_ns();
-                } else {
-                    // rows split over the CTAs
-                    const int64_t p0 = n * b / G, p1 = n * (b + 1) / G;
-                    for (int64_t p = p0 + tid; p < p1; p += blockDim.x) {
-                        const int64_t k = has_rows ? (int64_t)__ldg(P.rows + cb + p) : p;
-                        const double x = has_vals ? __ldg(P.vals + vb + p) : 1.0;
-                        update_entry(p, k, x, __ldcg(P.xbe + k), (COX && P.weighted) ? P.w[k] : 1.0, P.grp[k]);
-                    }
-                    if (!barrier()) return;
-                    if (trc) trc[2] = global_ns();
-                    add_runs(p0, p1);
-                    if (!barrier()) return;
-                    if (trc) trc[3] = global_ns();
+                // rows split over the CTAs
+                const int64_t p0 = n * b / G, p1 = n * (b + 1) / G;
+                for (int64_t p = p0 + tid; p < p1; p += blockDim.x) {
+                    const int64_t k = has_rows ? (int64_t)__ldg(P.rows + cb + p) : p;
+                    const double x = has_vals ? __ldg(P.vals + vb + p) : 1.0;
+                    update_entry(p, k, x, __ldcg(P.xbe + k), (COX && P.weighted) ? P.w[k] : 1.0, P.grp[k]);
                 }
+                if (!barrier()) return;
+                if (trc) trc[2] = global_ns();
+                add_runs(p0, p1);
+                if (!barrier()) return;
+                if (trc) trc[3] = global_ns();
             }
             if (COX && !cox_rebuild(Q, epoch, &s_fail, s_w3, &s_tot, &s_carry, trc)) return;
             if (trc) trc[6] = global_ns();

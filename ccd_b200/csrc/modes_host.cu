@@ -189,12 +189,13 @@ void Fit::kkt_swindle(const ccdb_mode_args& a, double bound, int* flag, int* ite
         if (j == intercept || ptype_h[j] != 1) active.push_back({j, 0.0, true});
         else inactive.push_back({j, 0.0, false});
     }
-    // The active set's findMode runs the fused dependency-level sweep unless the
-    // caller chose a strategy: its columns are the ones that violated their KKT
-    // condition, so most of them move, and a fixed set that changes each pass
-    // costs one schedule build instead of a launch per nonzero step.
+    // The active set's findMode runs the resident sweep when the rows fit it,
+    // else the fused dependency-level sweep, unless the caller chose a strategy:
+    // its columns are the ones that violated their KKT condition, so most of them
+    // move, and a fixed set that changes each pass costs one schedule build
+    // instead of a launch per nonzero step.
     ccdb_mode_args inner = a;
-    if (inner.strategy == CCDB_SWEEP_AUTO) inner.strategy = CCDB_SWEEP_LEVELS;
+    if (inner.strategy == CCDB_SWEEP_AUTO && !use_resident(inner)) inner.strategy = CCDB_SWEEP_LEVELS;
     auto lambda = [&](int j) { return std::sqrt(2.0 / pvar_h[j]); };
     auto meets = [&](const Score& s) { return s.score <= lambda(s.idx); };
     try {

@@ -1,0 +1,35 @@
+// resident.h -- the single-CTA sweep of small independent-row fits
+// (resident.cu): the row state lives in shared memory for the whole findMode.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "indep.h"
+
+namespace ccdb {
+
+// One active column in visiting order: its index, format flags (bit 0: row
+// ids, bit 1: values, bit 2: indicator or intercept), entry count and the
+// offsets of its row ids and values.
+struct ResCol {
+    int32_t j;
+    int32_t flags;
+    int64_t n;
+    int64_t cb;
+    int64_t vb;
+};
+
+struct ResidentParams {
+    IndepParams P;         // matrix, row and column state, convergence (no schedule)
+    const ResCol* recs;    // the active columns in visiting order
+    int32_t n_active;
+    int32_t weighted;      // 0: every row weight is 1.0 and is not read
+};
+
+int resident_threads();
+// the most rows whose state fits the kernel's shared memory on the current device
+cudaError_t resident_max_rows(int model, int64_t* rows);
+cudaError_t launch_resident_sweep(const ResidentParams& R, cudaStream_t stream);
+
+}  // namespace ccdb

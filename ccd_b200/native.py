@@ -26,7 +26,7 @@ OK = 0
 ERR_INVALID, ERR_CUDA, ERR_UNSUPPORTED, ERR_BUDGET, ERR_TIMEOUT = -1, -2, -3, -4, -5
 ALGORITHM_CCD, ALGORITHM_MM = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
-SWEEP_AUTO, SWEEP_LEVELS, SWEEP_SPECULATIVE, SWEEP_GRID_LEVELS = 0, 1, 2, 3
+SWEEP_AUTO, SWEEP_LEVELS, SWEEP_SPECULATIVE, SWEEP_GRID_LEVELS, SWEEP_RESIDENT = 0, 1, 2, 3, 4
 
 
 class CcdbError(RuntimeError):

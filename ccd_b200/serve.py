@@ -13,10 +13,11 @@ server only decides when it starts.
 Each slot's context limits its sweep kernels to its share of the SMs (SM
 count / slots CTAs), so the slots' kernels can all be resident at once and run
 side by side.  Every model runs a whole findMode attempt in one launch:
-logistic and Poisson fits the cluster sweep over dependency levels (a thread
-block cluster of at most that many CTAs), grouped models (conditional
-logistic, Cox) the persistent group sweep (a cooperative grid of at most that
-many CTAs).
+logistic and Poisson fits whose row state fits one CTA's shared memory the
+resident sweep (one CTA), larger ones the cluster sweep over dependency
+levels (a thread block cluster of at most that many CTAs), grouped models
+(conditional logistic, Cox) the persistent group sweep (a cooperative grid of
+at most that many CTAs).
 
 The reference has no serving layer; this loop drives the same C ABI entry
 point a single fit uses (ccdb_fit_model: upload, findMode, coefficients back).
@@ -38,7 +39,7 @@ from .data import CyclopsData
 class Request:
     rid: int
     data: CyclopsData
-    args: object = None          # native.ModeFindingArguments (None: defaults, speculative sweeps)
+    args: object = None          # native.ModeFindingArguments (None: the defaults)
     bytes: int = 0               # device-memory estimate used for admission
     arrival: float = 0.0         # time.perf_counter() at submission
 
@@ -165,7 +166,7 @@ class Server:
         if not hasattr(local, "ctx"):
             local.ctx = native.Context(self.device)
             local.ctx.set_max_ctas(max(1, local.ctx.sm_count // self.n_slots))
-        args = req.args or native.ModeFindingArguments(strategy=native.SWEEP_LEVELS)
+        args = req.args or native.ModeFindingArguments()
         r = native.fit_model(local.ctx, req.data, args)
         return r.beta, r.return_flag, r.iterations, r.log_likelihood
 

@@ -176,9 +176,13 @@ typedef struct {
     int32_t max_bound_count;   /* default 5 */
     int32_t per_coordinate;    /* 0: on-device mode finding (default); 1: host loop over
                                   the per-coordinate calls above (the reference's call pattern) */
-    int32_t strategy;          /* sweep strategy.  Logistic/Poisson: CCDB_SWEEP_AUTO and
-                                  _LEVELS run the cluster sweep (one launch per findMode over
-                                  dependency levels), _GRID_LEVELS the grid-wide level sweep,
+    int32_t strategy;          /* sweep strategy.  Logistic/Poisson: CCDB_SWEEP_AUTO runs
+                                  the resident sweep (one CTA, the row state in shared
+                                  memory) when the fit's rows fit it, else the cluster
+                                  sweep; _RESIDENT requires the former (an error for a fit
+                                  too large for it); _LEVELS runs the cluster sweep (one
+                                  launch per findMode over dependency levels),
+                                  _GRID_LEVELS the grid-wide level sweep,
                                   _SPECULATIVE host-driven batches of gradients that restart
                                   after each nonzero step.  Cox and conditional models: one
                                   persistent launch per findMode of device-driven speculative
@@ -201,6 +205,7 @@ typedef struct {
 #define CCDB_SWEEP_LEVELS 1        /* one thread-block cluster, levels ordered by cluster barriers */
 #define CCDB_SWEEP_SPECULATIVE 2
 #define CCDB_SWEEP_GRID_LEVELS 3   /* one CTA per SM, levels ordered by global counters */
+#define CCDB_SWEEP_RESIDENT 4      /* one CTA, the row state in shared memory (small fits) */
 
 typedef struct {
     int32_t return_flag;        /* UpdateReturnFlags */

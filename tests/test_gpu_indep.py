@@ -52,14 +52,14 @@ def test_per_coordinate_gradient_hessian(gpu_ctx, oracle_engine, model, kw):
 
 @pytest.mark.parametrize("model,kw", CASES)
 @pytest.mark.parametrize("conv", [GRADIENT, MITTAL, LANGE])
-@pytest.mark.parametrize("mode", ["levels", "grid_levels", "speculative", "per_coordinate"])
+@pytest.mark.parametrize("mode", ["levels", "grid_levels", "speculative", "resident", "per_coordinate"])
 def test_find_mode_matches_oracle(gpu_ctx, oracle_engine, model, kw, conv, mode):
     d = synthetic.small(model, **kw)
     want = oracle_engine(d).fit(conv, 1e-6)
     m = native.Matrix(gpu_ctx, d)
     f = native.Fit(gpu_ctx, m, d)
     strategy = {"levels": native.SWEEP_LEVELS, "grid_levels": native.SWEEP_GRID_LEVELS,
-                "speculative": native.SWEEP_SPECULATIVE}.get(mode, 0)
+                "speculative": native.SWEEP_SPECULATIVE, "resident": native.SWEEP_RESIDENT}.get(mode, 0)
     got = f.find_mode(native.ModeFindingArguments(convergence_type=conv, strategy=strategy,
                                                   per_coordinate=(mode == "per_coordinate")))
     assert got.return_flag == want["flag"]
@@ -68,7 +68,7 @@ def test_find_mode_matches_oracle(gpu_ctx, oracle_engine, model, kw, conv, mode)
     assert abs(got.log_likelihood - want["loglik"]) <= LL_TOL * abs(want["loglik"])
 
 
-@pytest.mark.parametrize("strategy", [1, 2, 3])
+@pytest.mark.parametrize("strategy", [1, 2, 3, 4])
 def test_logistic_l1_benchmark_problem(gpu_ctx, oracle_engine, strategy):
     """10,000 x 1,000 L1 logistic, MITTAL 1e-6, the reference's CPU-runnable case."""
     d = synthetic.logistic_l1(seed=1)
