@@ -74,6 +74,8 @@ def parse():
                     help="cv_grid: instances also fitted one at a time by the plain solver")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed",
                     help="cv_grid: the mixed-precision lockstep engine (default) or the FP64 one")
+    ap.add_argument("--cluster", type=int, default=0,
+                    help="cv_grid, mixed, with --group: CTAs per group (0: the engine's choice)")
     ap.add_argument("--group", type=int, default=0,
                     help="cv_grid, mixed: instances per lockstep group (0: the engine's choice)")
     ap.add_argument("--cv-columns", type=int, default=20_000,
@@ -834,7 +836,7 @@ def run_cv(args, world, rank, local, collect=False):
     margs = native.ModeFindingArguments(convergence_type=GRADIENT, tolerance=1e-6,
                                         max_iterations=args.max_sweeps)
     tuned = None
-    group, cluster = args.group, 0
+    group, cluster = args.group, args.cluster
     if mixed and not args.group:
         # the launch shape from one measured sweep per candidate (ccd_b200.tune), outside the timing
         from ccd_b200 import tune

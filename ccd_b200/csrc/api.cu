@@ -43,15 +43,17 @@ void* Context::alloc(size_t bytes) {
                                              " bytes exceeds the HBM budget");
         in_use += bytes;
     }
-    // stream-ordered: allocation and release are ordered with the context's own
-    // work and do not synchronize the device, so fits of other contexts (other
-    // streams) keep running through them
+    // stream-ordered from the context's own pool: allocation and release are
+    // ordered with the context's own work and never wait on another context's
+    // stream (the device's shared pool may reuse a block another stream freed by
+    // making this stream wait for that one), so fits of other contexts keep
+    // running through them
     void* p = nullptr;
-    cudaError_t e = cudaMallocAsync(&p, bytes, stream);
+    cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, pool, stream);
     if (e != cudaSuccess) {
         std::lock_guard<std::mutex> g(mu);
         in_use -= bytes;
-        check_cuda(e, "cudaMallocAsync");
+        check_cuda(e, "cudaMallocFromPoolAsync");
     }
     std::lock_guard<std::mutex> g(mu);
     sizes[p] = bytes;
@@ -67,6 +69,12 @@ void Context::release(void* p) {
         in_use -= it->second;
         sizes.erase(it);
     }
+}
+
+cudaError_t Context::wait() {
+    if (!blocking_wait) return cudaStreamSynchronize(stream);
+    cudaError_t e = cudaEventRecord(ev_wait, stream);
+    return e == cudaSuccess ? cudaEventSynchronize(ev_wait) : e;
 }
 
 template <typename T>
@@ -96,7 +104,7 @@ void Matrix::ensure_csr(cudaStream_t s) {
     d_row_ptr = upload(ctx, h.row_ptr.data(), h.row_ptr.size(), s);
     d_csr_col = upload(ctx, h.col.data(), h.col.size(), s);
     d_csr_val = upload(ctx, h.val.data(), h.val.size(), s);
-    check_cuda(cudaStreamSynchronize(s), "csr upload");
+    check_cuda(ctx->wait(), "csr upload");
 }
 
 // ------------------------------------------------------------------ Fit
@@ -189,7 +197,7 @@ void Fit::apply_weights() {
             ll_fixed += weighted ? t * wh[i] : t;
         }
     }
-    check_cuda(cudaStreamSynchronize(stream), "weights sync");
+    check_cuda(ctx->wait(), "weights sync");
     valid_weights = true;
     suff_known = false;
 }
@@ -248,7 +256,7 @@ void Fit::upload_beta() {
 void Fit::download_beta() {
     check_cuda(cudaMemcpyAsync(beta_h.data(), beta, sizeof(double) * J, cudaMemcpyDeviceToHost, stream),
                "beta download");
-    check_cuda(cudaStreamSynchronize(stream), "beta sync");
+    check_cuda(ctx->wait(), "beta sync");
 }
 
 int Fit::sweep_kind(const ccdb_mode_args& a) const {
@@ -291,7 +299,7 @@ void Fit::ensure_schedule(int kind) {
         s->cta_seg = upload(ctx, s->host.cta_seg.data(), s->host.cta_seg.size(), stream);
         s->tasks = upload(ctx, s->host.tasks.data(), s->host.tasks.size(), stream);
         s->level_split = upload(ctx, s->host.level_split.data(), s->host.level_split.size(), stream);
-        check_cuda(cudaStreamSynchronize(stream), "schedule upload");
+        check_cuda(ctx->wait(), "schedule upload");
         sched = std::move(s);
         return;
     }
@@ -319,7 +327,7 @@ void Fit::ensure_schedule(int kind) {
     s->level_done = static_cast<unsigned*>(ctx->alloc(sizeof(unsigned) * std::max(1, s->host.n_levels)));
     s->col_arrive = static_cast<unsigned*>(ctx->alloc(sizeof(unsigned) * std::max(1, J)));
     s->partials = static_cast<double2*>(ctx->alloc(sizeof(double2) * std::max(1, s->host.n_partials)));
-    check_cuda(cudaStreamSynchronize(stream), "schedule upload");
+    check_cuda(ctx->wait(), "schedule upload");
     sched = std::move(s);
 }
 
@@ -338,7 +346,7 @@ void Fit::objective_terms(double* out4) {
     std::vector<double2> parts(2 * nb);
     check_cuda(cudaMemcpyAsync(parts.data(), red, sizeof(double2) * 2 * nb, cudaMemcpyDeviceToHost, stream),
                "objective copy");
-    check_cuda(cudaStreamSynchronize(stream), "objective sync");
+    check_cuda(ctx->wait(), "objective sync");
     double t[4] = {0, 0, 0, 0};
     for (int c = 0; c < nb; ++c) {
         t[0] += parts[2 * c].x;
@@ -379,7 +387,7 @@ void Fit::gradient_hessian(int j, double* g, double* h) {
     launches += 2;
     double2 r;
     check_cuda(cudaMemcpyAsync(&r, gh_out, sizeof(double2), cudaMemcpyDeviceToHost, stream), "gh copy");
-    check_cuda(cudaStreamSynchronize(stream), "gh sync");
+    check_cuda(ctx->wait(), "gh sync");
     *g = r.x;
     *h = r.y;
 }
@@ -391,13 +399,13 @@ void Fit::update_xbeta(int j, double delta) {
                "beta j");
     if (group_engine()) {
         cox_update(j, delta);
-        check_cuda(cudaStreamSynchronize(stream), "update sync");
+        check_cuda(ctx->wait(), "update sync");
         return;
     }
     IndepParams P = params();
     check_cuda(launch_indep_update(P, j, m->fmt[j], m->entries(j), delta, stream), "update");
     launches += m->entries(j) > 0 ? 1 : 0;
-    check_cuda(cudaStreamSynchronize(stream), "update sync");
+    check_cuda(ctx->wait(), "update sync");
 }
 
 // findMode (CyclicCoordinateDescent.cpp:909-1216), CCD algorithm.
@@ -525,7 +533,7 @@ void Fit::find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* 
     check_cuda(cudaEventRecord(ev1, stream), "event");
     DevStatus out{};
     check_cuda(cudaMemcpyAsync(&out, st, sizeof(out), cudaMemcpyDeviceToHost, stream), "status");
-    check_cuda(cudaStreamSynchronize(stream), "sweep");
+    check_cuda(ctx->wait(), "sweep");
     check_cuda(cudaEventElapsedTime(ms, ev0, ev1), "elapsed");
     if (d_trace && kind == kSchedCluster) {
         const size_t n = 4 * (size_t)sched->host.n_levels * sched->cluster;
@@ -633,7 +641,7 @@ void Fit::find_mode_batched(const ccdb_mode_args& a, double bound, int* flag, in
     }
     check_cuda(cudaMemcpyAsync(hdelta, hd.data(), sizeof(double) * J, cudaMemcpyHostToDevice, stream),
                "bounds");
-    check_cuda(cudaStreamSynchronize(stream), "batched sync");
+    check_cuda(ctx->wait(), "batched sync");
     *iters = iteration;
     *obj = last;
 }
@@ -654,7 +662,7 @@ void Fit::gh_batch(const int32_t* cols, int n, double2* out) {
     ++launches;
     check_cuda(cudaMemcpyAsync(out, d_batch_out, sizeof(double2) * n, cudaMemcpyDeviceToHost, stream),
                "gh copy");
-    check_cuda(cudaStreamSynchronize(stream), "gh sync");
+    check_cuda(ctx->wait(), "gh sync");
 }
 
 void Fit::apply_step(int j, double delta) {
@@ -734,14 +742,33 @@ void Fit::find_mode_resident(const ccdb_mode_args& a, int* flag, int* iters, dou
     R.recs = d_res_recs;
     R.n_active = (int32_t)recs.size();
     R.weighted = weighted ? 1 : 0;
+    // CCDB_TRACE_FILE=<path>: SM-clock stamps of the first batches (profiling aid; off by default)
+    const char* trace_path = std::getenv("CCDB_TRACE_FILE");
+    const int trace_n = 4096;
+    if (trace_path) {
+        R.trace = static_cast<long long*>(ctx->alloc(sizeof(long long) * kResidentTraceWords * trace_n));
+        check_cuda(cudaMemsetAsync(R.trace, 0, sizeof(long long) * kResidentTraceWords * trace_n, stream), "trace");
+        R.trace_n = trace_n;
+    }
     check_cuda(cudaEventRecord(ev0, stream), "event");
     check_cuda(launch_resident_sweep(R, stream), "resident sweep launch");
     ++launches;
     check_cuda(cudaEventRecord(ev1, stream), "event");
     DevStatus out{};
     check_cuda(cudaMemcpyAsync(&out, st, sizeof(out), cudaMemcpyDeviceToHost, stream), "status");
-    check_cuda(cudaStreamSynchronize(stream), "resident sweep");
+    check_cuda(ctx->wait(), "resident sweep");
     check_cuda(cudaEventElapsedTime(ms, ev0, ev1), "elapsed");
+    if (R.trace) {
+        std::vector<long long> tr((size_t)kResidentTraceWords * trace_n);
+        check_cuda(cudaMemcpyAsync(tr.data(), R.trace, sizeof(long long) * tr.size(), cudaMemcpyDeviceToHost, stream),
+                   "trace copy");
+        check_cuda(ctx->wait(), "trace copy");
+        ctx->release(R.trace);
+        if (FILE* fh = std::fopen(trace_path, "wb")) {
+            std::fwrite(tr.data(), sizeof(long long), tr.size(), fh);
+            std::fclose(fh);
+        }
+    }
     *flag = out.flag;
     *iters = out.iterations;
     *obj = out.objective;
@@ -892,6 +919,13 @@ int ccdb_context_create(int device, size_t hbm_budget_bytes, ccdb_context** out)
             throw Error(CCDB_ERR_UNSUPPORTED, "device lacks cooperative launch");
         }
         check_cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream");
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        check_cuda(cudaMemPoolCreate(&c->pool, &props), "memory pool");
+        uint64_t keep = UINT64_MAX;  // freed blocks stay reserved for the next fit
+        check_cuda(cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep), "memory pool");
         check_cuda(cudaEventCreate(&c->ev_a), "event");
         check_cuda(cudaEventCreate(&c->ev_b), "event");
         *out = c;
@@ -905,8 +939,27 @@ int ccdb_context_destroy(ccdb_context* ctx) {
         cudaStreamSynchronize(ctx->stream);
         cudaEventDestroy(ctx->ev_a);
         cudaEventDestroy(ctx->ev_b);
+        if (ctx->ev_wait) cudaEventDestroy(ctx->ev_wait);
         cudaStreamDestroy(ctx->stream);
+        if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
         delete ctx;
+    });
+}
+
+int ccdb_context_set_blocking_wait(ccdb_context* ctx, int32_t on) {
+    return guard([&] {
+        require(ctx != nullptr, "NULL context");
+        check_cuda(cudaSetDevice(ctx->device), "cudaSetDevice");
+        check_cuda(cudaStreamSynchronize(ctx->stream), "sync");
+        ctx->blocking_wait = on != 0;
+        if (ctx->blocking_wait && !ctx->ev_wait)
+            check_cuda(cudaEventCreateWithFlags(&ctx->ev_wait, cudaEventBlockingSync | cudaEventDisableTiming),
+                       "event");
+        // the one-call fit's timing events follow the setting (fits made later do too)
+        for (cudaEvent_t* e : {&ctx->ev_a, &ctx->ev_b}) {
+            if (*e) check_cuda(cudaEventDestroy(*e), "event");
+            check_cuda(cudaEventCreateWithFlags(e, ctx->event_flags()), "event");
+        }
     });
 }
 
@@ -988,7 +1041,7 @@ int ccdb_matrix_create(ccdb_context* ctx, int64_t K, int32_t J, const int64_t* c
         m->d_fmt = upload(ctx, fmt, J, s);
         m->d_rows = upload(ctx, rows, nnz, s);
         m->d_vals = upload(ctx, vals, nv, s);
-        check_cuda(cudaStreamSynchronize(s), "matrix upload");
+        check_cuda(ctx->wait(), "matrix upload");
         *out = m.release();
     });
 }
@@ -1043,10 +1096,10 @@ int ccdb_fit_create(ccdb_context* ctx, const ccdb_matrix* m, const ccdb_fit_desc
         f->w = static_cast<double*>(ctx->alloc(sizeof(double) * K));
         f->gh_parts = static_cast<double2*>(ctx->alloc(sizeof(double2) * Fit::kGhParts));
         f->gh_out = static_cast<double2*>(ctx->alloc(sizeof(double2)));
-        check_cuda(cudaEventCreate(&f->ev0), "event");
-        check_cuda(cudaEventCreate(&f->ev1), "event");
-        check_cuda(cudaEventCreate(&f->evc0), "event");
-        check_cuda(cudaEventCreate(&f->evc1), "event");
+        check_cuda(cudaEventCreateWithFlags(&f->ev0, ctx->event_flags()), "event");
+        check_cuda(cudaEventCreateWithFlags(&f->ev1, ctx->event_flags()), "event");
+        check_cuda(cudaEventCreateWithFlags(&f->evc0, ctx->event_flags()), "event");
+        check_cuda(cudaEventCreateWithFlags(&f->evc1, ctx->event_flags()), "event");
         // CyclicCoordinateDescent::init (.cpp:200-239)
         f->beta_h.assign(J, 0.0);
         f->fixed.assign(J, 0);
@@ -1061,7 +1114,7 @@ int ccdb_fit_create(ccdb_context* ctx, const ccdb_matrix* m, const ccdb_fit_desc
         }
         f->upload_beta();
         if (grp_engine) f->cox_allocate();
-        check_cuda(cudaStreamSynchronize(f->stream), "fit upload");
+        check_cuda(f->ctx->wait(), "fit upload");
         *out = f.release();
     });
 }
@@ -1137,7 +1190,7 @@ int ccdb_compute_remaining_statistics(ccdb_fit* f) {
         require_fp64(f);
         f->check_lazy();
         f->remaining_statistics();
-        check_cuda(cudaStreamSynchronize(f->stream), "sync");
+        check_cuda(f->ctx->wait(), "sync");
     });
 }
 
@@ -1159,7 +1212,7 @@ int ccdb_get_xbeta(ccdb_fit* f, double* out) {
         std::vector<double2> r(stride * f->K);
         check_cuda(cudaMemcpyAsync(r.data(), src, sizeof(double2) * stride * f->K, cudaMemcpyDeviceToHost,
                                    f->stream), "xbeta copy");
-        check_cuda(cudaStreamSynchronize(f->stream), "sync");
+        check_cuda(f->ctx->wait(), "sync");
         for (int64_t k = 0; k < f->K; ++k) out[k] = r[stride * k].x;
     });
 }
@@ -1493,7 +1546,7 @@ int ccdb_batch_find_mode(ccdb_fit* f, const ccdb_batch_desc* b, const ccdb_mode_
             check_cuda(cudaMemcpyAsync(beta_out, P.beta, sizeof(double) * (size_t)J * n, cudaMemcpyDeviceToHost, s),
                        "beta");
         }
-        check_cuda(cudaStreamSynchronize(s), "batch sync");
+        check_cuda(f->ctx->wait(), "batch sync");
         if (trace_path) {
             std::vector<long long> tr(6 * (size_t)J);
             check_cuda(cudaMemcpy(tr.data(), P.trace, sizeof(long long) * tr.size(), cudaMemcpyDeviceToHost),

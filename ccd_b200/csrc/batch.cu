@@ -372,9 +372,14 @@ __global__ void __launch_bounds__(kBT, 1) batch_sweep_kernel(BatchParams P) {
 
 cudaError_t launch_batch_sweep(const BatchParams& P, cudaStream_t stream) {
     const size_t smem = sizeof(ColStage) * 2;
-    const void* fn = (P.model == M_LOGISTIC) ? (const void*)batch_sweep_kernel<M_LOGISTIC>
-                                             : (const void*)batch_sweep_kernel<M_POISSON>;
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    static std::atomic<uint64_t> done{0};
+    cudaError_t e = once_per_device(done, [&] {
+        cudaError_t r = cudaFuncSetAttribute(batch_sweep_kernel<M_LOGISTIC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (r != cudaSuccess) return r;
+        return cudaFuncSetAttribute(batch_sweep_kernel<M_POISSON>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem);
+    });
     if (e != cudaSuccess) return e;
     if (P.model == M_LOGISTIC) batch_sweep_kernel<M_LOGISTIC><<<P.n_inst, kBT, smem, stream>>>(P);
     else batch_sweep_kernel<M_POISSON><<<P.n_inst, kBT, smem, stream>>>(P);

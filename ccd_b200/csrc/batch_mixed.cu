@@ -286,13 +286,14 @@ template <int MODEL, int G, int SN>
 cudaError_t launch_g(const BatchParams& P, cudaStream_t stream) {
     const size_t smem = sizeof(MStage<SN>) * kNBuf;
     void (*fn)(BatchParams) = batch_mixed_kernel<MODEL, G, SN>;
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    static std::atomic<uint64_t> done{0};
+    cudaError_t e = once_per_device(done, [&] {
+        cudaError_t r = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (r != cudaSuccess) return r;
+        return cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    });
     if (e != cudaSuccess) return e;
     const int C = P.cluster > 0 ? P.cluster : 1;
-    if (C > 8) {
-        e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-        if (e != cudaSuccess) return e;
-    }
     const int n_groups = (P.n_inst + G - 1) / G;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(n_groups * C);

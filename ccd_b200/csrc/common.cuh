@@ -4,6 +4,7 @@
 // word instead of hanging).
 #pragma once
 
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -11,6 +12,22 @@
 #include "step.h"
 
 namespace ccdb {
+
+// ---------------------------------------------------------------- host: attributes
+// A kernel's function attributes (dynamic shared memory, cluster size) are set
+// once per device, at its first launch, not before every launch: fits on
+// other streams launch the same kernels concurrently.
+template <typename F>
+inline cudaError_t once_per_device(std::atomic<uint64_t>& done, F&& set) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const uint64_t bit = 1ull << (dev & 63);
+    if (done.load(std::memory_order_acquire) & bit) return cudaSuccess;
+    e = set();
+    if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_acq_rel);
+    return e;
+}
 
 // ---------------------------------------------------------------- reductions
 __device__ __forceinline__ double2 warp_sum2(double2 v) {
@@ -99,7 +116,7 @@ __device__ __forceinline__ bool wait_geq(const unsigned* p, unsigned target, lon
     unsigned n = 0;
     while ((int)(ld_acquire_gpu(p) - target) < 0) {
         ++n;
-        if ((n & 63) == 0) {
+        if (n == 1 || (n & 63) == 0) {  // the first look, then every 64th
             if (ld_volatile_i32(&st->abort)) return false;
             if ((long long)(global_ns() - t0) > limit_ns) {
                 if (atomicCAS(&st->error, 0, err) == 0) st->error_where = where;

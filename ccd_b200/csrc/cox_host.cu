@@ -134,7 +134,7 @@ void Fit::cox_allocate() {
                                    cudaMemcpyHostToDevice, stream), "grow");
         cox_grow_h = grow;
     }
-    check_cuda(cudaStreamSynchronize(stream), "cox alloc");
+    check_cuda(ctx->wait(), "cox alloc");
 }
 
 void Fit::cox_release() {
@@ -172,7 +172,7 @@ void Fit::cox_apply_weights() {
                 ll_fixed += weighted ? t * wh[i] : t;
             }
         }
-        check_cuda(cudaStreamSynchronize(stream), "grouped weights");
+        check_cuda(ctx->wait(), "grouped weights");
         valid_weights = true;
         suff_known = false;
         return;
@@ -215,7 +215,7 @@ void Fit::cox_apply_weights() {
                "xjy");
     ++launches;
     ll_fixed = 0.0;
-    check_cuda(cudaStreamSynchronize(stream), "cox weights");
+    check_cuda(ctx->wait(), "cox weights");
     valid_weights = true;
     suff_known = false;
 }
@@ -253,7 +253,7 @@ void Fit::cox_objective_terms(double* out4) {
     std::vector<double2> parts(2 * nb);
     check_cuda(cudaMemcpyAsync(parts.data(), red, sizeof(double2) * 2 * nb, cudaMemcpyDeviceToHost, stream),
                "objective copy");
-    check_cuda(cudaStreamSynchronize(stream), "objective sync");
+    check_cuda(ctx->wait(), "objective sync");
     double t[4] = {0, 0, 0, 0};
     for (int c = 0; c < nb; ++c) {
         t[0] += parts[2 * c].x;
@@ -274,7 +274,7 @@ void Fit::cox_gh_batch(const int32_t* cols, int n, double2* out) {
     ++launches;
     check_cuda(cudaMemcpyAsync(out, cox.batch_out, sizeof(double2) * n, cudaMemcpyDeviceToHost, stream),
                "gh copy");
-    check_cuda(cudaStreamSynchronize(stream), "gh sync");
+    check_cuda(ctx->wait(), "gh sync");
 }
 
 void Fit::cox_update(int j, double delta) {
@@ -310,6 +310,25 @@ void Fit::find_mode_group_sweep(const ccdb_mode_args& a, int* flag, int* iters, 
     if (bps < 1) throw Error(CCDB_ERR_CUDA, "the group sweep kernel does not fit on an SM");
     int n_cta = ctx->n_sm;
     if (ctx->max_ctas > 0) n_cta = std::min(n_cta, ctx->max_ctas);
+    // the cluster form (hardware barriers) when the fit is small enough for a few
+    // SMs or the context's share is a cluster's worth; CCDB_SWEEP_GRID_LEVELS asks
+    // for the grid form, CCDB_SWEEP_LEVELS for the cluster form
+    if (ctx->group_cluster < 0) {
+        int c = 0;
+        check_cuda(group_sweep_max_cluster(&c), "cluster occupancy");
+        ctx->group_cluster = c;
+    }
+    bool use_cluster = false;
+    if (ctx->group_cluster >= 2 && a.strategy != CCDB_SWEEP_GRID_LEVELS) {
+        const int64_t work = cox.N + max_entries;
+        use_cluster = a.strategy == CCDB_SWEEP_LEVELS || n_cta <= ctx->group_cluster + ctx->group_cluster / 4 ||
+                      work <= (int64_t)ctx->group_cluster * kGroupClusterWork;
+        if (use_cluster) {
+            int c = ctx->group_cluster;
+            while (c > 2 && c > n_cta) c /= 2;
+            n_cta = c;
+        }
+    }
     if (!cox.sweep_cols) {
         cox.sweep_cols = static_cast<int32_t*>(ctx->alloc(sizeof(int32_t) * std::max(1, J)));
         cox.agg = ctx->alloc(sizeof(SegAgg) * 2 * ctx->n_sm);
@@ -366,14 +385,14 @@ void Fit::find_mode_group_sweep(const ccdb_mode_args& a, int* flag, int* iters, 
         Q.trace_steps = trace_steps;
     }
     check_cuda(cudaEventRecord(ev0, stream), "event");
-    check_cuda(launch_group_sweep(Q, n_cta, stream), "group sweep launch");
+    check_cuda(launch_group_sweep(Q, n_cta, use_cluster, stream), "group sweep launch");
     ++launches;
     check_cuda(cudaEventRecord(ev1, stream), "event");
     DevStatus out{};
     int64_t cnt[2] = {0, 0};
     check_cuda(cudaMemcpyAsync(&out, st, sizeof(out), cudaMemcpyDeviceToHost, stream), "status");
     check_cuda(cudaMemcpyAsync(cnt, cox.counters, sizeof(cnt), cudaMemcpyDeviceToHost, stream), "counters");
-    check_cuda(cudaStreamSynchronize(stream), "group sweep");
+    check_cuda(ctx->wait(), "group sweep");
     check_cuda(cudaEventElapsedTime(ms, ev0, ev1), "elapsed");
     if (d_trace) {
         std::vector<unsigned long long> tr(kTraceStamps * (size_t)trace_steps);

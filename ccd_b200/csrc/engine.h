@@ -37,15 +37,25 @@ struct Context {
     int max_ctas = 0;  // persistent sweep grids: at most this many CTAs (0: n_sm)
     int sweep_cluster = -1;  // largest resident cluster of the cluster sweep (-1: not queried)
     int64_t resident_rows = -1;  // most rows of a shared-memory resident sweep (-1: not queried)
+    int group_cluster = -1;      // largest resident cluster of the group sweep (-1: not queried)
     size_t budget = 0;
     size_t in_use = 0;
     cudaStream_t stream = nullptr;
+    cudaMemPool_t pool = nullptr;  // this context's own stream-ordered pool
     std::mutex mu;
     std::map<void*, size_t> sizes;
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;  // around a one-call fit
+    // host waits: spin (default) or sleep until the device signals (blocking_wait),
+    // for processes that run many contexts' calls at once (serving slots)
+    bool blocking_wait = false;
+    cudaEvent_t ev_wait = nullptr;
 
     void* alloc(size_t bytes);
     void release(void* p);
+    // wait for everything queued on the context's stream
+    cudaError_t wait();
+    // event flags of this context's timing events
+    unsigned event_flags() const { return blocking_wait ? cudaEventBlockingSync : cudaEventDefault; }
 };
 
 struct Matrix {

@@ -28,8 +28,11 @@
 // the old values.  Convergence is tested on the device after each sweep, in
 // every CTA from the same partial sums.
 //
-// Every wait is a grid barrier bounded by wait_limit_ns (common.cuh); a wait
-// that runs out records an error, raises the abort word and all CTAs return.
+// Fits a few SMs cover run as one thread-block cluster whose barriers are the
+// hardware cluster barrier (no wait to bound); otherwise as a cooperative grid
+// whose every wait is a grid barrier bounded by wait_limit_ns (common.cuh): a
+// wait that runs out records an error, raises the abort word and all CTAs
+// return.
 #include <cstdint>
 
 #include "common.cuh"
@@ -198,8 +201,23 @@ __device__ __forceinline__ void load_rev(const CoxParams& P, int64_t g, int n, i
         }
 }
 
+// Every CTA's writes before it are visible to every CTA after it.  CL: the
+// launch is one thread-block cluster and the hardware cluster barrier (release
+// / acquire at cluster scope) does it; there is no wait to bound, and no CTA
+// leaves the kernel before the others.  Otherwise the bounded grid barrier of
+// a cooperative launch; false when its wait ran out.
+template <bool CL>
+__device__ __forceinline__ bool sync_all(const GroupSweepParams& Q, unsigned& epoch, int32_t* s_fail) {
+    if (CL) {
+        asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+        return true;
+    }
+    return grid_barrier(Q.grid_bar, epoch, Q.wait_limit_ns, Q.st, s_fail);
+}
+
 // D, S1, S2 rebuilt from the group denominators (Cox).  Three phases separated
 // by grid barriers; false when a barrier wait ran out.
+template <bool CL>
 __device__ bool cox_rebuild(const GroupSweepParams& Q, unsigned& epoch, int32_t* s_fail, Seg3* s_w,
                             Seg3* s_tot, Seg3* s_carry, unsigned long long* trc) {
     const CoxParams& P = Q.P;
@@ -228,7 +246,7 @@ __device__ bool cox_rebuild(const GroupSweepParams& Q, unsigned& epoch, int32_t*
         __stcg(&Q.agg[b].f, s_tot->f);
         __stcg(&Q.agg[b].v0, s_tot->a);
     }
-    if (!grid_barrier(Q.grid_bar, epoch, Q.wait_limit_ns, Q.st, s_fail)) return false;
+    if (!sync_all<CL>(Q, epoch, s_fail)) return false;
     if (trc) trc[4] = global_ns();
     // phase 2: carry-in from the CTAs before, D of the range; suffix aggregates
     if (threadIdx.x < 32) {
@@ -276,7 +294,7 @@ __device__ bool cox_rebuild(const GroupSweepParams& Q, unsigned& epoch, int32_t*
         __stcg(&Q.agg[G + b].v0, s_tot->a);
         __stcg(&Q.agg[G + b].v1, s_tot->b);
     }
-    if (!grid_barrier(Q.grid_bar, epoch, Q.wait_limit_ns, Q.st, s_fail)) return false;
+    if (!sync_all<CL>(Q, epoch, s_fail)) return false;
     if (trc) trc[5] = global_ns();
     // phase 3: carry-in from the CTAs after (suffix direction), S1 and S2 of the range
     prefetch_l1(P.D, t0, t1);
@@ -304,7 +322,7 @@ __device__ bool cox_rebuild(const GroupSweepParams& Q, unsigned& epoch, int32_t*
                 }
         }
     }
-    return grid_barrier(Q.grid_bar, epoch, Q.wait_limit_ns, Q.st, s_fail);
+    return sync_all<CL>(Q, epoch, s_fail);
 }
 
 // This CTA's objective partials {LL numerator, LL denominator, gradient
@@ -338,7 +356,7 @@ __device__ double4 objective_share(const GroupSweepParams& Q, double4* s_red4) {
     return block_sum4<kW>(acc, s_red4);
 }
 
-template <bool COX>
+template <bool COX, bool CL>
 __device__ bool objective_all(const GroupSweepParams& Q, unsigned& epoch, int32_t* s_fail, double4* s_red4,
                               double& obj, double& ll, double& lp) {
     const double4 o = objective_share<COX>(Q, s_red4);
@@ -346,7 +364,7 @@ __device__ bool objective_all(const GroupSweepParams& Q, unsigned& epoch, int32_
         __stcg(Q.red + 2 * blockIdx.x, make_double2(o.x, o.y));
         __stcg(Q.red + 2 * blockIdx.x + 1, make_double2(o.z, o.w));
     }
-    if (!grid_barrier(Q.grid_bar, epoch, Q.wait_limit_ns, Q.st, s_fail)) return false;
+    if (!sync_all<CL>(Q, epoch, s_fail)) return false;
     double4 t = make_double4(0.0, 0.0, 0.0, 0.0);
     for (int c = 0; c < (int)gridDim.x; ++c) {
         const double2 u = __ldcg(Q.red + 2 * c), v = __ldcg(Q.red + 2 * c + 1);
@@ -359,10 +377,10 @@ __device__ bool objective_all(const GroupSweepParams& Q, unsigned& epoch, int32_
     lp = t.w;
     obj = (Q.conv == C_GRADIENT) ? t.z : (Q.conv == C_MITTAL ? ll : ll + t.w);
     // every CTA has read the partials before any of them writes the next ones
-    return grid_barrier(Q.grid_bar, epoch, Q.wait_limit_ns, Q.st, s_fail);
+    return sync_all<CL>(Q, epoch, s_fail);
 }
 
-template <bool COX>
+template <bool COX, bool CL>
 __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) {
     __shared__ GhShared S;
     __shared__ double4 s_red4[kW];
@@ -384,7 +402,7 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
 
     // grid barrier, then CTA 0 applies the held-back writes of the last decision
     auto barrier = [&]() -> bool {
-        if (!grid_barrier(Q.grid_bar, epoch, Q.wait_limit_ns, Q.st, &s_fail)) return false;
+        if (!sync_all<CL>(Q, epoch, &s_fail)) return false;
         if (b == 0 && pend_n > 0) {
             for (int i = tid; i < pend_n; i += blockDim.x) Q.hdelta[Q.cols[pend_pos + i]] = s_pend_hd[i];
             if (tid == 0 && pend_col >= 0) Q.beta[pend_col] = s_newbeta;
@@ -396,7 +414,7 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
     };
 
     double last, ll, lp;
-    if (!objective_all<COX>(Q, epoch, &s_fail, s_red4, last, ll, lp)) return;
+    if (!objective_all<COX, CL>(Q, epoch, &s_fail, s_red4, last, ll, lp)) return;
 
     int iteration = 0;
     for (int it = 0; it < Q.max_iter; ++it) {
@@ -517,7 +535,7 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
                 if (!barrier()) return;
                 if (trc) trc[3] = global_ns();
             }
-            if (COX && !cox_rebuild(Q, epoch, &s_fail, s_w3, &s_tot, &s_carry, trc)) return;
+            if (COX && !cox_rebuild<CL>(Q, epoch, &s_fail, s_w3, &s_tot, &s_carry, trc)) return;
             if (trc) trc[6] = global_ns();
             pos += first + 1;
             if (trc) {
@@ -530,7 +548,7 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
         // the sweep is complete: held-back writes land, then the objective
         if (!barrier()) return;
         double cur;
-        if (!objective_all<COX>(Q, epoch, &s_fail, s_red4, cur, ll, lp)) return;
+        if (!objective_all<COX, CL>(Q, epoch, &s_fail, s_red4, cur, ll, lp)) return;
         iteration = it + 1;
         double conv;
         bool ill = false;
@@ -572,12 +590,60 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
 int group_sweep_threads() { return kT; }
 
 cudaError_t group_sweep_occupancy(int* blocks_per_sm) {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, group_sweep_kernel<true>, kT, 0);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, group_sweep_kernel<true, false>, kT, 0);
 }
 
-cudaError_t launch_group_sweep(const GroupSweepParams& Q, int n_cta, cudaStream_t stream) {
+namespace {
+cudaLaunchConfig_t cluster_cfg(int c, cudaStream_t stream, cudaLaunchAttribute* attr) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(c);
+    cfg.blockDim = dim3(kT);
+    cfg.stream = stream;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = c;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cfg;
+}
+}  // namespace
+
+// The largest cluster (16, 8, 4, 2) of the cluster form of which one can be
+// resident; 0 if none.  Sets the kernels' cluster attribute once.
+cudaError_t group_sweep_max_cluster(int* cluster) {
+    *cluster = 0;
+    for (const void* fn : {(const void*)group_sweep_kernel<true, true>, (const void*)group_sweep_kernel<false, true>}) {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return e;
+    }
+    for (int c = kMaxGroupCluster; c >= 2; c /= 2) {
+        cudaLaunchAttribute attr[1];
+        const cudaLaunchConfig_t cfg = cluster_cfg(c, 0, attr);
+        int n = 0, n2 = 0;
+        cudaError_t e = cudaOccupancyMaxActiveClusters(&n, group_sweep_kernel<true, true>, &cfg);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveClusters(&n2, group_sweep_kernel<false, true>, &cfg);
+        if (e != cudaSuccess) {
+            cudaGetLastError();  // a size the device rejects: try the next one
+            continue;
+        }
+        if (n >= 1 && n2 >= 1) {
+            *cluster = c;
+            return cudaSuccess;
+        }
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_group_sweep(const GroupSweepParams& Q, int n_cta, bool cluster, cudaStream_t stream) {
+    if (cluster) {
+        cudaLaunchAttribute attr[1];
+        const cudaLaunchConfig_t cfg = cluster_cfg(n_cta, stream, attr);
+        if (Q.cox) return cudaLaunchKernelEx(&cfg, group_sweep_kernel<true, true>, Q);
+        return cudaLaunchKernelEx(&cfg, group_sweep_kernel<false, true>, Q);
+    }
     void* args[] = {(void*)&Q};
-    const void* fn = Q.cox ? (const void*)group_sweep_kernel<true> : (const void*)group_sweep_kernel<false>;
+    const void* fn = Q.cox ? (const void*)group_sweep_kernel<true, false> : (const void*)group_sweep_kernel<false, false>;
     return cudaLaunchCooperativeKernel(fn, dim3(n_cta), dim3(kT), args, 0, stream);
 }
 

@@ -54,7 +54,13 @@ struct GroupSweepParams {
 };
 
 cudaError_t group_sweep_occupancy(int* blocks_per_sm);
-cudaError_t launch_group_sweep(const GroupSweepParams& Q, int n_cta, cudaStream_t stream);
+// The cluster form: one thread-block cluster of up to kMaxGroupCluster CTAs,
+// hardware cluster barriers instead of grid barriers (fits whose groups and
+// columns a few SMs cover).
+constexpr int kMaxGroupCluster = 16;
+constexpr int64_t kGroupClusterWork = 16384;  // groups + longest column per CTA below which a cluster serves
+cudaError_t group_sweep_max_cluster(int* cluster);
+cudaError_t launch_group_sweep(const GroupSweepParams& Q, int n_cta, bool cluster, cudaStream_t stream);
 int group_sweep_threads();
 
 }  // namespace ccdb

@@ -1225,10 +1225,13 @@ cudaError_t launch_indep_sweep(const IndepParams& P, int n_cta, cudaStream_t str
 
 template <int MODEL>
 static cudaError_t cluster_attrs() {
-    cudaError_t e = cudaFuncSetAttribute(cluster_sweep_kernel<MODEL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kClusterSmem);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(cluster_sweep_kernel<MODEL>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    static std::atomic<uint64_t> done{0};
+    return once_per_device(done, [] {
+        cudaError_t e = cudaFuncSetAttribute(cluster_sweep_kernel<MODEL>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClusterSmem);
+        if (e != cudaSuccess) return e;
+        return cudaFuncSetAttribute(cluster_sweep_kernel<MODEL>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    });
 }
 
 template <int MODEL>

@@ -54,7 +54,7 @@ void Fit::mm_gradient_hessian(const uint8_t* fixed_flags, double2* out) {
         check_cuda(launch_mm_gradient_hessian(P, stream), "mm gradient");
         ++launches;
         check_cuda(cudaMemcpyAsync(out, d_gh, sizeof(double2) * J, cudaMemcpyDeviceToHost, stream), "mm copy");
-        check_cuda(cudaStreamSynchronize(stream), "mm sync");
+        check_cuda(ctx->wait(), "mm sync");
     } catch (...) {
         ctx->release(d_gh);
         ctx->release(d_fixed);

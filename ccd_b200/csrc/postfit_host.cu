@@ -75,7 +75,7 @@ void Fit::fisher_information(const int32_t* idx, int n, double* out) {
     check_cuda(cudaEventRecord(evc1, stream), "event");
     check_cuda(cudaMemcpyAsync(out, P.out, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToHost, stream),
                "fisher copy");
-    check_cuda(cudaStreamSynchronize(stream), "fisher sync");
+    check_cuda(ctx->wait(), "fisher sync");
     float ms = 0.f;
     check_cuda(cudaEventElapsedTime(&ms, evc0, evc1), "elapsed");
     last_call_seconds = ms * 1e-3;
@@ -113,7 +113,7 @@ double Fit::predictive_log_likelihood(const double* weights) {
     }
     restore();
     check_lazy();
-    check_cuda(cudaStreamSynchronize(stream), "restore sync");
+    check_cuda(ctx->wait(), "restore sync");
     return ll;
 }
 
@@ -143,7 +143,7 @@ double Fit::predictive_sum(const double* weights) {
     std::vector<double> h(nb);
     check_cuda(cudaMemcpyAsync(h.data(), part, sizeof(double) * nb, cudaMemcpyDeviceToHost, stream),
                "predictive copy");
-    check_cuda(cudaStreamSynchronize(stream), "predictive sync");
+    check_cuda(ctx->wait(), "predictive sync");
     double ll = 0.0;
     for (int b = 0; b < nb; ++b) ll += h[b];
     return ll;
@@ -165,7 +165,7 @@ void Fit::predictive_estimates(double* out) {
     ++launches;
     check_cuda(cudaMemcpyAsync(out, d_out, sizeof(double) * K, cudaMemcpyDeviceToHost, stream),
                "estimates copy");
-    check_cuda(cudaStreamSynchronize(stream), "estimates sync");
+    check_cuda(ctx->wait(), "estimates sync");
 }
 
 }  // namespace ccdb

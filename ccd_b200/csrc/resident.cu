@@ -1,29 +1,27 @@
 // resident.cu -- one findMode of a small independent-row fit (logistic,
 // Poisson) in one CTA whose shared memory holds the row state.
 //
-// A fit of up to resident_max_rows() rows keeps {xBeta, denominator} of every
-// row in shared memory for the whole launch.  offsExpXBeta is not stored: every
-// value the engine ever holds for it is exp(xBeta) of the same xBeta (set by
-// computeRemainingStatistics and by every update, ModelSpecifics.hpp:1548-1571),
-// so it is recomputed where it is used.  The weights stay in global memory and
-// are read only by weighted fits (an unweighted fit's weights are 1.0, whose
-// products are exact).  With no other CTA to wait for, a coordinate costs
-// shared-memory latency and the L2 round trips of its column's entries, not a
-// grid or cluster barrier.
+// A fit of up to resident_max_rows() rows keeps {offsExpXBeta, denominator} of
+// every row in shared memory for the whole launch; xBeta and the weights stay
+// in global memory (L1-cached: this CTA is their only user), read where an
+// entry is updated and by the objective.  The weights are read only by
+// weighted fits (an unweighted fit's weights are 1.0, whose products are
+// exact).  With no other CTA to wait for, a coordinate costs shared-memory and
+// L1 latency and its arithmetic, not a grid or cluster barrier.
 //
 // The sweep is the sequential cycle (CyclicCoordinateDescent.cpp:1008-1021) run
 // as speculative batches: the warps compute the gradients of consecutive short
 // columns (one each) against one state, the first nonzero step in visiting
 // order is applied by its warp, and the batch restarts after it -- every zero
 // step leaves the state untouched, so each gradient is the one the sequential
-// cycle computes.  A long column (more than kLong entries: the intercept, dense
-// columns) is taken by the whole CTA on its own.  Bounds (hDelta) change with
-// every visited coordinate, zero steps included, as applyBounds does.  The
-// per-position column records (row offset, value offset, entry count, format)
-// are built by the host, so a batch reads one record per column before its
-// entries.  The convergence test runs on the device after each cycle from the
-// same objective terms as the other sweeps; at exit the row state is written
-// back to global memory.
+// cycle computes.  A batch is one column per warp: its cost is the latency of
+// one warp's gradient, step and update, whatever its width.  A long column
+// (more than kLong entries: the intercept, dense columns) is taken by the
+// whole CTA on its own.  Bounds (hDelta) change with every visited
+// coordinate, zero steps included, as applyBounds does.  The per-position column records (row offset, value
+// offset, entry count, format) are built by the host.  The convergence test
+// runs on the device after each cycle from the same objective terms as the
+// other sweeps; at exit the row state is written back to global memory.
 //
 // No wait spans CTAs (there is one), so the kernel has no wait to bound.
 #include <cstdint>
@@ -67,11 +65,13 @@ __device__ __forceinline__ void entry_gh(bool ind, double x, double e, double dn
 
 // updateXBeta for one entry: xBeta += delta x, offsExpXBeta = exp, the
 // denominator changed by the difference (ModelSpecifics.hpp:1548-1571).
-__device__ __forceinline__ void entry_update(double2* s_rs, int k, double x, double delta) {
-    const double2 xd = s_rs[k];
-    const double xb = xd.x + delta * x;
+__device__ __forceinline__ void entry_update(const IndepParams& P, double2* s_rs, int k, double xb_old, double x,
+                                             double delta) {
+    const double xb = xb_old + delta * x;
     const double en = exp(xb);
-    s_rs[k] = make_double2(xb, xd.y + (en - exp(xd.x)));
+    const double2 ed = s_rs[k];
+    s_rs[k] = make_double2(en, ed.y + (en - ed.x));
+    P.row[2 * (int64_t)k].x = xb;
 }
 
 // The step of column j from its (g, h) sums: Newton step with the prior,
@@ -113,13 +113,14 @@ __device__ double4 objective_terms(const ResidentParams& R, const double2* s_rs,
     const IndepParams& P = R.P;
     double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
     for (int64_t k = threadIdx.x; k < P.K; k += blockDim.x) {
-        const double2 xd = s_rs[k];
+        const double xb = P.row[2 * k].x;
+        const double dn = s_rs[k].y;
         const double w = R.weighted ? P.row[2 * k + 1].y : 1.0;
         const double yk = P.y[k];
-        acc.x += (double)((int)yk) * xd.x * w;
-        if (MODEL == M_LOGISTIC) acc.y += w * log(xd.y);
-        else acc.y += w * xd.y;
-        acc.z += xd.x * yk * w;
+        acc.x += (double)((int)yk) * xb * w;
+        if (MODEL == M_LOGISTIC) acc.y += w * log(dn);
+        else acc.y += w * dn;
+        acc.z += xb * yk * w;
     }
     for (int64_t j = threadIdx.x; j < P.J; j += blockDim.x) acc.w += log_prior_one(P.beta[j], P.ptype[j], P.pvar[j]);
     return block_sum4<kRW>(acc, s_red4);
@@ -142,14 +143,14 @@ __device__ __forceinline__ ResCol shfl_rec(const ResCol& r, int src) {
 }
 
 // Hint into L1 what the batch after this one reads: warp w the row ids,
-// values and metadata of the column kRW + w positions ahead (its record is in
-// lane kRW + w), warp 0 the records 32 positions ahead.  A batch that stops
+// values and metadata of the column nb + w positions ahead (its record is in
+// lane nb + w), warp 0 the records 32 positions ahead.  A batch that stops
 // early at a nonzero step restarts inside the current batch, whose data is
 // already in L1, and then reaches these columns.
-__device__ __forceinline__ void prefetch_ahead(const ResidentParams& R, const ResCol& rec, int wid, int lane,
-                                               int pos) {
+__device__ __forceinline__ void prefetch_ahead(const ResidentParams& R, const ResCol& rec, int nb, int wid,
+                                               int lane, int pos) {
     const IndepParams& P = R.P;
-    const ResCol c = shfl_rec(rec, kRW + wid);
+    const ResCol c = shfl_rec(rec, nb + wid);
     if (c.j >= 0 && c.n <= kLong) {
         const bool has_rows = c.flags & 1, has_vals = c.flags & 2;
         if (has_rows && lane * 32 < c.n) asm volatile("prefetch.global.L1 [%0];" ::"l"(P.rows + c.cb + lane * 32));
@@ -168,23 +169,26 @@ __device__ __forceinline__ void prefetch_ahead(const ResidentParams& R, const Re
 
 template <int MODEL>
 __global__ void __launch_bounds__(kRT, 1) resident_sweep_kernel(ResidentParams R) {
-    extern __shared__ __align__(16) double2 s_rs[];  // {xBeta, denominator} of every row
+    extern __shared__ __align__(16) double2 s_rs[];  // {offsExpXBeta, denominator} of every row
     __shared__ double2 s_red2[kRW];
     __shared__ double4 s_red4[kRW];
     __shared__ double s_delta[kRW], s_hd[kRW], s_beta[kRW];
 
     const IndepParams& P = R.P;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    for (int64_t k = tid; k < P.K; k += kRT) s_rs[k] = make_double2(P.row[2 * k].x, P.row[2 * k + 1].x);
+    for (int64_t k = tid; k < P.K; k += kRT) s_rs[k] = make_double2(P.row[2 * k].y, P.row[2 * k + 1].x);
     __syncthreads();
 
     double ll;
     double last = conv_objective(P.conv, objective_terms<MODEL>(R, s_rs, s_red4), P.ll_fixed, ll);
     unsigned long long moved = 0;
+    long long* tr = (R.trace && tid == 0) ? R.trace : nullptr;
+    int trn = R.trace_n;
 
     for (int it = 0; it < P.max_iter; ++it) {
         int pos = 0;
         while (pos < R.n_active) {
+            const long long tb0 = tr ? clock64() : 0;
             // the column records of the next 32 positions (lanes kRW.. hold the batch
             // after this one); the run of short ones among the first kRW
             ResCol rec{-1, 0, 0, 0, 0};
@@ -206,8 +210,8 @@ __global__ void __launch_bounds__(kRT, 1) resident_sweep_kernel(ResidentParams R
                     const int k = has_rows ? __ldg(P.rows + c.cb + p) : (int)p;
                     const double x = has_vals ? __ldg(P.vals + c.vb + p) : 1.0;
                     const double w = R.weighted ? P.row[2 * (int64_t)k + 1].y : 1.0;
-                    const double2 xd = s_rs[k];
-                    entry_gh<MODEL>(ind, x, exp(xd.x), xd.y, w, g, h);
+                    const double2 ed = s_rs[k];
+                    entry_gh<MODEL>(ind, x, ed.x, ed.y, w, g, h);
                 }
                 const double2 s = cta_sum2_all(make_double2(g, h), s_red2);
                 const double d = col_step(c.n, s.x, s.y, xjy, b0, ptype, pvar, hd);
@@ -215,7 +219,7 @@ __global__ void __launch_bounds__(kRT, 1) resident_sweep_kernel(ResidentParams R
                     for (int64_t p = tid; p < c.n; p += kRT) {
                         const int k = has_rows ? __ldg(P.rows + c.cb + p) : (int)p;
                         const double x = has_vals ? __ldg(P.vals + c.vb + p) : 1.0;
-                        entry_update(s_rs, k, x, d);
+                        entry_update(P, s_rs, k, P.row[2 * (int64_t)k].x, x, d);
                     }
                 }
                 if (tid == 0) {
@@ -227,13 +231,20 @@ __global__ void __launch_bounds__(kRT, 1) resident_sweep_kernel(ResidentParams R
                 }
                 __syncthreads();  // the state is read by the next columns
                 pos += 1;
+                if (tr) {
+                    tr[0] = tb0;
+                    tr[4] = clock64();
+                    tr[5] = -1;  // a long column
+                    tr += kResidentTraceWords;
+                    if (--trn <= 0) tr = nullptr;
+                }
                 continue;
             }
             // ---- a batch of nb short columns, one per warp, against the same state
             const ResCol c = shfl_rec(rec, wid < nb ? wid : 0);
             const bool has_rows = c.flags & 1, has_vals = c.flags & 2, ind = c.flags & 4;
             int k[kLanePer];
-            double x[kLanePer];
+            double x[kLanePer], xb[kLanePer];
             if (wid < nb) {
                 const int j = c.j;
 #pragma unroll
@@ -249,14 +260,15 @@ __global__ void __launch_bounds__(kRT, 1) resident_sweep_kernel(ResidentParams R
                 const double xjy = P.xjy[j], pvar = P.pvar[j], b0 = P.beta[j];
                 const int ptype = P.ptype[j];
                 double hd = P.hdelta[j];
-                prefetch_ahead(R, rec, wid, lane, pos);
+                prefetch_ahead(R, rec, nb, wid, lane, pos);
                 double g = 0.0, h = 0.0;
 #pragma unroll
                 for (int i = 0; i < kLanePer; ++i)
                     if (k[i] >= 0) {
                         const double w = R.weighted ? P.row[2 * (int64_t)k[i] + 1].y : 1.0;
-                        const double2 xd = s_rs[k[i]];
-                        entry_gh<MODEL>(ind, x[i], exp(xd.x), xd.y, w, g, h);
+                        xb[i] = P.row[2 * (int64_t)k[i]].x;  // kept for the update
+                        const double2 ed = s_rs[k[i]];
+                        entry_gh<MODEL>(ind, x[i], ed.x, ed.y, w, g, h);
                     }
                 // the butterfly leaves the same sums in every lane
                 const double2 s = warp_sum2(make_double2(g, h));
@@ -267,7 +279,9 @@ __global__ void __launch_bounds__(kRT, 1) resident_sweep_kernel(ResidentParams R
                     s_beta[wid] = b0;
                 }
             }
+            const long long tb1 = tr ? clock64() : 0;
             __syncthreads();
+            const long long tb2 = tr ? clock64() : 0;
             // the first nonzero step in visiting order; the columns up to it are visited
             const unsigned nz = __ballot_sync(0xffffffffu, lane < nb && s_delta[lane] != 0.0);
             const int first = nz ? __ffs(nz) - 1 : nb;
@@ -283,10 +297,22 @@ __global__ void __launch_bounds__(kRT, 1) resident_sweep_kernel(ResidentParams R
                 const double d = s_delta[wid];
 #pragma unroll
                 for (int i = 0; i < kLanePer; ++i)
-                    if (k[i] >= 0) entry_update(s_rs, k[i], x[i], d);
+                    if (k[i] >= 0) entry_update(P, s_rs, k[i], xb[i], x[i], d);
             }
+            const long long tb3 = tr ? clock64() : 0;
             __syncthreads();
             pos += walked;
+            if (tr) {
+                tr[0] = tb0;
+                tr[1] = tb1;
+                tr[2] = tb2;
+                tr[3] = tb3;
+                tr[4] = clock64();
+                tr[5] = nb;
+                tr[6] = first;
+                tr += kResidentTraceWords;
+                if (--trn <= 0) tr = nullptr;
+            }
         }
         // ---- the cycle is complete: convergence (findMode, CyclicCoordinateDescent.cpp:1023-1056)
         const double4 t = objective_terms<MODEL>(R, s_rs, s_red4);
@@ -320,9 +346,9 @@ __global__ void __launch_bounds__(kRT, 1) resident_sweep_kernel(ResidentParams R
     }
     // the row state back to global memory for the calls that follow
     for (int64_t k = tid; k < P.K; k += kRT) {
-        const double2 xd = s_rs[k];
-        P.row[2 * k] = make_double2(xd.x, exp(xd.x));
-        P.row[2 * k + 1].x = xd.y;
+        const double2 ed = s_rs[k];
+        P.row[2 * k].y = ed.x;
+        P.row[2 * k + 1].x = ed.y;
     }
     if (moved) atomicAdd(&P.st->nonzero_steps, moved);
 }
@@ -345,19 +371,22 @@ cudaError_t resident_max_rows(int model, int64_t* rows) {
 }
 
 cudaError_t launch_resident_sweep(const ResidentParams& R, cudaStream_t stream) {
+    // the dynamic shared memory limit is raised once to the most a CTA can hold
+    static std::atomic<uint64_t> done{0};
+    cudaError_t e = once_per_device(done, [] {
+        int dev = 0, optin = 0;
+        cudaError_t r = cudaGetDevice(&dev);
+        if (r == cudaSuccess) r = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (r != cudaSuccess) return r;
+        const int dyn = optin - (int)kStaticSmemBound;
+        r = cudaFuncSetAttribute(resident_sweep_kernel<M_LOGISTIC>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+        if (r != cudaSuccess) return r;
+        return cudaFuncSetAttribute(resident_sweep_kernel<M_POISSON>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    });
+    if (e != cudaSuccess) return e;
     const size_t smem = sizeof(double2) * (size_t)R.P.K;
-    cudaError_t e;
-    if (R.P.model == M_LOGISTIC) {
-        e = cudaFuncSetAttribute(resident_sweep_kernel<M_LOGISTIC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-        if (e != cudaSuccess) return e;
-        resident_sweep_kernel<M_LOGISTIC><<<1, kRT, smem, stream>>>(R);
-    } else {
-        e = cudaFuncSetAttribute(resident_sweep_kernel<M_POISSON>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-        if (e != cudaSuccess) return e;
-        resident_sweep_kernel<M_POISSON><<<1, kRT, smem, stream>>>(R);
-    }
+    if (R.P.model == M_LOGISTIC) resident_sweep_kernel<M_LOGISTIC><<<1, kRT, smem, stream>>>(R);
+    else resident_sweep_kernel<M_POISSON><<<1, kRT, smem, stream>>>(R);
     return cudaGetLastError();
 }
 

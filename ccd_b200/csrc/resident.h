@@ -25,7 +25,15 @@ struct ResidentParams {
     const ResCol* recs;    // the active columns in visiting order
     int32_t n_active;
     int32_t weighted;      // 0: every row weight is 1.0 and is not read
+    // optional per-batch SM-clock stamps of the first trace_n batches (profiling
+    // aid): start, gradients done, decided, applied, next; batch size, first
+    // nonzero step (kResidentTraceWords per batch)
+    long long* trace;
+    int32_t trace_n;
+    int32_t pad;
 };
+
+constexpr int kResidentTraceWords = 8;
 
 int resident_threads();
 // the most rows whose state fits the kernel's shared memory on the current device

@@ -117,6 +117,7 @@ def lib() -> C.CDLL:
         L.ccdb_context_memory.argtypes = [_P, C.POINTER(C.c_size_t)]
         L.ccdb_context_sm_count.argtypes = [_P, C.POINTER(C.c_int32)]
         L.ccdb_context_set_max_ctas.argtypes = [_P, C.c_int32]
+        L.ccdb_context_set_blocking_wait.argtypes = [_P, C.c_int32]
         L.ccdb_matrix_create.argtypes = [_P, C.c_int64, C.c_int32, _P, _P, _P, _P, _P, C.POINTER(_P)]
         L.ccdb_matrix_destroy.argtypes = [_P]
         L.ccdb_fit_create.argtypes = [_P, _P, C.POINTER(_FitDesc), C.POINTER(_P)]
@@ -180,6 +181,11 @@ class Context:
         v = C.c_int32()
         _check(lib().ccdb_context_sm_count(self.h, C.byref(v)))
         return v.value
+
+    def set_blocking_wait(self, on: bool = True) -> None:
+        """Host waits sleep until the device signals instead of spinning
+        (ccdb_context_set_blocking_wait); for many concurrent contexts."""
+        _check(lib().ccdb_context_set_blocking_wait(self.h, int(bool(on))))
 
     def set_max_ctas(self, max_ctas: int) -> None:
         """Persistent sweep grids of this context's fits use at most max_ctas CTAs."""

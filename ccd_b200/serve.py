@@ -166,6 +166,7 @@ class Server:
         if not hasattr(local, "ctx"):
             local.ctx = native.Context(self.device)
             local.ctx.set_max_ctas(max(1, local.ctx.sm_count // self.n_slots))
+            local.ctx.set_blocking_wait(True)  # slots wait without spinning the host cores
         args = req.args or native.ModeFindingArguments()
         r = native.fit_model(local.ctx, req.data, args)
         return r.beta, r.return_flag, r.iterations, r.log_likelihood

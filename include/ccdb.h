@@ -62,6 +62,13 @@ int ccdb_context_memory(const ccdb_context* ctx, size_t* bytes_in_use);
 /* Streaming multiprocessors of the context's GPU.  No reference counterpart. */
 int ccdb_context_sm_count(const ccdb_context* ctx, int32_t* n_sm);
 
+/* Host waits of this context's calls sleep until the device signals instead
+ * of spinning (cudaEventBlockingSync).  Off by default: a spinning wait
+ * returns sooner, but a process that runs many contexts' calls at once (one
+ * per serving slot) starves its own host threads when every waiting thread
+ * spins.  Affects fits made after the call.  No reference counterpart. */
+int ccdb_context_set_blocking_wait(ccdb_context* ctx, int32_t on);
+
 /* Persistent sweep kernels launched by this context's fits use at most
  * max_ctas CTAs (0: one per SM, the default).  Contexts that run fits at the
  * same time on one GPU (the serving loop's slots) split the SMs between them
@@ -186,7 +193,10 @@ typedef struct {
                                   _SPECULATIVE host-driven batches of gradients that restart
                                   after each nonzero step.  Cox and conditional models: one
                                   persistent launch per findMode of device-driven speculative
-                                  batches, or with _SPECULATIVE the host-driven batches */
+                                  batches -- one thread-block cluster with hardware barriers
+                                  for fits a few SMs cover (forced by _LEVELS), else a
+                                  cooperative grid (forced by _GRID_LEVELS) -- or with
+                                  _SPECULATIVE the host-driven batches */
     int32_t algorithm;         /* AlgorithmType (Types.h:149-153): CCDB_ALGORITHM_CCD (0,
                                   default) or CCDB_ALGORITHM_MM (findMode's MM cycle,
                                   CyclicCoordinateDescent.cpp:974-1001; conditional logistic,

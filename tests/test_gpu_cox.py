@@ -50,18 +50,20 @@ def test_cox_gradient_hessian(gpu_ctx, oracle_engine, kw):
 
 @pytest.mark.parametrize("kw", CASES)
 @pytest.mark.parametrize("conv", [GRADIENT, MITTAL, LANGE])
-@pytest.mark.parametrize("mode", ["device", "host_batches", "per_coordinate"])
+@pytest.mark.parametrize("mode", ["device", "device_grid", "host_batches", "per_coordinate"])
 def test_cox_find_mode(gpu_ctx, oracle_engine, kw, conv, mode):
-    """device: one persistent launch per findMode (group_sweep.cu); host_batches:
-    the host-driven speculative batches; per_coordinate: the reference's call
-    pattern, one round trip per coordinate."""
+    """device: one persistent launch per findMode (group_sweep.cu; a small fit
+    takes its cluster form); device_grid: its cooperative grid form;
+    host_batches: the host-driven speculative batches; per_coordinate: the
+    reference's call pattern, one round trip per coordinate."""
     d = synthetic.small(MODEL_COX, **kw)
     want = oracle_engine(d).fit(conv, 1e-6)
     m = native.Matrix(gpu_ctx, d)
     f = native.Fit(gpu_ctx, m, d)
     got = f.find_mode(native.ModeFindingArguments(
         convergence_type=conv, per_coordinate=(mode == "per_coordinate"),
-        strategy=native.SWEEP_SPECULATIVE if mode == "host_batches" else native.SWEEP_AUTO))
+        strategy={"host_batches": native.SWEEP_SPECULATIVE, "device_grid": native.SWEEP_GRID_LEVELS}.get(
+            mode, native.SWEEP_AUTO)))
     assert got.return_flag == want["flag"]
     assert got.iterations == want["iterations"]
     assert rel_beta(got.beta, want["beta"]) <= BETA_TOL
@@ -93,8 +95,9 @@ def test_cox_deterministic(gpu_ctx):
     assert r1.log_likelihood == r2.log_likelihood
 
 
+@pytest.mark.parametrize("form", [native.SWEEP_LEVELS, native.SWEEP_GRID_LEVELS])
 @pytest.mark.parametrize("prior,var", [(PRIOR_LAPLACE, 0.05), (PRIOR_NORMAL, 1.0)])
-def test_cox_device_sweep_on_many_ctas(gpu_ctx, oracle_engine, prior, var):
+def test_cox_device_sweep_on_many_ctas(gpu_ctx, oracle_engine, prior, var, form):
     """A problem large enough that the persistent sweep's row updates, group
     runs and scans spread over every CTA: 60,000 rows in 150 strata of uneven
     size, daily ties, 300 indicator columns; the device sweep against the
@@ -104,7 +107,7 @@ def test_cox_device_sweep_on_many_ctas(gpu_ctx, oracle_engine, prior, var):
     want = oracle_engine(d).fit(GRADIENT, 1e-6)
     m = native.Matrix(gpu_ctx, d)
     f = native.Fit(gpu_ctx, m, d)
-    got = f.find_mode(native.ModeFindingArguments(convergence_type=GRADIENT), beta=np.zeros(d.J))
+    got = f.find_mode(native.ModeFindingArguments(convergence_type=GRADIENT, strategy=form), beta=np.zeros(d.J))
     host = f.find_mode(native.ModeFindingArguments(convergence_type=GRADIENT, strategy=native.SWEEP_SPECULATIVE),
                        beta=np.zeros(d.J))
     for r in (got, host):

@@ -46,7 +46,7 @@ def test_grouped_gradient_hessian(gpu_ctx, oracle_engine, model, kw):
 
 @pytest.mark.parametrize("model,kw", CASES)
 @pytest.mark.parametrize("conv", [GRADIENT, MITTAL, LANGE])
-@pytest.mark.parametrize("strategy", [native.SWEEP_AUTO, native.SWEEP_SPECULATIVE])
+@pytest.mark.parametrize("strategy", [native.SWEEP_AUTO, native.SWEEP_GRID_LEVELS, native.SWEEP_SPECULATIVE])
 def test_grouped_find_mode(gpu_ctx, oracle_engine, model, kw, conv, strategy):
     """AUTO: one persistent launch per findMode; SPECULATIVE: host-driven batches."""
     d = synthetic.small(model, **kw)
@@ -72,12 +72,14 @@ def test_clr_weighted(gpu_ctx, oracle_engine):
     assert rel_beta(got.beta, want["beta"]) <= BETA_TOL
 
 
-def test_clr_device_sweep_on_many_ctas(gpu_ctx, oracle_engine):
+@pytest.mark.parametrize("form", [native.SWEEP_LEVELS, native.SWEEP_GRID_LEVELS])
+def test_clr_device_sweep_on_many_ctas(gpu_ctx, oracle_engine, form):
     """20,000 matched sets (~130,000 rows), 400 indicator columns: the persistent
-    sweep's row updates and stratum runs spread over every CTA."""
+    sweep's row updates and stratum runs spread over every CTA of its cluster
+    form (LEVELS) and of its grid form (GRID_LEVELS)."""
     d = synthetic.conditional_logistic(seed=13, n_sets=20_000, P=400)
     want = oracle_engine(d).fit(GRADIENT, 1e-6)
-    got = native.fit_model(gpu_ctx, d, native.ModeFindingArguments(convergence_type=GRADIENT))
+    got = native.fit_model(gpu_ctx, d, native.ModeFindingArguments(convergence_type=GRADIENT, strategy=form))
     assert got.return_flag == want["flag"]
     assert got.iterations == want["iterations"]
     assert rel_beta(got.beta, want["beta"]) <= BETA_TOL

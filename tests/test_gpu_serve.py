@@ -17,7 +17,7 @@ def test_served_results_equal_alone(gpu_ctx):
         srv.close()
     assert all(c.error is None for c in done), [c.error for c in done if c.error]
     assert srv.peak_running >= 2  # requests were admitted while others ran
-    args = native.ModeFindingArguments(strategy=native.SWEEP_LEVELS)
+    args = native.ModeFindingArguments()  # the server's default arguments
     alone_ctx = native.Context(0)
     alone_ctx.set_max_ctas(max(1, alone_ctx.sm_count // 4))  # the slots' grid size
     for c, (_, d) in zip(done, stream):

@@ -10,6 +10,8 @@ the same problem correctly on the same context:
 * the grid-wide level sweep (CCDB_SWEEP_GRID_LEVELS): its waits for a
   level's arrivals and for the grid barrier raise the launch's abort word and
   every CTA leaves;
+* the persistent group sweep's grid form (Cox, CCDB_SWEEP_GRID_LEVELS): the
+  same for its grid barriers;
 * the mixed-precision batch engine on a cluster of two CTAs per group: a wait
   for the other CTA's column sums raises the abort word; every CTA of the
   cluster stops stepping, finishes the sweep's exchanges (nothing is left in
@@ -61,3 +63,24 @@ def test_batch_cluster_exchange_wait_runs_out_then_recovers(gpu_ctx):
     assert np.array_equal(b, b_want)
     assert [x["iterations"] for x in r] == [x["iterations"] for x in r_want]
     assert all(x["flag"] == 0 for x in r)
+
+
+def test_group_sweep_grid_wait_runs_out_then_recovers(gpu_ctx, oracle_engine):
+    """The persistent group sweep's grid form (Cox): a grid barrier whose wait
+    runs out raises the abort word and every CTA leaves; the cluster form has
+    only hardware cluster barriers and no wait to bound."""
+    from ccd_b200.data import MODEL_COX
+    d = synthetic.small(MODEL_COX, seed=81, K=2000, P=30)
+    m = native.Matrix(gpu_ctx, d)
+    f = native.Fit(gpu_ctx, m, d)
+    args = native.ModeFindingArguments(convergence_type=MITTAL, strategy=native.SWEEP_GRID_LEVELS)
+    f.set_wait_limit(1)
+    with pytest.raises(native.CcdbError) as ex:
+        f.find_mode(args, beta=np.zeros(d.J))
+    assert ex.value.code == native.ERR_TIMEOUT
+    f.set_wait_limit(0)
+    want = oracle_engine(d).fit(MITTAL, 1e-6)
+    r = f.find_mode(args, beta=np.zeros(d.J))
+    assert r.return_flag == want["flag"] == 0
+    assert r.iterations == want["iterations"]
+    assert _rel(r.beta, want["beta"]) <= 1e-6
