@@ -570,7 +570,7 @@ def run_ours(args, world, rank, local, collect=False):
                           "algorithmic_bytes_per_launch": per_launch_bytes,
                           "kernel": ("cluster_sweep_kernel<POISSON>" if args.strategy != "grid_levels"
                                      else "indep_sweep_kernel<POISSON>") + " (one launch per findMode attempt)",
-                          "bytes": "SURVEY 8(d) bytes of every sweep that ran plus the objective checks",
+                          "bytes": "per-coordinate algorithmic bytes (column entries and the row state they gather and update) of every sweep that ran, plus the objective checks",
                           "traffic": traffic} if WORKLOAD == "poisson_offset" else
                          {"bound": "hbm", "achieved": cox_bytes(d, sweeps, nonzero) / ker_t / 1e9, "peak": peak,
                           "unit": "GB/s", "frac": cox_bytes(d, sweeps, nonzero) / ker_t / 1e9 / peak,

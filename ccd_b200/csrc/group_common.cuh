@@ -197,7 +197,7 @@ struct GhShared {
 // and weight; the group's suffix sums) are issued for all its entries at once
 // and one block scan serves the pass; the carry continues across passes.
 // Result valid in thread 0.
-constexpr int kIt = 8;  // column entries per thread per pass
+constexpr int kIt = 4;  // column entries per thread per pass
 
 __device__ __forceinline__ double2 cox_column_gh(const CoxParams& P, int j, GhShared& S) {
     const uint8_t f = P.fmt[j];

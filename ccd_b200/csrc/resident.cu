@@ -1,27 +1,29 @@
 // resident.cu -- one findMode of a small independent-row fit (logistic,
 // Poisson) in one CTA whose shared memory holds the row state.
 //
-// A fit of up to resident_max_rows() rows keeps {offsExpXBeta, denominator} of
-// every row in shared memory for the whole launch; xBeta and the weights stay
-// in global memory (L1-cached: this CTA is their only user), read where an
-// entry is updated and by the objective.  The weights are read only by
-// weighted fits (an unweighted fit's weights are 1.0, whose products are
-// exact).  With no other CTA to wait for, a coordinate costs shared-memory and
-// L1 latency and its arithmetic, not a grid or cluster barrier.
+// A fit of up to resident_max_rows() rows keeps {xBeta, denominator} of every
+// row in shared memory for the whole launch.  offsExpXBeta is not stored: every
+// value the engine ever holds for it is exp(xBeta) of the same xBeta (set by
+// computeRemainingStatistics and by every update, ModelSpecifics.hpp:1548-1571),
+// so it is recomputed where it is used.  The weights stay in global memory and
+// are read only by weighted fits (an unweighted fit's weights are 1.0, whose
+// products are exact).  With no other CTA to wait for, a coordinate costs
+// shared-memory latency and the L2 round trips of its column's entries, not a
+// grid or cluster barrier.
 //
 // The sweep is the sequential cycle (CyclicCoordinateDescent.cpp:1008-1021) run
 // as speculative batches: the warps compute the gradients of consecutive short
 // columns (one each) against one state, the first nonzero step in visiting
 // order is applied by its warp, and the batch restarts after it -- every zero
 // step leaves the state untouched, so each gradient is the one the sequential
-// cycle computes.  A batch is one column per warp: its cost is the latency of
-// one warp's gradient, step and update, whatever its width.  A long column
-// (more than kLong entries: the intercept, dense columns) is taken by the
-// whole CTA on its own.  Bounds (hDelta) change with every visited
-// coordinate, zero steps included, as applyBounds does.  The per-position column records (row offset, value
-// offset, entry count, format) are built by the host.  The convergence test
-// runs on the device after each cycle from the same objective terms as the
-// other sweeps; at exit the row state is written back to global memory.
+// cycle computes.  A long column (more than kLong entries: the intercept, dense
+// columns) is taken by the whole CTA on its own.  Bounds (hDelta) change with
+// every visited coordinate, zero steps included, as applyBounds does.  The
+// per-position column records (row offset, value offset, entry count, format)
+// are built by the host, so a batch reads one record per column before its
+// entries.  The convergence test runs on the device after each cycle from the
+// same objective terms as the other sweeps; at exit the row state is written
+// back to global memory.
 //
 // No wait spans CTAs (there is one), so the kernel has no wait to bound.
 #include <cstdint>
@@ -65,13 +67,11 @@ __device__ __forceinline__ void entry_gh(bool ind, double x, double e, double dn
 
 // updateXBeta for one entry: xBeta += delta x, offsExpXBeta = exp, the
 // denominator changed by the difference (ModelSpecifics.hpp:1548-1571).
-__device__ __forceinline__ void entry_update(const IndepParams& P, double2* s_rs, int k, double xb_old, double x,
-                                             double delta) {
-    const double xb = xb_old + delta * x;
+__device__ __forceinline__ void entry_update(double2* s_rs, int k, double x, double delta) {
+    const double2 xd = s_rs[k];
+    const double xb = xd.x + delta * x;
     const double en = exp(xb);
-    const double2 ed = s_rs[k];
-    s_rs[k] = make_double2(en, ed.y + (en - ed.x));
-    P.row[2 * (int64_t)k].x = xb;
+    s_rs[k] = make_double2(xb, xd.y + (en - exp(xd.x)));
 }
 
 // The step of column j from its (g, h) sums: Newton step with the prior,
@@ -113,14 +113,13 @@ __device__ double4 objective_terms(const ResidentParams& R, const double2* s_rs,
     const IndepParams& P = R.P;
     double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
     for (int64_t k = threadIdx.x; k < P.K; k += blockDim.x) {
-        const double xb = P.row[2 * k].x;
-        const double dn = s_rs[k].y;
+        const double2 xd = s_rs[k];
         const double w = R.weighted ? P.row[2 * k + 1].y : 1.0;
         const double yk = P.y[k];
-        acc.x += (double)((int)yk) * xb * w;
-        if (MODEL == M_LOGISTIC) acc.y += w * log(dn);
-        else acc.y += w * dn;
-        acc.z += xb * yk * w;
+        acc.x += (double)((int)yk) * xd.x * w;
+        if (MODEL == M_LOGISTIC) acc.y += w * log(xd.y);
+        else acc.y += w * xd.y;
+        acc.z += xd.x * yk * w;
     }
     for (int64_t j = threadIdx.x; j < P.J; j += blockDim.x) acc.w += log_prior_one(P.beta[j], P.ptype[j], P.pvar[j]);
     return block_sum4<kRW>(acc, s_red4);
@@ -142,41 +141,16 @@ __device__ __forceinline__ ResCol shfl_rec(const ResCol& r, int src) {
     return o;
 }
 
-// Hint into L1 what the batch after this one reads: warp w the row ids,
-// values and metadata of the column nb + w positions ahead (its record is in
-// lane nb + w), warp 0 the records 32 positions ahead.  A batch that stops
-// early at a nonzero step restarts inside the current batch, whose data is
-// already in L1, and then reaches these columns.
-__device__ __forceinline__ void prefetch_ahead(const ResidentParams& R, const ResCol& rec, int nb, int wid,
-                                               int lane, int pos) {
-    const IndepParams& P = R.P;
-    const ResCol c = shfl_rec(rec, nb + wid);
-    if (c.j >= 0 && c.n <= kLong) {
-        const bool has_rows = c.flags & 1, has_vals = c.flags & 2;
-        if (has_rows && lane * 32 < c.n) asm volatile("prefetch.global.L1 [%0];" ::"l"(P.rows + c.cb + lane * 32));
-        if (has_vals && lane * 16 < c.n) asm volatile("prefetch.global.L1 [%0];" ::"l"(P.vals + c.vb + lane * 16));
-        if (lane == 31) {
-            asm volatile("prefetch.global.L1 [%0];" ::"l"(P.xjy + c.j));
-            asm volatile("prefetch.global.L1 [%0];" ::"l"(P.pvar + c.j));
-            asm volatile("prefetch.global.L1 [%0];" ::"l"(P.ptype + c.j));
-            asm volatile("prefetch.global.L1 [%0];" ::"l"(P.beta + c.j));
-            asm volatile("prefetch.global.L1 [%0];" ::"l"(P.hdelta + c.j));
-        }
-    }
-    if (wid == 0 && lane < 8 && pos + 32 + lane * 4 < R.n_active)
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(R.recs + pos + 32 + lane * 4));
-}
-
 template <int MODEL>
 __global__ void __launch_bounds__(kRT, 1) resident_sweep_kernel(ResidentParams R) {
-    extern __shared__ __align__(16) double2 s_rs[];  // {offsExpXBeta, denominator} of every row
+    extern __shared__ __align__(16) double2 s_rs[];  // {xBeta, denominator} of every row
     __shared__ double2 s_red2[kRW];
     __shared__ double4 s_red4[kRW];
     __shared__ double s_delta[kRW], s_hd[kRW], s_beta[kRW];
 
     const IndepParams& P = R.P;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    for (int64_t k = tid; k < P.K; k += kRT) s_rs[k] = make_double2(P.row[2 * k].y, P.row[2 * k + 1].x);
+    for (int64_t k = tid; k < P.K; k += kRT) s_rs[k] = make_double2(P.row[2 * k].x, P.row[2 * k + 1].x);
     __syncthreads();
 
     double ll;
@@ -210,8 +184,8 @@ __global__ void __launch_bounds__(kRT, 1) resident_sweep_kernel(ResidentParams R
                     const int k = has_rows ? __ldg(P.rows + c.cb + p) : (int)p;
                     const double x = has_vals ? __ldg(P.vals + c.vb + p) : 1.0;
                     const double w = R.weighted ? P.row[2 * (int64_t)k + 1].y : 1.0;
-                    const double2 ed = s_rs[k];
-                    entry_gh<MODEL>(ind, x, ed.x, ed.y, w, g, h);
+                    const double2 xd = s_rs[k];
+                    entry_gh<MODEL>(ind, x, exp(xd.x), xd.y, w, g, h);
                 }
                 const double2 s = cta_sum2_all(make_double2(g, h), s_red2);
                 const double d = col_step(c.n, s.x, s.y, xjy, b0, ptype, pvar, hd);
@@ -219,7 +193,7 @@ __global__ void __launch_bounds__(kRT, 1) resident_sweep_kernel(ResidentParams R
                     for (int64_t p = tid; p < c.n; p += kRT) {
                         const int k = has_rows ? __ldg(P.rows + c.cb + p) : (int)p;
                         const double x = has_vals ? __ldg(P.vals + c.vb + p) : 1.0;
-                        entry_update(P, s_rs, k, P.row[2 * (int64_t)k].x, x, d);
+                        entry_update(s_rs, k, x, d);
                     }
                 }
                 if (tid == 0) {
@@ -244,7 +218,7 @@ __global__ void __launch_bounds__(kRT, 1) resident_sweep_kernel(ResidentParams R
             const ResCol c = shfl_rec(rec, wid < nb ? wid : 0);
             const bool has_rows = c.flags & 1, has_vals = c.flags & 2, ind = c.flags & 4;
             int k[kLanePer];
-            double x[kLanePer], xb[kLanePer];
+            double x[kLanePer];
             if (wid < nb) {
                 const int j = c.j;
 #pragma unroll
@@ -260,15 +234,13 @@ __global__ void __launch_bounds__(kRT, 1) resident_sweep_kernel(ResidentParams R
                 const double xjy = P.xjy[j], pvar = P.pvar[j], b0 = P.beta[j];
                 const int ptype = P.ptype[j];
                 double hd = P.hdelta[j];
-                prefetch_ahead(R, rec, nb, wid, lane, pos);
                 double g = 0.0, h = 0.0;
 #pragma unroll
                 for (int i = 0; i < kLanePer; ++i)
                     if (k[i] >= 0) {
                         const double w = R.weighted ? P.row[2 * (int64_t)k[i] + 1].y : 1.0;
-                        xb[i] = P.row[2 * (int64_t)k[i]].x;  // kept for the update
-                        const double2 ed = s_rs[k[i]];
-                        entry_gh<MODEL>(ind, x[i], ed.x, ed.y, w, g, h);
+                        const double2 xd = s_rs[k[i]];
+                        entry_gh<MODEL>(ind, x[i], exp(xd.x), xd.y, w, g, h);
                     }
                 // the butterfly leaves the same sums in every lane
                 const double2 s = warp_sum2(make_double2(g, h));
@@ -297,7 +269,7 @@ __global__ void __launch_bounds__(kRT, 1) resident_sweep_kernel(ResidentParams R
                 const double d = s_delta[wid];
 #pragma unroll
                 for (int i = 0; i < kLanePer; ++i)
-                    if (k[i] >= 0) entry_update(P, s_rs, k[i], xb[i], x[i], d);
+                    if (k[i] >= 0) entry_update(s_rs, k[i], x[i], d);
             }
             const long long tb3 = tr ? clock64() : 0;
             __syncthreads();
@@ -346,9 +318,9 @@ __global__ void __launch_bounds__(kRT, 1) resident_sweep_kernel(ResidentParams R
     }
     // the row state back to global memory for the calls that follow
     for (int64_t k = tid; k < P.K; k += kRT) {
-        const double2 ed = s_rs[k];
-        P.row[2 * k].y = ed.x;
-        P.row[2 * k + 1].x = ed.y;
+        const double2 xd = s_rs[k];
+        P.row[2 * k] = make_double2(xd.x, exp(xd.x));
+        P.row[2 * k + 1].x = xd.y;
     }
     if (moved) atomicAdd(&P.st->nonzero_steps, moved);
 }

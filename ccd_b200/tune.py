@@ -72,10 +72,23 @@ def batch_candidates() -> Iterable[Tuple[int, int]]:
             yield g, c
 
 
+def filling(candidates, n_instances: int, n_sm: int):
+    """The candidates whose grid puts a CTA on every SM (groups x cluster >= SMs),
+    or all of them when none does.  A grid's time is its slowest group's chain
+    of sweeps (the least regularised instances take the most), and that chain
+    is shorter when the group's instances spread over more CTAs; one measured
+    sweep of the whole grid sees throughput, not that chain, and favours shapes
+    that leave SMs idle."""
+    cands = list(candidates)
+    fill = [(g, c) for g, c in cands if ((n_instances + g - 1) // g) * c >= n_sm]
+    return fill or cands
+
+
 def tune_batch(fit, variance, holdout, row_fold, args=None, candidates=None) -> BatchChoice:
     """The (group, cluster) of the mixed-precision batched engine that runs one
-    sweep of this grid fastest.  `fit` is a native.Fit (or anything with its
-    batch_find_mode); the grid is the one about to be fitted."""
+    sweep of this grid fastest among the shapes that occupy every SM.  `fit` is a
+    native.Fit (or anything with its batch_find_mode and ctx.sm_count); the grid
+    is the one about to be fitted."""
     from . import native
     var = np.asarray(variance, dtype=np.float64)
     key = ("batch", histogram_key(fit.d), int(var.shape[0]), int(getattr(fit, "precision", 0)))
@@ -85,7 +98,11 @@ def tune_batch(fit, variance, holdout, row_fold, args=None, candidates=None) -> 
     base = args or native.ModeFindingArguments()
     one = dataclasses.replace(base, max_iterations=1)
     seconds: Dict[Tuple[int, int], float] = {}
-    for g, c in (candidates or batch_candidates()):
+    n_sm = int(getattr(getattr(fit, "ctx", None), "sm_count", 0) or 0)
+    cands = list(candidates or batch_candidates())
+    if n_sm > 0:
+        cands = filling(cands, int(var.shape[0]), n_sm)
+    for g, c in cands:
         try:
             _, _, secs = fit.batch_find_mode(var, holdout, row_fold, one, group=g, cluster=c)
         except native.CcdbError:

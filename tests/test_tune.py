@@ -87,3 +87,26 @@ def test_tune_sweep_sets_the_fastest_cluster_size():
     ctx2 = StandInCtx()
     ch2 = tune.tune_sweep(ctx2, StandInFit(d, ctx2, {}))
     assert ch2.cached and ctx2.max_ctas == [8]
+
+
+def test_filling_keeps_shapes_that_occupy_every_sm():
+    cands = list(tune.batch_candidates())
+    # 200 instances on 148 SMs: 100 groups of 2 on one CTA each leave SMs idle
+    kept = tune.filling(cands, 200, 148)
+    assert (2, 1) not in kept and (4, 2) not in kept and (4, 1) not in kept
+    assert (4, 4) in kept and (2, 2) in kept and (1, 1) in kept
+    # nothing fills a tiny grid: every candidate stays
+    assert tune.filling(cands, 2, 148) == cands
+
+
+def test_tune_batch_ignores_shapes_that_leave_sms_idle():
+    d = synthetic.small(MODEL_LOGISTIC, seed=3, K=400, P=8)
+    secs = {(g, c): 1.0 for g, c in tune.batch_candidates()}
+    secs[(2, 1)] = 0.1   # fastest single sweep, but 100 CTAs on 148 SMs
+    secs[(4, 4)] = 0.5
+    f = StandInBatch(d, secs)
+    f.ctx = type("Ctx", (), {"sm_count": 148})()
+    tune.clear_cache()
+    ch = tune.tune_batch(f, np.full(200, 0.1), np.arange(200) % 10, np.zeros(d.K, int))
+    assert (ch.group, ch.cluster) == (4, 4)
+    assert (2, 1) not in ch.seconds
