@@ -117,8 +117,6 @@ Fit::~Fit() {
         ctx->release(p);
     release_schedule();
     if (group_engine()) cox_release();
-    for (cudaEvent_t e : {ev0, ev1, evc0, evc1})
-        if (e) cudaEventDestroy(e);
 }
 
 void Fit::release_schedule() {
@@ -526,15 +524,15 @@ void Fit::find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* 
         P.trace = d_trace;
         P.trace2 = d_trace + 3 * n_seg;
     }
-    check_cuda(cudaEventRecord(ev0, stream), "event");
+    check_cuda(cudaEventRecord(ctx->fev[0], stream), "event");
     if (kind == kSchedCluster) check_cuda(launch_cluster_sweep(P, sched->cluster, stream), "sweep launch");
     else check_cuda(launch_indep_sweep(P, sched->host.n_cta, stream), "sweep launch");
     ++launches;
-    check_cuda(cudaEventRecord(ev1, stream), "event");
+    check_cuda(cudaEventRecord(ctx->fev[1], stream), "event");
     DevStatus out{};
     check_cuda(cudaMemcpyAsync(&out, st, sizeof(out), cudaMemcpyDeviceToHost, stream), "status");
     check_cuda(ctx->wait(), "sweep");
-    check_cuda(cudaEventElapsedTime(ms, ev0, ev1), "elapsed");
+    check_cuda(cudaEventElapsedTime(ms, ctx->fev[0], ctx->fev[1]), "elapsed");
     if (d_trace && kind == kSchedCluster) {
         const size_t n = 4 * (size_t)sched->host.n_levels * sched->cluster;
         std::vector<unsigned long long> tr(n);
@@ -750,14 +748,14 @@ void Fit::find_mode_resident(const ccdb_mode_args& a, int* flag, int* iters, dou
         check_cuda(cudaMemsetAsync(R.trace, 0, sizeof(long long) * kResidentTraceWords * trace_n, stream), "trace");
         R.trace_n = trace_n;
     }
-    check_cuda(cudaEventRecord(ev0, stream), "event");
+    check_cuda(cudaEventRecord(ctx->fev[0], stream), "event");
     check_cuda(launch_resident_sweep(R, stream), "resident sweep launch");
     ++launches;
-    check_cuda(cudaEventRecord(ev1, stream), "event");
+    check_cuda(cudaEventRecord(ctx->fev[1], stream), "event");
     DevStatus out{};
     check_cuda(cudaMemcpyAsync(&out, st, sizeof(out), cudaMemcpyDeviceToHost, stream), "status");
     check_cuda(ctx->wait(), "resident sweep");
-    check_cuda(cudaEventElapsedTime(ms, ev0, ev1), "elapsed");
+    check_cuda(cudaEventElapsedTime(ms, ctx->fev[0], ctx->fev[1]), "elapsed");
     if (R.trace) {
         std::vector<long long> tr((size_t)kResidentTraceWords * trace_n);
         check_cuda(cudaMemcpyAsync(tr.data(), R.trace, sizeof(long long) * tr.size(), cudaMemcpyDeviceToHost, stream),
@@ -807,7 +805,7 @@ void Fit::find_mode(const ccdb_mode_args& a, double* beta_inout, ccdb_fit_result
     const int64_t launches0 = launches;
     nz_steps = 0;
     nz_known = true;
-    check_cuda(cudaEventRecord(evc0, stream), "event");
+    check_cuda(cudaEventRecord(ctx->fev[2], stream), "event");
     double bound = a.initial_bound;
     int count = 0, flag = R_FAIL, sweeps_total = 0;
     double obj = 0.0, secs = 0.0;
@@ -844,10 +842,10 @@ void Fit::find_mode(const ccdb_mode_args& a, double* beta_inout, ccdb_fit_result
     if (beta_inout)
         for (int j = 0; j < J; ++j) beta_inout[j] = beta_h[j];
     const double ll = log_likelihood();
-    check_cuda(cudaEventRecord(evc1, stream), "event");
-    check_cuda(cudaEventSynchronize(evc1), "event sync");
+    check_cuda(cudaEventRecord(ctx->fev[3], stream), "event");
+    check_cuda(cudaEventSynchronize(ctx->fev[3]), "event sync");
     float call_ms = 0.f;
-    check_cuda(cudaEventElapsedTime(&call_ms, evc0, evc1), "elapsed");
+    check_cuda(cudaEventElapsedTime(&call_ms, ctx->fev[2], ctx->fev[3]), "elapsed");
     if (res) {
         res->return_flag = flag;
         res->iterations = last_iterations;
@@ -928,6 +926,7 @@ int ccdb_context_create(int device, size_t hbm_budget_bytes, ccdb_context** out)
         check_cuda(cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep), "memory pool");
         check_cuda(cudaEventCreate(&c->ev_a), "event");
         check_cuda(cudaEventCreate(&c->ev_b), "event");
+        for (cudaEvent_t& e : c->fev) check_cuda(cudaEventCreate(&e), "event");
         *out = c;
     });
 }
@@ -939,6 +938,7 @@ int ccdb_context_destroy(ccdb_context* ctx) {
         cudaStreamSynchronize(ctx->stream);
         cudaEventDestroy(ctx->ev_a);
         cudaEventDestroy(ctx->ev_b);
+        for (cudaEvent_t e : ctx->fev) cudaEventDestroy(e);
         if (ctx->ev_wait) cudaEventDestroy(ctx->ev_wait);
         cudaStreamDestroy(ctx->stream);
         if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
@@ -955,8 +955,8 @@ int ccdb_context_set_blocking_wait(ccdb_context* ctx, int32_t on) {
         if (ctx->blocking_wait && !ctx->ev_wait)
             check_cuda(cudaEventCreateWithFlags(&ctx->ev_wait, cudaEventBlockingSync | cudaEventDisableTiming),
                        "event");
-        // the one-call fit's timing events follow the setting (fits made later do too)
-        for (cudaEvent_t* e : {&ctx->ev_a, &ctx->ev_b}) {
+        // the context's timing events follow the setting
+        for (cudaEvent_t* e : {&ctx->ev_a, &ctx->ev_b, &ctx->fev[0], &ctx->fev[1], &ctx->fev[2], &ctx->fev[3]}) {
             if (*e) check_cuda(cudaEventDestroy(*e), "event");
             check_cuda(cudaEventCreateWithFlags(e, ctx->event_flags()), "event");
         }
@@ -1096,10 +1096,6 @@ int ccdb_fit_create(ccdb_context* ctx, const ccdb_matrix* m, const ccdb_fit_desc
         f->w = static_cast<double*>(ctx->alloc(sizeof(double) * K));
         f->gh_parts = static_cast<double2*>(ctx->alloc(sizeof(double2) * Fit::kGhParts));
         f->gh_out = static_cast<double2*>(ctx->alloc(sizeof(double2)));
-        check_cuda(cudaEventCreateWithFlags(&f->ev0, ctx->event_flags()), "event");
-        check_cuda(cudaEventCreateWithFlags(&f->ev1, ctx->event_flags()), "event");
-        check_cuda(cudaEventCreateWithFlags(&f->evc0, ctx->event_flags()), "event");
-        check_cuda(cudaEventCreateWithFlags(&f->evc1, ctx->event_flags()), "event");
         // CyclicCoordinateDescent::init (.cpp:200-239)
         f->beta_h.assign(J, 0.0);
         f->fixed.assign(J, 0);

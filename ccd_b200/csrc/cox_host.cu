@@ -384,16 +384,16 @@ void Fit::find_mode_group_sweep(const ccdb_mode_args& a, int* flag, int* iters, 
         Q.trace = d_trace;
         Q.trace_steps = trace_steps;
     }
-    check_cuda(cudaEventRecord(ev0, stream), "event");
+    check_cuda(cudaEventRecord(ctx->fev[0], stream), "event");
     check_cuda(launch_group_sweep(Q, n_cta, use_cluster, stream), "group sweep launch");
     ++launches;
-    check_cuda(cudaEventRecord(ev1, stream), "event");
+    check_cuda(cudaEventRecord(ctx->fev[1], stream), "event");
     DevStatus out{};
     int64_t cnt[2] = {0, 0};
     check_cuda(cudaMemcpyAsync(&out, st, sizeof(out), cudaMemcpyDeviceToHost, stream), "status");
     check_cuda(cudaMemcpyAsync(cnt, cox.counters, sizeof(cnt), cudaMemcpyDeviceToHost, stream), "counters");
     check_cuda(ctx->wait(), "group sweep");
-    check_cuda(cudaEventElapsedTime(ms, ev0, ev1), "elapsed");
+    check_cuda(cudaEventElapsedTime(ms, ctx->fev[0], ctx->fev[1]), "elapsed");
     if (d_trace) {
         std::vector<unsigned long long> tr(kTraceStamps * (size_t)trace_steps);
         check_cuda(cudaMemcpy(tr.data(), d_trace, sizeof(unsigned long long) * tr.size(), cudaMemcpyDeviceToHost),

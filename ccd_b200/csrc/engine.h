@@ -45,6 +45,11 @@ struct Context {
     std::mutex mu;
     std::map<void*, size_t> sizes;
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;  // around a one-call fit
+    // timing events of this context's fits (their calls are serialised on its
+    // stream): [0], [1] around the sweep launches, [2], [3] around a whole
+    // findMode.  Made once: creating and destroying events per fit waited on
+    // other streams' work while they ran
+    cudaEvent_t fev[4] = {nullptr, nullptr, nullptr, nullptr};
     // host waits: spin (default) or sleep until the device signals (blocking_wait),
     // for processes that run many contexts' calls at once (serving slots)
     bool blocking_wait = false;
@@ -158,8 +163,6 @@ struct Fit {
     double* w = nullptr;
     double2* gh_parts = nullptr;
     double2* gh_out = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;    // around the sweep launches
-    cudaEvent_t evc0 = nullptr, evc1 = nullptr;  // around a whole find_mode
     int64_t launches = 0;                        // engine kernels launched so far
     double last_call_seconds = 0.0;              // device time of the last fisher_information passes
     int last_iterations = 0;                     // getIterationCount: the last findMode's cycles

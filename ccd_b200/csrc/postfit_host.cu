@@ -61,7 +61,7 @@ void Fit::fisher_information(const int32_t* idx, int n, double* out) {
     P.idx = d_idx;
     P.n = n;
     P.out = s.get<double>((size_t)n * n);
-    check_cuda(cudaEventRecord(evc0, stream), "event");
+    check_cuda(cudaEventRecord(ctx->fev[2], stream), "event");
     for (int p0 = 0; p0 < n; p0 += kFisherSlots) {
         const int ns = std::min(kFisherSlots, n - p0);
         int64_t most = 0;
@@ -72,12 +72,12 @@ void Fit::fisher_information(const int32_t* idx, int n, double* out) {
         check_cuda(launch_fisher_gather(P, p0, ns, stream), "fisher gather");
         launches += 2;
     }
-    check_cuda(cudaEventRecord(evc1, stream), "event");
+    check_cuda(cudaEventRecord(ctx->fev[3], stream), "event");
     check_cuda(cudaMemcpyAsync(out, P.out, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToHost, stream),
                "fisher copy");
     check_cuda(ctx->wait(), "fisher sync");
     float ms = 0.f;
-    check_cuda(cudaEventElapsedTime(&ms, evc0, evc1), "elapsed");
+    check_cuda(cudaEventElapsedTime(&ms, ctx->fev[2], ctx->fev[3]), "elapsed");
     last_call_seconds = ms * 1e-3;
 }
 

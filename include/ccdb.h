@@ -66,7 +66,8 @@ int ccdb_context_sm_count(const ccdb_context* ctx, int32_t* n_sm);
  * of spinning (cudaEventBlockingSync).  Off by default: a spinning wait
  * returns sooner, but a process that runs many contexts' calls at once (one
  * per serving slot) starves its own host threads when every waiting thread
- * spins.  Affects fits made after the call.  No reference counterpart. */
+ * spins.  Call it between calls of the context's fits (it remakes the
+ * context's timing events).  No reference counterpart. */
 int ccdb_context_set_blocking_wait(ccdb_context* ctx, int32_t on);
 
 /* Persistent sweep kernels launched by this context's fits use at most
