@@ -11,6 +11,16 @@ breakdown by segment kind.
 engine: CTA 0's SM clock at six points of every column of one sweep
 (``CCDB_BATCH_TRACE_SWEEP``, default 1).  ``python -m ccd_b200.trace --batch
 <path> [sm_mhz]`` prints the per-phase breakdown.
+
+The default sweeps write their own formats to the same ``CCDB_TRACE_FILE``
+(the last findMode of the process wins):
+
+* ``--cluster <path>``: the cluster sweep, per level and CTA of the first
+  sweep the global timer at entry, opening, end of phase A and release;
+* ``--group <path>``: the group sweep (Cox), CTA 0's global timer at eight
+  points of each of the first 4,096 nonzero steps;
+* ``--resident <path> [sm_mhz]``: the resident sweep, SM clock stamps of the
+  first 4,096 batches.
 """
 from __future__ import annotations
 
@@ -91,8 +101,69 @@ def summarise_batch(path: str, sm_mhz: float = 1965.0) -> str:
     return "\n".join(out)
 
 
+def summarise_cluster(path: str) -> str:
+    """Level timing of the cluster sweep's first sweep."""
+    raw = open(path, "rb").read()
+    nl, C = (int(v) for v in np.frombuffer(raw[:16], np.int64))
+    rest = len(raw) - 16
+    J = (rest - nl - 32 * nl * C) // 4
+    off = 16 + 4 * J
+    split = np.frombuffer(raw[off:off + nl], np.uint8)
+    off += nl
+    tr = np.frombuffer(raw[off:], np.uint64).reshape(nl, C, 4).astype(np.int64)
+    entry, opened, done_a, rel = (tr[..., i] for i in range(4))
+    period = np.diff(opened.max(axis=1)) / 1e3
+    phase_a = (done_a - opened).max(axis=1) / 1e3
+    lag = (opened[1:].max(axis=1) - rel[:-1].max(axis=1)) / 1e3
+    plain = split[:-1] == 0
+    lines = [f"levels {nl}, CTAs {C}, split levels {int(split.sum())}",
+             f"level period median {np.median(period):.2f} us (plain {np.median(period[plain]):.2f}, "
+             f"split {np.median(period[~plain]) if (~plain).any() else 0:.2f})",
+             f"slowest CTA's phase A median {np.median(phase_a):.2f} us",
+             f"last release to every CTA opened median {np.median(lag):.2f} us",
+             f"sweep {(rel.max() - opened.min()) / 1e3:.1f} us"]
+    return "\n".join(lines)
+
+
+def summarise_group(path: str) -> str:
+    """Per-stage timing of the group sweep's nonzero steps (Cox)."""
+    t = np.fromfile(path, dtype=np.uint64).reshape(-1, 8).astype(np.int64)
+    t = t[t[:, 0] > 0]
+    d = np.diff(t, axis=1) / 1e3
+    names = ["gradients of the batch + barrier", "rows + barrier", "denominators + barrier",
+             "rebuild phase 1 + barrier", "rebuild phase 2 + barrier", "rebuild phase 3 + barrier"]
+    lines = [f"nonzero steps traced {len(t)}"]
+    lines += [f"{n}: median {np.median(d[:, i]):.2f} us" for i, n in enumerate(names)]
+    lines.append(f"one nonzero step: median {np.median(np.diff(t[:, 0])) / 1e3:.2f} us")
+    return "\n".join(lines)
+
+
+def summarise_resident(path: str, sm_mhz: float = 1965.0) -> str:
+    """Per-batch timing of the resident sweep."""
+    t = np.fromfile(path, dtype=np.int64).reshape(-1, 8)
+    t = t[t[:, 0] != 0]
+    long_col = t[:, 5] == -1
+    b = t[~long_col]
+    us = lambda x: x / sm_mhz
+    lines = [f"batches {len(b)}, long columns {int(long_col.sum())}, "
+             f"batches ending at a nonzero step {int((b[:, 6] < b[:, 5]).sum())}",
+             f"batch median {np.median(us(b[:, 4] - b[:, 0])):.2f} us: gradients "
+             f"{np.median(us(b[:, 1] - b[:, 0])):.2f}, decision {np.median(us(b[:, 2] - b[:, 1])):.2f}, "
+             f"update {np.median(us(b[:, 3] - b[:, 2])):.2f}, barrier {np.median(us(b[:, 4] - b[:, 3])):.2f}"]
+    if long_col.any():
+        L = t[long_col]
+        lines.append(f"long column median {np.median(us(L[:, 4] - L[:, 0])):.2f} us")
+    return "\n".join(lines)
+
+
 if __name__ == "__main__":
     if sys.argv[1] == "--batch":
         print(summarise_batch(sys.argv[2], *(float(a) for a in sys.argv[3:4])))
+    elif sys.argv[1] == "--cluster":
+        print(summarise_cluster(sys.argv[2]))
+    elif sys.argv[1] == "--group":
+        print(summarise_group(sys.argv[2]))
+    elif sys.argv[1] == "--resident":
+        print(summarise_resident(sys.argv[2], *(float(a) for a in sys.argv[3:4])))
     else:
         print(summarise(sys.argv[1]))
