@@ -73,8 +73,22 @@ def estimate_bytes(d: CyclopsData) -> int:
     return 2 * core + (64 << 20)
 
 
+def is_small(d: CyclopsData, max_entries: int) -> bool:
+    """A request the fast lane may take: at most max_entries matrix entries
+    (dense-like columns count K each)."""
+    return int(d.nnz) <= max_entries
+
+
 class Server:
-    """`slots` concurrent fits under an HBM budget of `hbm_budget` bytes.
+    """`slots` concurrent fits under an HBM budget of `hbm_budget` bytes, plus
+    `fast_slots` slots that take only small requests (at most `fast_entries`
+    matrix entries).
+
+    The general slots take requests in arrival order (no overtaking).  A fast
+    slot takes the oldest pending small request, ahead of any large one: a
+    small fit takes milliseconds, a large one seconds, and without the lane a
+    burst of large requests holds every slot while the small ones queue.
+    Within each class the order of arrival is kept.
 
     ``fit_fn(slot, request, slot_state) -> (beta, flag, iterations, loglik)``
     runs one fit (`slot_state` is the slot thread's own attribute holder); the
@@ -83,10 +97,12 @@ class Server:
     """
 
     def __init__(self, device: int = 0, hbm_budget: float = 150e9, slots: int = 8,
-                 fit_fn: Optional[Callable] = None):
+                 fit_fn: Optional[Callable] = None, fast_slots: int = 0, fast_entries: int = 200_000):
         self.device = device
         self.budget = int(hbm_budget)
         self.n_slots = slots
+        self.n_fast = fast_slots
+        self.fast_entries = int(fast_entries)
         self._fit_fn = fit_fn or self._gpu_fit
         self._cv = threading.Condition()
         self._pending: collections.deque = collections.deque()
@@ -96,7 +112,8 @@ class Server:
         self.peak_reserved = 0
         self.peak_running = 0
         self.done: List[Completed] = []
-        self._threads = [threading.Thread(target=self._worker, args=(i,), daemon=True) for i in range(slots)]
+        self._threads = [threading.Thread(target=self._worker, args=(i,), daemon=True)
+                         for i in range(slots + fast_slots)]
         for t in self._threads:
             t.start()
 
@@ -130,20 +147,34 @@ class Server:
             t.join()
 
     # -- the slots
+    def _next(self, fast: bool):
+        """Index of the request this slot may admit now, or None."""
+        if not fast:
+            if self._pending and self._reserved + self._pending[0].bytes <= self.budget:
+                return 0  # the oldest request fits: admit it (arrival order)
+            return None
+        for i, r in enumerate(self._pending):  # the oldest small request that fits
+            if is_small(r.data, self.fast_entries):
+                return i if self._reserved + r.bytes <= self.budget else None
+        return None
+
     def _worker(self, slot: int) -> None:
         local = threading.local()
+        fast = slot >= self.n_slots
         while True:
             with self._cv:
                 while True:
-                    if self._pending and self._reserved + self._pending[0].bytes <= self.budget:
-                        break  # the oldest request fits: admit it (arrival order, no overtaking)
+                    i = self._next(fast)
+                    if i is not None:
+                        break
                     if self._stop and not self._pending:
                         ctx = getattr(local, "ctx", None)
                         if ctx is not None:
                             ctx.close()
                         return
                     self._cv.wait()
-                req = self._pending.popleft()
+                req = self._pending[i]
+                del self._pending[i]
                 self._reserved += req.bytes
                 self._running += 1
                 self.peak_reserved = max(self.peak_reserved, self._reserved)
@@ -165,7 +196,10 @@ class Server:
         from . import native
         if not hasattr(local, "ctx"):
             local.ctx = native.Context(self.device)
-            local.ctx.set_max_ctas(max(1, local.ctx.sm_count // self.n_slots))
+            n = local.ctx.sm_count
+            # general slots share the SMs; a fast slot's small fits take one CTA
+            # (the resident sweep) or a small cluster
+            local.ctx.set_max_ctas(4 if slot >= self.n_slots else max(1, n // self.n_slots))
             local.ctx.set_blocking_wait(True)  # slots wait without spinning the host cores
         args = req.args or native.ModeFindingArguments()
         r = native.fit_model(local.ctx, req.data, args)

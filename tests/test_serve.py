@@ -95,3 +95,39 @@ def test_latency_summary_and_stream_shape():
         srv.close()
     s = serve.latency_summary(done)
     assert s["requests"] == 12 and s["failed"] == 0 and s["p99_s"] >= s["p50_s"] > 0
+
+
+def test_fast_lane_takes_small_requests_ahead_of_large_ones():
+    """One general slot busy with a queue of large requests; the fast slot
+    serves the small requests that arrived after them, in their own arrival
+    order, and never takes a large one."""
+    taken = []
+    lock = threading.Lock()
+
+    def fit(slot, req, local):
+        with lock:
+            taken.append((slot, req.rid))
+        time.sleep(0.15 if req.data.nnz > 400 else 0.005)
+        return np.zeros(3), 0, 1, -1.0
+
+    big = [serve.Request(i, synthetic.small(MODEL_LOGISTIC, seed=i, K=2000, P=10, density=0.1), bytes=1)
+           for i in range(3)]
+    small = [serve.Request(10 + i, synthetic.small(MODEL_LOGISTIC, seed=10 + i, K=50, P=3), bytes=1)
+             for i in range(4)]
+    assert all(r.data.nnz > 400 for r in big) and all(r.data.nnz <= 400 for r in small)
+    srv = serve.Server(hbm_budget=1e9, slots=1, fast_slots=1, fast_entries=400, fit_fn=fit)
+    try:
+        for r in big + small:
+            srv.submit(r)
+        done = srv.drain(7, timeout=30)
+    finally:
+        srv.close()
+    by_rid = {c.rid: c for c in done}
+    # every small request finished before the last large one
+    assert max(by_rid[r.rid].end for r in small) < max(by_rid[r.rid].end for r in big)
+    # the fast slot (slot 1) took only small requests, in arrival order
+    fast = [rid for s, rid in taken if s == 1]
+    assert fast and all(rid >= 10 for rid in fast) and fast == sorted(fast)
+    # the general slot kept arrival order over what it took
+    general = [rid for s, rid in taken if s == 0]
+    assert general == sorted(general)
