@@ -1081,6 +1081,8 @@ def run_serve(args, world, rank, local, collect=False):
                    for k, v in sorted(svc.items())}
         errors = collections.Counter(
             f"model {int(stream[c.rid][1].model_type)}: {c.error[:160]}" for c in done if c.error)
+        # the requests the reference arm's sample serves, within this whole replay
+        head = np.array([c.latency for c in done if c.rid < SERVE_REF_REQUESTS])
         clk = clocks.stop()
         peak = srv.peak_running
     finally:
@@ -1100,6 +1102,10 @@ def run_serve(args, world, rank, local, collect=False):
         "p99_s": s["p99_s"], "mean_s": s["mean_s"], "fits_per_s": s["fits_per_s"],
         "failed": s["failed"], "errors": dict(errors.most_common(5)), "peak_concurrent_fits": peak,
         "service_by_model": service,
+        "first_requests": {"n": int(head.size), "p50_s": float(np.percentile(head, 50)),
+                           "p99_s": float(np.percentile(head, 99)),
+                           "note": "the first requests of the trace (the reference arm's sample), "
+                                   "served within the whole replay"},
         "e2e": {"value": s["p50_s"], "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "roofline": None, "cpu_baseline": cpu, "gpu_launches": None, "clocks": clk,
     }
