@@ -282,7 +282,7 @@ void Fit::ensure_schedule(int kind) {
         sp.warps_per_cta = indep_threads() / 32;
         sp.warp_max = 128;   // warp tasks stage 4 entries per lane
         sp.cta_max = 4096;   // CTA tasks and chunks stage 8 entries per thread
-        sp.chunk = 4096;
+        sp.chunk = 1024;     // split columns: chunks of ~1024 entries spread a long column over more CTAs
         std::vector<int64_t> entries(J);
         for (int j = 0; j < J; ++j) entries[j] = m->entries(j);
         auto s = std::make_unique<DevSchedule>();
