@@ -325,6 +325,113 @@ __device__ bool cox_rebuild(const GroupSweepParams& Q, unsigned& epoch, int32_t*
     return sync_all<CL>(Q, epoch, s_fail);
 }
 
+// The staged rebuild: a CTA whose group range holds at most kStageCap groups
+// copies the range's inputs into shared memory with coalesced loads (one group
+// per thread a step) once, walks its thread-contiguous shares there, and
+// writes D, S1, S2 back with coalesced stores.  The direct form above reads
+// and writes a thread's contiguous share straight from global memory: each
+// warp access then touches 32 lines, and the CTA's load/store transactions,
+// not bytes, bound it.
+constexpr int kStageCap = 6144;
+struct RbStage {
+    double a[kStageCap];   // denominators, then D, then S1
+    double b[kStageCap];   // nEv, then S2
+    int32_t f[kStageCap];  // gfirst
+    int32_t g[kStageCap];  // glast
+};
+
+template <bool CL>
+__device__ bool cox_rebuild_staged(const GroupSweepParams& Q, unsigned& epoch, int32_t* s_fail, Seg3* s_w,
+                                   Seg3* s_tot, Seg3* s_carry, RbStage& T, unsigned long long* trc) {
+    const CoxParams& P = Q.P;
+    const int64_t G = gridDim.x, b = blockIdx.x;
+    const int tid = threadIdx.x;
+    const int64_t g0 = P.N * b / G, g1 = P.N * (b + 1) / G;
+    const int n = (int)(g1 - g0);
+    int64_t a0, a1;
+    thread_share(0, n, a0, a1);  // this thread's contiguous share, as offsets into the range
+    const int t0 = (int)a0, t1 = (int)a1;
+
+    // phase 1: the range's inputs into shared memory; the CTA's prefix aggregate
+    for (int i = tid; i < n; i += kT) {
+        T.f[i] = P.gfirst[g0 + i];
+        T.a[i] = P.denom[g0 + i];
+        T.g[i] = P.glast[g0 + i];
+        T.b[i] = P.nEv[g0 + i];
+    }
+    __syncthreads();
+    Seg3 mine{0, 0.0, 0.0};
+    for (int i = t0; i < t1; ++i) {
+        const Seg3 e{T.f[i], T.a[i], 0.0};
+        mine = (i == t0) ? e : seg3_combine(mine, e);
+    }
+    block_excl_scan3<false>(mine, s_w, s_tot);
+    if (tid == 0) {
+        __stcg(&Q.agg[b].f, s_tot->f);
+        __stcg(&Q.agg[b].v0, s_tot->a);
+    }
+    if (!sync_all<CL>(Q, epoch, s_fail)) return false;
+    if (trc) trc[4] = global_ns();
+
+    // phase 2: carry-in from the CTAs before, D of the range; suffix aggregates
+    if (tid < 32) {
+        const Seg3 c = warp_agg_combine<false>(Q.agg, 0, b, false);
+        if (tid == 0) *s_carry = c;
+    }
+    __syncthreads();
+    const Seg3 pre = block_excl_scan3<false>(mine, s_w, s_tot);
+    {
+        Seg3 run = (b == 0) ? pre : (tid == 0 ? *s_carry : seg3_combine(*s_carry, pre));
+        const bool has_run = (b > 0) || (tid > 0);
+        Seg3 rs{0, 0.0, 0.0};  // the share's suffix aggregate: each group is the highest so far
+        for (int i = t0; i < t1; ++i) {
+            const Seg3 e{T.f[i], T.a[i], 0.0};
+            run = (!has_run && i == t0) ? e : seg3_combine(run, e);
+            const double D = run.a;
+            T.a[i] = D;
+            const double ne = T.b[i];
+            const Seg3 r{T.g[i], ne / D, ne / (D * D)};
+            rs = (i == t0) ? r : seg3_combine(r, rs);
+        }
+        mine = rs;
+    }
+    block_excl_scan3<true>(mine, s_w, s_tot);  // its barriers also order the D written above
+    if (tid == 0) {
+        __stcg(&Q.agg[G + b].f, s_tot->f);
+        __stcg(&Q.agg[G + b].v0, s_tot->a);
+        __stcg(&Q.agg[G + b].v1, s_tot->b);
+    }
+    for (int i = tid; i < n; i += kT) __stcg(P.D + g0 + i, T.a[i]);
+    if (!sync_all<CL>(Q, epoch, s_fail)) return false;
+    if (trc) trc[5] = global_ns();
+
+    // phase 3: carry-in from the CTAs after (suffix direction), S1 and S2 of the range
+    if (tid < 32) {
+        const Seg3 c = warp_agg_combine<true>(Q.agg + G, b + 1, G, true);
+        if (tid == 0) *s_carry = c;
+    }
+    __syncthreads();
+    const Seg3 suf = block_excl_scan3<true>(mine, s_w, s_tot);
+    {
+        const bool last_cta = (b == G - 1);
+        Seg3 run = last_cta ? suf : (tid == kT - 1 ? *s_carry : seg3_combine(*s_carry, suf));
+        const bool has_run = !last_cta || (tid < kT - 1);
+        for (int i = t1 - 1; i >= t0; --i) {
+            const double D = T.a[i], ne = T.b[i];
+            const Seg3 e{T.g[i], ne / D, ne / (D * D)};
+            run = (!has_run && i == t1 - 1) ? e : seg3_combine(run, e);
+            T.a[i] = run.a;
+            T.b[i] = run.b;
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += kT) {
+        __stcg(P.S1 + g0 + i, T.a[i]);
+        __stcg(P.S2 + g0 + i, T.b[i]);
+    }
+    return sync_all<CL>(Q, epoch, s_fail);
+}
+
 // This CTA's objective partials {LL numerator, LL denominator, gradient
 // objective, log prior} (ModelSpecifics.hpp:103-120, 605-650; JointPrior.h:121-128).
 template <bool COX>
@@ -390,6 +497,7 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
     __shared__ int32_t s_first;
     __shared__ double s_delta, s_newbeta;
     __shared__ double s_pend_hd[kGroupBatchMax];  // CTA 0: bounds of the last decision
+    extern __shared__ __align__(16) unsigned char s_dyn[];  // Cox: the staged rebuild's range (RbStage)
 
     const CoxParams& P = Q.P;
     const int tid = threadIdx.x;
@@ -535,7 +643,13 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
                 if (!barrier()) return;
                 if (trc) trc[3] = global_ns();
             }
-            if (COX && !cox_rebuild<CL>(Q, epoch, &s_fail, s_w3, &s_tot, &s_carry, trc)) return;
+            if (COX) {
+                const bool ok = ((P.N + G - 1) / G <= kStageCap)
+                                    ? cox_rebuild_staged<CL>(Q, epoch, &s_fail, s_w3, &s_tot, &s_carry,
+                                                             *reinterpret_cast<RbStage*>(s_dyn), trc)
+                                    : cox_rebuild<CL>(Q, epoch, &s_fail, s_w3, &s_tot, &s_carry, trc);
+                if (!ok) return;
+            }
             if (trc) trc[6] = global_ns();
             pos += first + 1;
             if (trc) {
@@ -589,8 +703,28 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
 
 int group_sweep_threads() { return kT; }
 
+// The Cox kernels hold the staged rebuild's range in dynamic shared memory;
+// the limit is raised, and the cluster-size attribute set, once per device.
+cudaError_t group_sweep_attrs() {
+    static std::atomic<uint64_t> done{0};
+    return once_per_device(done, [] {
+        for (const void* fn : {(const void*)group_sweep_kernel<true, false>, (const void*)group_sweep_kernel<true, true>}) {
+            cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RbStage));
+            if (e != cudaSuccess) return e;
+        }
+        for (const void* fn : {(const void*)group_sweep_kernel<true, true>, (const void*)group_sweep_kernel<false, true>}) {
+            cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    });
+}
+
 cudaError_t group_sweep_occupancy(int* blocks_per_sm) {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, group_sweep_kernel<true, false>, kT, 0);
+    cudaError_t e = group_sweep_attrs();
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, group_sweep_kernel<true, false>, kT,
+                                                         sizeof(RbStage));
 }
 
 namespace {
@@ -610,18 +744,18 @@ cudaLaunchConfig_t cluster_cfg(int c, cudaStream_t stream, cudaLaunchAttribute* 
 }  // namespace
 
 // The largest cluster (16, 8, 4, 2) of the cluster form of which one can be
-// resident; 0 if none.  Sets the kernels' cluster attribute once.
+// resident; 0 if none.
 cudaError_t group_sweep_max_cluster(int* cluster) {
     *cluster = 0;
-    for (const void* fn : {(const void*)group_sweep_kernel<true, true>, (const void*)group_sweep_kernel<false, true>}) {
-        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-        if (e != cudaSuccess) return e;
-    }
+    cudaError_t e0 = group_sweep_attrs();
+    if (e0 != cudaSuccess) return e0;
     for (int c = kMaxGroupCluster; c >= 2; c /= 2) {
         cudaLaunchAttribute attr[1];
-        const cudaLaunchConfig_t cfg = cluster_cfg(c, 0, attr);
+        cudaLaunchConfig_t cfg = cluster_cfg(c, 0, attr);
         int n = 0, n2 = 0;
+        cfg.dynamicSmemBytes = sizeof(RbStage);
         cudaError_t e = cudaOccupancyMaxActiveClusters(&n, group_sweep_kernel<true, true>, &cfg);
+        cfg.dynamicSmemBytes = 0;
         if (e == cudaSuccess) e = cudaOccupancyMaxActiveClusters(&n2, group_sweep_kernel<false, true>, &cfg);
         if (e != cudaSuccess) {
             cudaGetLastError();  // a size the device rejects: try the next one
@@ -636,15 +770,19 @@ cudaError_t group_sweep_max_cluster(int* cluster) {
 }
 
 cudaError_t launch_group_sweep(const GroupSweepParams& Q, int n_cta, bool cluster, cudaStream_t stream) {
+    cudaError_t e = group_sweep_attrs();
+    if (e != cudaSuccess) return e;
+    const size_t smem = Q.cox ? sizeof(RbStage) : 0;
     if (cluster) {
         cudaLaunchAttribute attr[1];
-        const cudaLaunchConfig_t cfg = cluster_cfg(n_cta, stream, attr);
+        cudaLaunchConfig_t cfg = cluster_cfg(n_cta, stream, attr);
+        cfg.dynamicSmemBytes = smem;
         if (Q.cox) return cudaLaunchKernelEx(&cfg, group_sweep_kernel<true, true>, Q);
         return cudaLaunchKernelEx(&cfg, group_sweep_kernel<false, true>, Q);
     }
     void* args[] = {(void*)&Q};
     const void* fn = Q.cox ? (const void*)group_sweep_kernel<true, false> : (const void*)group_sweep_kernel<false, false>;
-    return cudaLaunchCooperativeKernel(fn, dim3(n_cta), dim3(kT), args, 0, stream);
+    return cudaLaunchCooperativeKernel(fn, dim3(n_cta), dim3(kT), args, smem, stream);
 }
 
 }  // namespace ccdb

@@ -136,3 +136,23 @@ def test_cox_mixed_precision_against_fp64_oracle(gpu_ctx, oracle_engine, kw):
     print(f"mixed Cox: max relative coefficient error {err:.2e}")
     assert err <= 1e-6
     assert abs(got.log_likelihood - want["loglik"]) <= 1e-8 * abs(want["loglik"])
+
+
+@pytest.mark.parametrize("form", [native.SWEEP_LEVELS, native.SWEEP_GRID_LEVELS])
+def test_cox_device_sweep_direct_rebuild_on_two_ctas(oracle_engine, form):
+    """Two CTAs for about 45,000 groups: each CTA's group range is larger than
+    the staged rebuild holds in shared memory, so the risk-set sums are rebuilt
+    straight from global memory (the direct form)."""
+    d = synthetic.small(MODEL_COX, seed=12, K=60_000, P=120, density=0.004, n_strata=150, tie_days=4,
+                        formats=("indicator",), prior=PRIOR_LAPLACE, variance=0.05)
+    want = oracle_engine(d).fit(GRADIENT, 1e-6)
+    ctx = native.Context(0)
+    ctx.set_max_ctas(2)
+    try:
+        got = native.fit_model(ctx, d, native.ModeFindingArguments(convergence_type=GRADIENT, strategy=form))
+    finally:
+        ctx.close()
+    assert got.return_flag == want["flag"]
+    assert got.iterations == want["iterations"]
+    assert rel_beta(got.beta, want["beta"]) <= BETA_TOL
+    assert abs(got.log_likelihood - want["loglik"]) <= LL_TOL * abs(want["loglik"])
