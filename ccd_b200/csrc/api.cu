@@ -529,6 +529,10 @@ void Fit::find_mode_once(const ccdb_mode_args& a, double bound, int* flag, int* 
     else check_cuda(launch_indep_sweep(P, sched->host.n_cta, stream), "sweep launch");
     ++launches;
     check_cuda(cudaEventRecord(ctx->fev[1], stream), "event");
+    // the host waits for the sweep before it queues the copy back: a device-to-host
+    // copy queued behind a long kernel held up the copies of other contexts'
+    // streams, so fits served side by side finished together with the longest one
+    check_cuda(ctx->wait(), "sweep");
     DevStatus out{};
     check_cuda(cudaMemcpyAsync(&out, st, sizeof(out), cudaMemcpyDeviceToHost, stream), "status");
     check_cuda(ctx->wait(), "sweep");
@@ -752,6 +756,7 @@ void Fit::find_mode_resident(const ccdb_mode_args& a, int* flag, int* iters, dou
     check_cuda(launch_resident_sweep(R, stream), "resident sweep launch");
     ++launches;
     check_cuda(cudaEventRecord(ctx->fev[1], stream), "event");
+    check_cuda(ctx->wait(), "resident sweep");  // the sweep is done before a copy is queued behind it
     DevStatus out{};
     check_cuda(cudaMemcpyAsync(&out, st, sizeof(out), cudaMemcpyDeviceToHost, stream), "status");
     check_cuda(ctx->wait(), "resident sweep");
@@ -1527,6 +1532,7 @@ int ccdb_batch_find_mode(ccdb_fit* f, const ccdb_batch_desc* b, const ccdb_mode_
         if (mixed) check_cuda(launch_batch_mixed(P, s), "batch sweep (mixed)");
         else check_cuda(launch_batch_sweep(P, s), "batch sweep");
         check_cuda(cudaEventRecord(e1, s), "event");
+        check_cuda(f->ctx->wait(), "batch sync");  // the sweep is done before a copy is queued behind it
         std::vector<BatchResult> res(n);
         check_cuda(cudaMemcpyAsync(res.data(), P.results, sizeof(BatchResult) * n, cudaMemcpyDeviceToHost, s),
                    "results");

@@ -325,7 +325,7 @@ void Fit::find_mode_group_sweep(const ccdb_mode_args& a, int* flag, int* iters, 
                       work <= (int64_t)ctx->group_cluster * kGroupClusterWork;
         if (use_cluster) {
             int c = ctx->group_cluster;
-            while (c > 2 && c > n_cta) c /= 2;
+            while (c > 1 && c > n_cta) c /= 2;
             n_cta = c;
         }
     }
@@ -388,6 +388,7 @@ void Fit::find_mode_group_sweep(const ccdb_mode_args& a, int* flag, int* iters, 
     check_cuda(launch_group_sweep(Q, n_cta, use_cluster, stream), "group sweep launch");
     ++launches;
     check_cuda(cudaEventRecord(ctx->fev[1], stream), "event");
+    check_cuda(ctx->wait(), "group sweep");  // the sweep is done before a copy is queued behind it
     DevStatus out{};
     int64_t cnt[2] = {0, 0};
     check_cuda(cudaMemcpyAsync(&out, st, sizeof(out), cudaMemcpyDeviceToHost, stream), "status");

@@ -524,9 +524,15 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
     double last, ll, lp;
     if (!objective_all<COX, CL>(Q, epoch, &s_fail, s_red4, last, ll, lp)) return;
 
+    // a batch opens with at most one column per CTA (and at most 32): a CTA's
+    // columns are evaluated one after another, and after a nonzero step the
+    // next one usually comes within a few columns, so a wider opening batch on
+    // a few CTAs mostly computes gradients that are thrown away; a batch of
+    // zero steps doubles the next one
+    const int batch0 = (int)min((int64_t)32, G);
     int iteration = 0;
     for (int it = 0; it < Q.max_iter; ++it) {
-        int pos = 0, batch = 32;
+        int pos = 0, batch = batch0;
         while (pos < Q.n_active) {
             const int nb = min(batch, Q.n_active - pos);
             // optional timestamps of the first nonzero steps (CTA 0): batch start, decided,
@@ -657,7 +663,7 @@ __global__ void __launch_bounds__(kT, 1) group_sweep_kernel(GroupSweepParams Q) 
                 trc += kTraceStamps;
                 if (--trn <= 0) trc = nullptr;
             }
-            batch = 32;
+            batch = batch0;
         }
         // the sweep is complete: held-back writes land, then the objective
         if (!barrier()) return;

@@ -82,7 +82,7 @@ def is_small(d: CyclopsData, max_entries: int) -> bool:
 class Server:
     """`slots` concurrent fits under an HBM budget of `hbm_budget` bytes, plus
     `fast_slots` slots that take only small requests (at most `fast_entries`
-    matrix entries).
+    matrix entries) on at most `fast_ctas` CTAs each.
 
     The general slots take requests in arrival order (no overtaking).  A fast
     slot takes the oldest pending small request, ahead of any large one: a
@@ -97,12 +97,14 @@ class Server:
     """
 
     def __init__(self, device: int = 0, hbm_budget: float = 150e9, slots: int = 8,
-                 fit_fn: Optional[Callable] = None, fast_slots: int = 0, fast_entries: int = 200_000):
+                 fit_fn: Optional[Callable] = None, fast_slots: int = 0, fast_entries: int = 200_000,
+                 fast_ctas: int = 1):
         self.device = device
         self.budget = int(hbm_budget)
         self.n_slots = slots
         self.n_fast = fast_slots
         self.fast_entries = int(fast_entries)
+        self.fast_ctas = max(1, int(fast_ctas))
         self._fit_fn = fit_fn or self._gpu_fit
         self._cv = threading.Condition()
         self._pending: collections.deque = collections.deque()
@@ -161,6 +163,11 @@ class Server:
     def _worker(self, slot: int) -> None:
         local = threading.local()
         fast = slot >= self.n_slots
+        if self._fit_fn == self._gpu_fit:  # the slot's context exists before its first request
+            try:
+                self._gpu_slot_init(slot, local)
+            except Exception:  # retried by the first request, which then fails with the error
+                local.__dict__.pop("ctx", None)
         while True:
             with self._cv:
                 while True:
@@ -192,15 +199,22 @@ class Server:
                 self.done.append(Completed(req.rid, beta, flag, iters, ll, req.arrival, start, end, slot, err))
                 self._cv.notify_all()
 
+    def _gpu_slot_init(self, slot: int, local) -> None:
+        from . import native
+        local.ctx = native.Context(self.device)
+        n = local.ctx.sm_count
+        # general slots share the SMs the fast slots leave; a fast slot's small fits
+        # run on fast_ctas CTAs (default one: the resident sweep, or a one-CTA
+        # cluster or group sweep), which find a free SM beside the general slots'
+        # clusters, where a multi-CTA cluster may have to wait for a whole GPC
+        general = max(1, (n - self.n_fast * self.fast_ctas) // max(1, self.n_slots))
+        local.ctx.set_max_ctas(self.fast_ctas if slot >= self.n_slots else general)
+        local.ctx.set_blocking_wait(True)  # slots wait without spinning the host cores
+
     def _gpu_fit(self, slot: int, req: Request, local):
         from . import native
         if not hasattr(local, "ctx"):
-            local.ctx = native.Context(self.device)
-            n = local.ctx.sm_count
-            # general slots share the SMs; a fast slot's small fits take one CTA
-            # (the resident sweep) or a small cluster
-            local.ctx.set_max_ctas(4 if slot >= self.n_slots else max(1, n // self.n_slots))
-            local.ctx.set_blocking_wait(True)  # slots wait without spinning the host cores
+            self._gpu_slot_init(slot, local)
         args = req.args or native.ModeFindingArguments()
         r = native.fit_model(local.ctx, req.data, args)
         return r.beta, r.return_flag, r.iterations, r.log_likelihood

@@ -156,3 +156,27 @@ def test_cox_device_sweep_direct_rebuild_on_two_ctas(oracle_engine, form):
     assert got.iterations == want["iterations"]
     assert rel_beta(got.beta, want["beta"]) <= BETA_TOL
     assert abs(got.log_likelihood - want["loglik"]) <= LL_TOL * abs(want["loglik"])
+
+
+@pytest.mark.parametrize("form", [native.SWEEP_LEVELS, native.SWEEP_GRID_LEVELS])
+@pytest.mark.parametrize("kind", ["cox", "clr"])
+def test_group_sweep_on_one_cta(oracle_engine, kind, form):
+    """A context limited to one CTA (a serving slot for small fits): the group
+    sweep runs as a one-CTA cluster (LEVELS) or a one-CTA grid (GRID_LEVELS);
+    every row, stratum run and risk-set sum is that CTA's."""
+    if kind == "cox":
+        d = synthetic.small(MODEL_COX, seed=21, K=8_000, P=60, density=0.02, n_strata=8, tie_days=3,
+                            formats=("indicator", "sparse"), prior=PRIOR_LAPLACE, variance=0.1)
+    else:
+        d = synthetic.conditional_logistic(seed=22, n_sets=900, P=80)
+    want = oracle_engine(d).fit(GRADIENT, 1e-6)
+    ctx = native.Context(0)
+    ctx.set_max_ctas(1)
+    try:
+        got = native.fit_model(ctx, d, native.ModeFindingArguments(convergence_type=GRADIENT, strategy=form))
+    finally:
+        ctx.close()
+    assert got.return_flag == want["flag"]
+    assert got.iterations == want["iterations"]
+    assert rel_beta(got.beta, want["beta"]) <= BETA_TOL
+    assert abs(got.log_likelihood - want["loglik"]) <= LL_TOL * abs(want["loglik"])

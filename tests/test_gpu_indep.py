@@ -123,7 +123,7 @@ def test_split_columns_beyond_the_stage(gpu_ctx, oracle_engine, model, kw, strat
     assert abs(r.log_likelihood - want["loglik"]) <= LL_TOL * abs(want["loglik"])
 
 
-@pytest.mark.parametrize("max_ctas", [3, 18])
+@pytest.mark.parametrize("max_ctas", [1, 3, 18])
 def test_find_mode_on_a_share_of_the_sms(oracle_engine, max_ctas):
     """A context limited to a few CTAs (the serving loop's slots) builds its
     sweep schedule for that grid: longer chunks, more split columns per CTA."""
