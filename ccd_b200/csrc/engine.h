@@ -218,6 +218,7 @@ struct Fit {
     void find_mode_resident(const ccdb_mode_args& a, int* flag, int* iters, double* obj, float* ms);
     ResCol* d_res_recs = nullptr;  // its active columns' records in visiting order
     int32_t d_res_cap = 0;
+    double2* d_res_rs = nullptr;   // the row state of the global form (K entries)
     int32_t* d_batch_cols = nullptr;  // independent-row models
     double2* d_batch_out = nullptr;
     bool is_cox() const { return model == M_COX; }

@@ -25,6 +25,14 @@
 // same objective terms as the other sweeps; at exit the row state is written
 // back to global memory.
 //
+// A fit with more rows than shared memory holds runs the same sweep with the
+// row state in a global array (GL): only this CTA touches it, so the block
+// barriers order its reads and writes and L1 keeps what fits.  Warps then take
+// columns of up to kResidentWarpMaxGlobal entries, in chunks of 256: a large
+// L1-penalised fit, whose steps are mostly zero and whose columns share rows,
+// moves a whole batch of columns per round instead of one dependency level a
+// column.
+//
 // No wait spans CTAs (there is one), so the kernel has no wait to bound.
 #include <cstdint>
 
@@ -141,15 +149,17 @@ __device__ __forceinline__ ResCol shfl_rec(const ResCol& r, int src) {
     return o;
 }
 
-template <int MODEL>
+template <int MODEL, bool GL>
 __global__ void __launch_bounds__(kRT, 1) resident_sweep_kernel(ResidentParams R) {
-    extern __shared__ __align__(16) double2 s_rs[];  // {xBeta, denominator} of every row
+    extern __shared__ __align__(16) double2 s_dyn[];  // {xBeta, denominator} of every row (shared form)
     __shared__ double2 s_red2[kRW];
     __shared__ double4 s_red4[kRW];
     __shared__ double s_delta[kRW], s_hd[kRW], s_beta[kRW];
 
     const IndepParams& P = R.P;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    double2* const s_rs = GL ? R.rs : s_dyn;
+    const int64_t warp_max = GL ? kResidentWarpMaxGlobal : kLong;
     for (int64_t k = tid; k < P.K; k += kRT) s_rs[k] = make_double2(P.row[2 * k].x, P.row[2 * k + 1].x);
     __syncthreads();
 
@@ -168,7 +178,7 @@ __global__ void __launch_bounds__(kRT, 1) resident_sweep_kernel(ResidentParams R
             ResCol rec{-1, 0, 0, 0, 0};
             const int q = pos + lane;
             if (q < R.n_active) rec = R.recs[q];
-            const bool short_col = lane < kRW && rec.j >= 0 && rec.n <= kLong;
+            const bool short_col = lane < kRW && rec.j >= 0 && rec.n <= warp_max;
             const unsigned run = __ballot_sync(0xffffffffu, short_col);
             const int nb = (~run == 0u) ? 32 : __ffs(~run) - 1;  // at most kRW: lanes >= kRW are false
             if (nb == 0) {
@@ -217,30 +227,45 @@ __global__ void __launch_bounds__(kRT, 1) resident_sweep_kernel(ResidentParams R
             // ---- a batch of nb short columns, one per warp, against the same state
             const ResCol c = shfl_rec(rec, wid < nb ? wid : 0);
             const bool has_rows = c.flags & 1, has_vals = c.flags & 2, ind = c.flags & 4;
+            // the warp's column in chunks of kLong entries, kLanePer a lane (one
+            // chunk in the shared form); the last chunk stays in registers
             int k[kLanePer];
             double x[kLanePer];
-            if (wid < nb) {
-                const int j = c.j;
+            auto load_chunk = [&](int64_t base) {
 #pragma unroll
                 for (int i = 0; i < kLanePer; ++i) {
-                    const int p = lane + 32 * i;
+                    const int64_t p = base + lane + 32 * i;
                     k[i] = -1;
                     x[i] = 1.0;
                     if (p < c.n) {
-                        k[i] = has_rows ? __ldg(P.rows + c.cb + p) : p;
+                        k[i] = has_rows ? __ldg(P.rows + c.cb + p) : (int)p;
                         if (has_vals) x[i] = __ldg(P.vals + c.vb + p);
                     }
                 }
-                const double xjy = P.xjy[j], pvar = P.pvar[j], b0 = P.beta[j];
-                const int ptype = P.ptype[j];
-                double hd = P.hdelta[j];
-                double g = 0.0, h = 0.0;
+            };
+            double g = 0.0, h = 0.0;
+            auto add_chunk = [&]() {
 #pragma unroll
                 for (int i = 0; i < kLanePer; ++i)
                     if (k[i] >= 0) {
                         const double w = R.weighted ? P.row[2 * (int64_t)k[i] + 1].y : 1.0;
                         const double2 xd = s_rs[k[i]];
                         entry_gh<MODEL>(ind, x[i], exp(xd.x), xd.y, w, g, h);
+                    }
+            };
+#pragma unroll
+            for (int i = 0; i < kLanePer; ++i) k[i] = -1;
+            if (wid < nb) {
+                const int j = c.j;
+                load_chunk(0);  // the entries' loads go out before the column's scalars
+                const double xjy = P.xjy[j], pvar = P.pvar[j], b0 = P.beta[j];
+                const int ptype = P.ptype[j];
+                double hd = P.hdelta[j];
+                add_chunk();
+                if (GL)
+                    for (int64_t base = kLong; base < c.n; base += kLong) {
+                        load_chunk(base);
+                        add_chunk();
                     }
                 // the butterfly leaves the same sums in every lane
                 const double2 s = warp_sum2(make_double2(g, h));
@@ -267,9 +292,18 @@ __global__ void __launch_bounds__(kRT, 1) resident_sweep_kernel(ResidentParams R
             }
             if (wid == first && first < nb) {
                 const double d = s_delta[wid];
+                if (GL && c.n > kLong) {  // a column of several chunks: read them again
+                    for (int64_t base = 0; base < c.n; base += kLong) {
+                        load_chunk(base);
 #pragma unroll
-                for (int i = 0; i < kLanePer; ++i)
-                    if (k[i] >= 0) entry_update(s_rs, k[i], x[i], d);
+                        for (int i = 0; i < kLanePer; ++i)
+                            if (k[i] >= 0) entry_update(s_rs, k[i], x[i], d);
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < kLanePer; ++i)
+                        if (k[i] >= 0) entry_update(s_rs, k[i], x[i], d);
+                }
             }
             const long long tb3 = tr ? clock64() : 0;
             __syncthreads();
@@ -351,14 +385,21 @@ cudaError_t launch_resident_sweep(const ResidentParams& R, cudaStream_t stream) 
         if (r == cudaSuccess) r = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
         if (r != cudaSuccess) return r;
         const int dyn = optin - (int)kStaticSmemBound;
-        r = cudaFuncSetAttribute(resident_sweep_kernel<M_LOGISTIC>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+        r = cudaFuncSetAttribute(resident_sweep_kernel<M_LOGISTIC, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
         if (r != cudaSuccess) return r;
-        return cudaFuncSetAttribute(resident_sweep_kernel<M_POISSON>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+        return cudaFuncSetAttribute(resident_sweep_kernel<M_POISSON, false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
     });
     if (e != cudaSuccess) return e;
+    if (R.rs) {  // the row state in global memory
+        if (R.P.model == M_LOGISTIC) resident_sweep_kernel<M_LOGISTIC, true><<<1, kRT, 0, stream>>>(R);
+        else resident_sweep_kernel<M_POISSON, true><<<1, kRT, 0, stream>>>(R);
+        return cudaGetLastError();
+    }
     const size_t smem = sizeof(double2) * (size_t)R.P.K;
-    if (R.P.model == M_LOGISTIC) resident_sweep_kernel<M_LOGISTIC><<<1, kRT, smem, stream>>>(R);
-    else resident_sweep_kernel<M_POISSON><<<1, kRT, smem, stream>>>(R);
+    if (R.P.model == M_LOGISTIC) resident_sweep_kernel<M_LOGISTIC, false><<<1, kRT, smem, stream>>>(R);
+    else resident_sweep_kernel<M_POISSON, false><<<1, kRT, smem, stream>>>(R);
     return cudaGetLastError();
 }
 

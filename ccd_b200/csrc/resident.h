@@ -1,5 +1,6 @@
-// resident.h -- the single-CTA sweep of small independent-row fits
-// (resident.cu): the row state lives in shared memory for the whole findMode.
+// resident.h -- the single-CTA sweep of independent-row fits (resident.cu):
+// the row state lives in shared memory for the whole findMode when it fits
+// there, else in a global array the CTA alone reads and writes.
 #pragma once
 
 #include <cstdint>
@@ -31,6 +32,9 @@ struct ResidentParams {
     long long* trace;
     int32_t trace_n;
     int32_t pad;
+    // {xBeta, denominator} of every row in global memory (K entries), for fits
+    // whose row state does not fit shared memory; nullptr: shared memory
+    double2* rs;
 };
 
 constexpr int kResidentTraceWords = 8;
@@ -38,6 +42,9 @@ constexpr int kResidentTraceWords = 8;
 int resident_threads();
 // the most rows whose state fits the kernel's shared memory on the current device
 cudaError_t resident_max_rows(int model, int64_t* rows);
+// a column of at most this many entries is one warp's in a speculative batch
+// when the row state is in global memory (shared memory: 256)
+constexpr int64_t kResidentWarpMaxGlobal = 2048;
 cudaError_t launch_resident_sweep(const ResidentParams& R, cudaStream_t stream);
 
 }  // namespace ccdb

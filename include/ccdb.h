@@ -187,8 +187,9 @@ typedef struct {
     int32_t strategy;          /* sweep strategy.  Logistic/Poisson: CCDB_SWEEP_AUTO runs
                                   the resident sweep (one CTA, the row state in shared
                                   memory) when the fit's rows fit it, else the cluster
-                                  sweep; _RESIDENT requires the former (an error for a fit
-                                  too large for it); _LEVELS runs the cluster sweep (one
+                                  sweep; _RESIDENT asks for the resident sweep (beyond
+                                  shared memory its global form, the row state in device
+                                  memory); _LEVELS runs the cluster sweep (one
                                   launch per findMode over dependency levels),
                                   _GRID_LEVELS the grid-wide level sweep,
                                   _SPECULATIVE host-driven batches of gradients that restart
@@ -216,7 +217,7 @@ typedef struct {
 #define CCDB_SWEEP_LEVELS 1        /* one thread-block cluster, levels ordered by cluster barriers */
 #define CCDB_SWEEP_SPECULATIVE 2
 #define CCDB_SWEEP_GRID_LEVELS 3   /* one CTA per SM, levels ordered by global counters */
-#define CCDB_SWEEP_RESIDENT 4      /* one CTA, the row state in shared memory (small fits) */
+#define CCDB_SWEEP_RESIDENT 4      /* one CTA, the row state in shared memory (or device memory) */
 
 typedef struct {
     int32_t return_flag;        /* UpdateReturnFlags */

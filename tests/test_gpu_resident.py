@@ -1,6 +1,7 @@
-"""GPU parity of the resident sweep (one CTA, the row state in shared memory)
-against the CPU oracle: short columns in speculative warp batches, long
-columns on the whole CTA, weights, fixed columns, the capacity limit."""
+"""GPU parity of the resident sweep (one CTA, the row state in shared memory,
+or in global memory for larger fits) against the CPU oracle: short columns in
+speculative warp batches, long columns on the whole CTA, weights, fixed
+columns, the global form and AUTO's choice of it."""
 import numpy as np
 import pytest
 
@@ -95,10 +96,35 @@ def test_auto_takes_resident_for_small_fits(gpu_ctx):
     assert np.array_equal(r0.beta, r1.beta)
 
 
-def test_resident_rejects_a_fit_beyond_capacity(gpu_ctx):
-    d = synthetic.small(MODEL_LOGISTIC, seed=19, K=40_000, P=5, density=0.01)
-    with pytest.raises(native.CcdbError):
-        native.fit_model(gpu_ctx, d, RESIDENT)
-    # the default strategy falls back to the cluster sweep
-    r = native.fit_model(gpu_ctx, d, native.ModeFindingArguments())
-    assert r.return_flag == 0
+GLOBAL_CASES = [
+    # 40,000 rows: the row state in global memory; columns of ~400 entries, two
+    # chunks of one warp each
+    (MODEL_LOGISTIC, dict(seed=19, K=40_000, P=60, density=0.01, formats=("indicator", "sparse"))),
+    (MODEL_POISSON, dict(seed=20, K=30_000, P=40, density=0.02, offset=True, prior=PRIOR_NORMAL,
+                         formats=("indicator", "sparse"))),
+    # ~3,000-entry columns (above the warp limit) and dense ones on the whole CTA
+    (MODEL_LOGISTIC, dict(seed=21, K=25_000, P=24, density=0.12)),
+]
+
+
+@pytest.mark.parametrize("model,kw", GLOBAL_CASES)
+@pytest.mark.parametrize("conv", [GRADIENT, MITTAL])
+def test_resident_global_form_matches_oracle(gpu_ctx, oracle_engine, model, kw, conv):
+    """More rows than shared memory holds: the same sweep with the row state in
+    a global array, asked for by CCDB_SWEEP_RESIDENT."""
+    d = synthetic.small(model, **kw)
+    want = oracle_engine(d).fit(conv, 1e-6)
+    args = native.ModeFindingArguments(convergence_type=conv, strategy=native.SWEEP_RESIDENT)
+    check(native.fit_model(gpu_ctx, d, args), want)
+
+
+def test_auto_leaves_large_fits_to_the_cluster_sweep(gpu_ctx, oracle_engine):
+    """Beyond shared memory AUTO runs the cluster sweep (the same bits as
+    asking for it); the global resident form, asked for, matches the oracle."""
+    d = synthetic.logistic_l1(seed=22, K=30_000, P=400, density=0.01)
+    want = oracle_engine(d).fit(GRADIENT, 1e-6)
+    a = native.fit_model(gpu_ctx, d, native.ModeFindingArguments())
+    b = native.fit_model(gpu_ctx, d, native.ModeFindingArguments(strategy=native.SWEEP_LEVELS))
+    assert np.array_equal(a.beta, b.beta)
+    check(a, want)
+    check(native.fit_model(gpu_ctx, d, RESIDENT), want)
