@@ -167,7 +167,12 @@ class Server:
             try:
                 self._gpu_slot_init(slot, local)
             except Exception:  # retried by the first request, which then fails with the error
-                local.__dict__.pop("ctx", None)
+                ctx = local.__dict__.pop("ctx", None)
+                if ctx is not None:
+                    try:
+                        ctx.close()
+                    except Exception:
+                        pass
         while True:
             with self._cv:
                 while True:
