@@ -20,6 +20,7 @@
 
 #include "../../include/ccdb.h"
 #include "batch.h"
+#include "csr_device.h"
 #include "csr_host.h"
 #include "engine.h"
 #include "resident.h"
@@ -96,15 +97,38 @@ Matrix::~Matrix() {
 }
 
 // Row-major copy for computeXBeta: per row, entries in increasing column order
-// (dense-like columns included), built once on the host threads (csr_host.cpp).
+// (dense-like columns included), built once, on the device from the uploaded
+// columns (csr_device.cu); a matrix with a row longer than kCsrDeviceMaxRow
+// entries is built on the host threads instead (csr_host.cpp, the same layout).
 void Matrix::ensure_csr(cudaStream_t s) {
     if (d_row_ptr) return;
-    const HostCsr h = build_csr(K, J, col_start.data(), rows_h.data(), val_start.data(), vals_h.data(),
-                                fmt.data(), (int)std::max(1u, std::thread::hardware_concurrency()));
-    d_row_ptr = upload(ctx, h.row_ptr.data(), h.row_ptr.size(), s);
-    d_csr_col = upload(ctx, h.col.data(), h.col.size(), s);
-    d_csr_val = upload(ctx, h.val.data(), h.val.size(), s);
-    check_cuda(ctx->wait(), "csr upload");
+    int64_t total = 0;
+    for (int j = 0; j < J; ++j) total += entries(j);
+    CsrDeviceArgs a{K, J, d_col_ptr, d_rows, d_val_ptr, d_vals, d_fmt};
+    auto* counts = static_cast<int32_t*>(ctx->alloc(sizeof(int32_t) * (size_t)std::max<int64_t>(K, 1)));
+    auto* cursor = static_cast<int64_t*>(ctx->alloc(sizeof(int64_t) * (size_t)std::max<int64_t>(K, 1)));
+    auto* d_max = static_cast<int32_t*>(ctx->alloc(sizeof(int32_t)));
+    d_row_ptr = static_cast<int64_t*>(ctx->alloc(sizeof(int64_t) * (size_t)(K + 1)));
+    int32_t longest = 0;
+    check_cuda(csr_device_count(a, counts, d_row_ptr, cursor, d_max, s), "row counts");
+    check_cuda(cudaMemcpyAsync(&longest, d_max, sizeof(int32_t), cudaMemcpyDeviceToHost, s), "longest row");
+    check_cuda(ctx->wait(), "row counts");
+    if (longest <= kCsrDeviceMaxRow) {
+        d_csr_col = static_cast<int32_t*>(ctx->alloc(sizeof(int32_t) * (size_t)std::max<int64_t>(total, 1)));
+        d_csr_val = static_cast<double*>(ctx->alloc(sizeof(double) * (size_t)std::max<int64_t>(total, 1)));
+        check_cuda(csr_device_fill(a, d_row_ptr, cursor, d_csr_col, d_csr_val, s), "row-major fill");
+    } else {
+        ctx->release(d_row_ptr);
+        const HostCsr h = build_csr(K, J, col_start.data(), rows_h.data(), val_start.data(), vals_h.data(),
+                                    fmt.data(), (int)std::max(1u, std::thread::hardware_concurrency()));
+        d_row_ptr = upload(ctx, h.row_ptr.data(), h.row_ptr.size(), s);
+        d_csr_col = upload(ctx, h.col.data(), h.col.size(), s);
+        d_csr_val = upload(ctx, h.val.data(), h.val.size(), s);
+    }
+    ctx->release(counts);
+    ctx->release(cursor);
+    ctx->release(d_max);
+    check_cuda(ctx->wait(), "row-major copy");
 }
 
 // ------------------------------------------------------------------ Fit
@@ -1057,6 +1081,26 @@ int ccdb_matrix_create(ccdb_context* ctx, int64_t K, int32_t J, const int64_t* c
 
 int ccdb_matrix_destroy(ccdb_matrix* m) {
     return guard([&] { delete m; });
+}
+
+int ccdb_matrix_row_major(ccdb_matrix* m, int64_t* row_ptr, int32_t* col, double* val) {
+    return guard([&] {
+        require(m && row_ptr && col && val, "NULL argument");
+        check_cuda(cudaSetDevice(m->ctx->device), "cudaSetDevice");
+        cudaStream_t s = m->ctx->stream;
+        m->ensure_csr(s);
+        int64_t total = 0;
+        for (int j = 0; j < m->J; ++j) total += m->entries(j);
+        check_cuda(cudaMemcpyAsync(row_ptr, m->d_row_ptr, sizeof(int64_t) * (size_t)(m->K + 1),
+                                   cudaMemcpyDeviceToHost, s), "row offsets");
+        if (total > 0) {
+            check_cuda(cudaMemcpyAsync(col, m->d_csr_col, sizeof(int32_t) * (size_t)total, cudaMemcpyDeviceToHost, s),
+                       "columns");
+            check_cuda(cudaMemcpyAsync(val, m->d_csr_val, sizeof(double) * (size_t)total, cudaMemcpyDeviceToHost, s),
+                       "values");
+        }
+        check_cuda(m->ctx->wait(), "row-major copy");
+    });
 }
 
 int ccdb_fit_create(ccdb_context* ctx, const ccdb_matrix* m, const ccdb_fit_desc* d, ccdb_fit** out) {

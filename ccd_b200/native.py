@@ -17,7 +17,7 @@ from typing import Optional
 
 import numpy as np
 
-from .data import CyclopsData, GRADIENT
+from .data import DENSE, INTERCEPT, CyclopsData, GRADIENT
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libccdb.so")
@@ -120,6 +120,7 @@ def lib() -> C.CDLL:
         L.ccdb_context_set_blocking_wait.argtypes = [_P, C.c_int32]
         L.ccdb_matrix_create.argtypes = [_P, C.c_int64, C.c_int32, _P, _P, _P, _P, _P, C.POINTER(_P)]
         L.ccdb_matrix_destroy.argtypes = [_P]
+        L.ccdb_matrix_row_major.argtypes = [_P, _P, _P, _P]
         L.ccdb_fit_create.argtypes = [_P, _P, C.POINTER(_FitDesc), C.POINTER(_P)]
         L.ccdb_fit_destroy.argtypes = [_P]
         L.ccdb_set_weights.argtypes = [_P, _P]
@@ -217,12 +218,24 @@ class Matrix:
     def __init__(self, ctx: Context, d: CyclopsData):
         self.ctx = ctx
         self.K, self.J = d.K, d.J
+        dense_like = np.isin(np.asarray(d.fmt), (DENSE, INTERCEPT))
+        self.entries = int(np.sum(np.where(dense_like, d.K, np.diff(np.asarray(d.col_start)))))
         arrs = [_c(d.col_start, np.int64), _c(d.rows, np.int32), _c(d.val_start, np.int64),
                 _c(d.vals, np.float64), _c(d.fmt, np.uint8)]
         h = _P()
         _check(lib().ccdb_matrix_create(ctx.h, d.K, d.J, *[_p(a) for a in arrs], C.byref(h)))
         self.h = h
         ctx._children.add(self)
+
+    def row_major(self):
+        """The row-major copy (row offsets, columns, values) the engine builds on
+        the device for computeXBeta and the MM cycle."""
+        total = int(self.entries)
+        row_ptr = np.zeros(self.K + 1, np.int64)
+        col = np.zeros(max(total, 1), np.int32)
+        val = np.zeros(max(total, 1), np.float64)
+        _check(lib().ccdb_matrix_row_major(self.h, _p(row_ptr), _p(col), _p(val)))
+        return row_ptr, col[:total], val[:total]
 
     def close(self):
         if getattr(self, "h", None):

@@ -86,6 +86,12 @@ int ccdb_matrix_create(ccdb_context* ctx, int64_t K, int32_t J, const int64_t* c
                        const int32_t* rows, const int64_t* val_start, const double* vals,
                        const uint8_t* fmt, ccdb_matrix** out);
 int ccdb_matrix_destroy(ccdb_matrix* m);
+/* The matrix's row-major copy, the one computeXBeta's row sums and the MM
+ * cycle read (the transpose ModelSpecifics.hpp:313-361 walks), copied to host
+ * buffers: row_ptr (K + 1 offsets), col and val (one entry per matrix entry,
+ * DENSE and INTERCEPT columns at every row): per row the columns in increasing
+ * order.  Built on the device on first use and kept with the matrix. */
+int ccdb_matrix_row_major(ccdb_matrix* m, int64_t* row_ptr, int32_t* col, double* val);
 
 typedef struct {
     int32_t model_type;    /* ModelType */
