@@ -64,6 +64,8 @@ def parse():
                     help="serve: requests in the replayed stream")
     ap.add_argument("--serve-slots", type=int, default=8, help="serve: concurrent fits")
     ap.add_argument("--serve-fast-ctas", type=int, default=1, help="serve: CTAs of a fast slot's fit")
+    ap.add_argument("--serve-slot-ctas", type=int, default=0,
+                    help="serve: at most this many CTAs for a general slot's fit (0: an even share)")
     ap.add_argument("--serve-fast-slots", type=int, default=4,
                     help="serve: extra slots that take only small requests (at most 200,000 entries)")
     ap.add_argument("--workload", choices=["poisson_offset", "logistic_l1", "cv_grid", "cox_breslow", "serve",
@@ -1064,7 +1066,7 @@ def run_serve(args, world, rank, local, collect=False):
     warm = synthetic.serving_stream(max(16, args.serve_slots + args.serve_fast_slots), seed=12, rate=1e3,
                                     K_range=(1e3, 3e4), J_range=(50, 200))
     srv = serve.Server(device=local, hbm_budget=150e9, slots=args.serve_slots, fast_slots=args.serve_fast_slots,
-                       fast_ctas=args.serve_fast_ctas)
+                       fast_ctas=args.serve_fast_ctas, slot_ctas=args.serve_slot_ctas)
     try:
         for _ in range(args.warmup):
             srv.done.clear()
@@ -1126,6 +1128,7 @@ def serve_config(args, stream) -> dict:
             "K": "log-uniform 1e3..1e5", "J": "log-uniform 1e2..1e4",
             "density": "uniform 0.001..0.02", "prior": "Laplace, variance 0.1",
             "slots": args.serve_slots, "fast_slots": args.serve_fast_slots, "fast_slot_ctas": args.serve_fast_ctas,
+            "slot_ctas": args.serve_slot_ctas or "even share",
             "fast_lane": "requests of at most 200,000 matrix entries, oldest first",
             "hbm_budget_bytes": 150e9,
             "step": "replay of the whole stream; latency = completion - arrival",

@@ -10,14 +10,14 @@ on the device.  A fit runs exactly as it would alone (same engine, same
 kernels, same arithmetic: its result does not depend on its neighbours); the
 server only decides when it starts.
 
-Each slot's context limits its sweep kernels to its share of the SMs (SM
-count / slots CTAs), so the slots' kernels can all be resident at once and run
-side by side.  Every model runs a whole findMode attempt in one launch:
-logistic and Poisson fits whose row state fits one CTA's shared memory the
-resident sweep (one CTA), larger ones the cluster sweep over dependency
-levels (a thread block cluster of at most that many CTAs), grouped models
-(conditional logistic, Cox) the persistent group sweep (a cooperative grid of
-at most that many CTAs).
+Each slot's context limits its sweep kernels to its share of the SMs (a
+fast slot one CTA, a general slot an even share of the rest), so the slots'
+kernels can all be resident at once and run side by side.  Every model runs
+a whole findMode attempt in one launch: logistic and Poisson fits whose row
+state fits one CTA's shared memory the resident sweep (one CTA), larger ones
+the cluster sweep over dependency levels (a thread block cluster of at most
+that many CTAs), grouped models (conditional logistic, Cox) the persistent
+group sweep (a cluster, or a cooperative grid, of at most that many CTAs).
 
 The reference has no serving layer; this loop drives the same C ABI entry
 point a single fit uses (ccdb_fit_model: upload, findMode, coefficients back).
@@ -82,7 +82,9 @@ def is_small(d: CyclopsData, max_entries: int) -> bool:
 class Server:
     """`slots` concurrent fits under an HBM budget of `hbm_budget` bytes, plus
     `fast_slots` slots that take only small requests (at most `fast_entries`
-    matrix entries) on at most `fast_ctas` CTAs each.
+    matrix entries) on at most `fast_ctas` CTAs each; a general slot's fits
+    take at most `slot_ctas` CTAs (0: an even share of the SMs the fast slots
+    leave).
 
     The general slots take requests in arrival order (no overtaking).  A fast
     slot takes the oldest pending small request, ahead of any large one: a
@@ -98,13 +100,14 @@ class Server:
 
     def __init__(self, device: int = 0, hbm_budget: float = 150e9, slots: int = 8,
                  fit_fn: Optional[Callable] = None, fast_slots: int = 0, fast_entries: int = 200_000,
-                 fast_ctas: int = 1):
+                 fast_ctas: int = 1, slot_ctas: int = 0):
         self.device = device
         self.budget = int(hbm_budget)
         self.n_slots = slots
         self.n_fast = fast_slots
         self.fast_entries = int(fast_entries)
         self.fast_ctas = max(1, int(fast_ctas))
+        self.slot_ctas = max(0, int(slot_ctas))  # 0: the SMs the fast slots leave, shared evenly
         self._fit_fn = fit_fn or self._gpu_fit
         self._cv = threading.Condition()
         self._pending: collections.deque = collections.deque()
@@ -213,6 +216,8 @@ class Server:
         # cluster or group sweep), which find a free SM beside the general slots'
         # clusters, where a multi-CTA cluster may have to wait for a whole GPC
         general = max(1, (n - self.n_fast * self.fast_ctas) // max(1, self.n_slots))
+        if self.slot_ctas:
+            general = min(general, self.slot_ctas)
         local.ctx.set_max_ctas(self.fast_ctas if slot >= self.n_slots else general)
         local.ctx.set_blocking_wait(True)  # slots wait without spinning the host cores
 
