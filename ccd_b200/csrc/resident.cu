@@ -1,5 +1,6 @@
-// resident.cu -- one findMode of a small independent-row fit (logistic,
-// Poisson) in one CTA whose shared memory holds the row state.
+// resident.cu -- one findMode of an independent-row fit (logistic, Poisson)
+// in one CTA whose shared memory holds the row state (or, for a fit with more
+// rows than that, a global array only this CTA touches).
 //
 // A fit of up to resident_max_rows() rows keeps {xBeta, denominator} of every
 // row in shared memory for the whole launch.  offsExpXBeta is not stored: every
