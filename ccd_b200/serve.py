@@ -207,18 +207,23 @@ class Server:
                 self.done.append(Completed(req.rid, beta, flag, iters, ll, req.arrival, start, end, slot, err))
                 self._cv.notify_all()
 
+    def slot_max_ctas(self, slot: int, n_sm: int) -> int:
+        """The CTA limit of a slot's context on a GPU of n_sm SMs.
+
+        General slots share the SMs the fast slots leave (at most slot_ctas
+        each when set); a fast slot's small fits run on fast_ctas CTAs (default
+        one: the resident sweep, or a one-CTA cluster or group sweep), which
+        find a free SM beside the general slots' clusters, where a multi-CTA
+        cluster may have to wait for a whole GPC."""
+        if slot >= self.n_slots:
+            return self.fast_ctas
+        general = max(1, (n_sm - self.n_fast * self.fast_ctas) // max(1, self.n_slots))
+        return min(general, self.slot_ctas) if self.slot_ctas else general
+
     def _gpu_slot_init(self, slot: int, local) -> None:
         from . import native
         local.ctx = native.Context(self.device)
-        n = local.ctx.sm_count
-        # general slots share the SMs the fast slots leave; a fast slot's small fits
-        # run on fast_ctas CTAs (default one: the resident sweep, or a one-CTA
-        # cluster or group sweep), which find a free SM beside the general slots'
-        # clusters, where a multi-CTA cluster may have to wait for a whole GPC
-        general = max(1, (n - self.n_fast * self.fast_ctas) // max(1, self.n_slots))
-        if self.slot_ctas:
-            general = min(general, self.slot_ctas)
-        local.ctx.set_max_ctas(self.fast_ctas if slot >= self.n_slots else general)
+        local.ctx.set_max_ctas(self.slot_max_ctas(slot, local.ctx.sm_count))
         local.ctx.set_blocking_wait(True)  # slots wait without spinning the host cores
 
     def _gpu_fit(self, slot: int, req: Request, local):

@@ -131,3 +131,25 @@ def test_fast_lane_takes_small_requests_ahead_of_large_ones():
     # the general slot kept arrival order over what it took
     general = [rid for s, rid in taken if s == 0]
     assert general == sorted(general)
+
+
+def test_slot_cta_limits():
+    """Fast slots take fast_ctas CTAs; general slots share the SMs the fast
+    slots leave, capped by slot_ctas when it is set; the slots' CTAs together
+    never exceed the SM count."""
+    fit, _ = _stub()
+    cases = [(dict(slots=8, fast_slots=4), 148, 18, 1),
+             (dict(slots=8, fast_slots=4, fast_ctas=4), 148, 16, 4),
+             (dict(slots=8, fast_slots=4, slot_ctas=8), 148, 8, 1),
+             (dict(slots=3, fast_slots=0), 148, 49, None),
+             (dict(slots=200, fast_slots=2), 148, 1, 1)]
+    for kw, n_sm, general, fast in cases:
+        srv = serve.Server(hbm_budget=1e9, fit_fn=fit, **kw)
+        try:
+            limits = [srv.slot_max_ctas(s, n_sm) for s in range(kw["slots"] + kw["fast_slots"])]
+        finally:
+            srv.close()
+        assert limits[:kw["slots"]] == [general] * kw["slots"]
+        assert limits[kw["slots"]:] == [fast] * kw["fast_slots"]
+        if general * kw["slots"] >= kw["slots"] and kw["slots"] <= n_sm:
+            assert sum(limits) <= n_sm
