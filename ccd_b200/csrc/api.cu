@@ -1020,6 +1020,45 @@ int ccdb_context_memory(const ccdb_context* ctx, size_t* bytes) {
 
 // The CompressedDataMatrix contract every matrix is checked against before any
 // device work (host only).
+// The first of columns [0, n_cols) whose row ids are not ascending within
+// [0, K), or n_cols: column ranges of about equal entry counts checked on
+// host threads (the check is a memory-bound walk of the row ids, vectorised
+// within a column), the lowest failing column kept -- the one a walk in
+// column order would report.
+static int32_t first_row_error(int64_t K, int32_t n_cols, const int64_t* col_start, const int32_t* rows) {
+    auto bad = [&](int32_t j) {
+        const int64_t b = col_start[j], e = col_start[j + 1];
+        if (e <= b) return false;
+        unsigned ok = (unsigned)(rows[b] >= 0) & (unsigned)((int64_t)rows[e - 1] < K);
+        for (int64_t p = b + 1; p < e; ++p) ok &= (unsigned)(rows[p] > rows[p - 1]);
+        return ok == 0u;
+    };
+    const int64_t total = n_cols > 0 ? col_start[n_cols] : 0;
+    const int64_t per_thread = int64_t(1) << 21;
+    const int T = (int)std::max<int64_t>(
+        1, std::min<int64_t>({(int64_t)std::max(1u, std::thread::hardware_concurrency()), total / per_thread, 16}));
+    if (T == 1) {
+        for (int32_t j = 0; j < n_cols; ++j)
+            if (bad(j)) return j;
+        return n_cols;
+    }
+    std::vector<int32_t> lo(T + 1, n_cols), found(T, n_cols);
+    lo[0] = 0;
+    for (int32_t j = 0, t = 1; j < n_cols && t < T; ++j)
+        if (col_start[j + 1] >= total * t / T) lo[t++] = j + 1;
+    std::vector<std::thread> pool;
+    for (int t = 0; t < T; ++t)
+        pool.emplace_back([&, t] {
+            for (int32_t j = lo[t]; j < lo[t + 1]; ++j)
+                if (bad(j)) {
+                    found[t] = j;
+                    return;
+                }
+        });
+    for (auto& th : pool) th.join();
+    return *std::min_element(found.begin(), found.end());
+}
+
 static void validate_matrix(int64_t K, int32_t J, const int64_t* col_start, const int32_t* rows,
                             const int64_t* val_start, const double* vals, const uint8_t* fmt) {
     require(col_start && val_start && fmt, "NULL argument");
@@ -1028,22 +1067,28 @@ static void validate_matrix(int64_t K, int32_t J, const int64_t* col_start, cons
     require(col_start[0] == 0 && val_start[0] == 0 && nnz >= 0 && nv >= 0, "bad offsets");
     require(nnz == 0 || rows, "rows is NULL");
     require(nv == 0 || vals, "vals is NULL");
-    for (int j = 0; j < J; ++j) {
+    // offsets and formats column by column; the columns before the first bad
+    // one have offsets within [0, nnz] and [0, nv], so their row ids can be read
+    int32_t first_bad = J;
+    const char* why = nullptr;
+    for (int32_t j = 0; j < J && !why; ++j) {
         const int64_t nr = col_start[j + 1] - col_start[j], nvj = val_start[j + 1] - val_start[j];
-        require(nr >= 0 && nvj >= 0, "offsets must be non-decreasing");
-        switch (fmt[j]) {
-        case F_DENSE: require(nr == 0 && nvj == K, "DENSE column needs K values, no rows"); break;
-        case F_INTERCEPT: require(nr == 0 && nvj == 0, "INTERCEPT column takes no data"); break;
-        case F_INDICATOR: require(nvj == 0, "INDICATOR column takes no values"); break;
-        case F_SPARSE: require(nvj == nr, "SPARSE column needs one value per row"); break;
-        default: require(false, "unknown column format");
+        if (nr < 0 || nvj < 0 || col_start[j + 1] > nnz || val_start[j + 1] > nv) {
+            why = "offsets must be non-decreasing";
+        } else {
+            switch (fmt[j]) {
+            case F_DENSE: if (!(nr == 0 && nvj == K)) why = "DENSE column needs K values, no rows"; break;
+            case F_INTERCEPT: if (!(nr == 0 && nvj == 0)) why = "INTERCEPT column takes no data"; break;
+            case F_INDICATOR: if (nvj != 0) why = "INDICATOR column takes no values"; break;
+            case F_SPARSE: if (nvj != nr) why = "SPARSE column needs one value per row"; break;
+            default: why = "unknown column format";
+            }
         }
-        int32_t last = -1;
-        for (int64_t p = col_start[j]; p < col_start[j + 1]; ++p) {
-            require(rows[p] > last && rows[p] < K, "row ids must be ascending and < K");
-            last = rows[p];
-        }
+        if (why) first_bad = j;
     }
+    // a row-id error in an earlier column comes first, as in a walk in column order
+    require(first_row_error(K, first_bad, col_start, rows) == first_bad, "row ids must be ascending and < K");
+    require(why == nullptr, why ? why : "");
 }
 
 int ccdb_matrix_validate(int64_t K, int32_t J, const int64_t* col_start, const int32_t* rows,

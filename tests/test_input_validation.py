@@ -53,3 +53,43 @@ def test_offsets():
     d = _data([(np.array([1], np.int32), None)], [INDICATOR])
     d.col_start = np.array([1, 2], np.int64)
     _refused(d, "bad offsets")
+
+
+def _big(J=400, per=12_000, K=2_000_000, seed=5):
+    """~4.8e6 indicator entries: enough that the row-id check runs on several
+    host threads."""
+    rng = np.random.default_rng(seed)
+    cols = [(np.sort(rng.choice(K, size=per, replace=False)).astype(np.int32), None) for _ in range(J)]
+    return _data(cols, [INDICATOR] * J, K=K)
+
+
+def test_large_matrix_checks_in_column_order():
+    d = _big()
+    native.validate_matrix(d)
+    cs = np.asarray(d.col_start)
+    # a row-id error in the last column is found
+    bad = _big()
+    bad.rows = np.array(bad.rows)
+    bad.rows[cs[-1] - 1] = bad.rows[cs[-1] - 2]
+    _refused(bad, "ascending")
+    # an out-of-range row early and a format error late: the earlier column is reported
+    bad = _big()
+    bad.rows = np.array(bad.rows)
+    bad.rows[cs[3] - 1] = bad.K
+    bad.fmt = np.array(bad.fmt)
+    bad.fmt[-1] = 7
+    _refused(bad, "< K")
+    # a format error early and a row error late: the format error is reported
+    bad = _big()
+    bad.rows = np.array(bad.rows)
+    bad.rows[cs[-1] - 1] = -5
+    bad.fmt = np.array(bad.fmt)
+    bad.fmt[2] = 7
+    _refused(bad, "unknown column format")
+
+
+def test_offsets_beyond_the_total_are_refused():
+    """A column whose end offset passes the total would read past the row ids."""
+    d = _data([(np.array([1, 2], np.int32), None), (np.array([3], np.int32), None)], [INDICATOR, INDICATOR])
+    d.col_start = np.array([0, 100, 3], np.int64)
+    _refused(d, "non-decreasing")
