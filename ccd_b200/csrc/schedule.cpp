@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <functional>
+#include <limits>
 #include <numeric>
 #include <queue>
 #include <stdexcept>
@@ -23,33 +24,53 @@ Schedule build_schedule(int64_t K, int32_t J, const int64_t* col_start, const in
     s.level_of.assign(J, -1);
     s.col_chunks.assign(J, 0);
 
-    // ---- levels: level(j) = 1 + max level of earlier columns sharing a key
-    std::vector<int32_t> last(n_keys > 0 ? n_keys : 1, -1);
-    int32_t floor_level = -1, max_level = -1;
-    for (int32_t j = 0; j < J; ++j) {
-        if (fixed && fixed[j]) continue;
-        int32_t L;
-        if (dense_like(fmt[j])) {
-            L = max_level + 1;
-            floor_level = L;
-        } else {
-            int32_t m = floor_level;
-            for (int64_t p = col_start[j]; p < col_start[j + 1]; ++p) {
-                const int64_t key = key_of_row ? key_of_row[rows[p]] : rows[p];
-                if (key < 0 || key >= n_keys) continue;  // rows outside every group
-                m = std::max(m, last[key]);
+    // ---- levels: level(j) = 1 + max level of earlier columns sharing a key.
+    // The table of each key's last level (stored + 1, 0 for none) is 16-bit
+    // while the levels fit, which halves its cache footprint, and the walk over
+    // a column's keys prefetches the entries it will read; beyond 65,533
+    // levels the walk restarts with a 32-bit table.
+    int32_t max_level = -1;
+    auto levels = [&](auto tag) -> bool {
+        using T = decltype(tag);
+        const int32_t cap = (int32_t)std::numeric_limits<T>::max() - 1;
+        std::vector<T> last(n_keys > 0 ? n_keys : 1, T(0));
+        auto key_at = [&](int64_t p) -> int64_t { return key_of_row ? key_of_row[rows[p]] : rows[p]; };
+        int32_t floor_level = -1;
+        max_level = -1;
+        s.n_active = 0;
+        for (int32_t j = 0; j < J; ++j) {
+            if (fixed && fixed[j]) continue;
+            int32_t L;
+            if (dense_like(fmt[j])) {
+                L = max_level + 1;
+                floor_level = L;
+            } else {
+                const int64_t b = col_start[j], e = col_start[j + 1];
+                int32_t m = floor_level + 1;  // (the highest level met) + 1
+                for (int64_t p = b; p < e; ++p) {
+                    if (p + 24 < e) {
+                        if (key_of_row) __builtin_prefetch(&key_of_row[rows[p + 24]]);
+                        else __builtin_prefetch(&last[rows[p + 24]]);
+                    }
+                    const int64_t key = key_at(p);
+                    if (key < 0 || key >= n_keys) continue;  // rows outside every group
+                    m = std::max<int32_t>(m, (int32_t)last[key]);
+                }
+                L = m;
+                if (L > cap) return false;
+                for (int64_t p = b; p < e; ++p) {
+                    const int64_t key = key_at(p);
+                    if (key < 0 || key >= n_keys) continue;
+                    last[key] = (T)(L + 1);
+                }
             }
-            L = m + 1;
-            for (int64_t p = col_start[j]; p < col_start[j + 1]; ++p) {
-                const int64_t key = key_of_row ? key_of_row[rows[p]] : rows[p];
-                if (key < 0 || key >= n_keys) continue;
-                last[key] = L;
-            }
+            s.level_of[j] = L;
+            max_level = std::max(max_level, L);
+            s.n_active++;
         }
-        s.level_of[j] = L;
-        max_level = std::max(max_level, L);
-        s.n_active++;
-    }
+        return true;
+    };
+    if (!levels(uint16_t{})) levels(int32_t{});
     s.n_levels = max_level + 1;
 
     // columns of each level, in visiting order
