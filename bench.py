@@ -64,6 +64,9 @@ def parse():
                     help="serve: requests in the replayed stream")
     ap.add_argument("--serve-slots", type=int, default=8, help="serve: concurrent fits")
     ap.add_argument("--serve-fast-ctas", type=int, default=1, help="serve: CTAs of a fast slot's fit")
+    ap.add_argument("--serve-detail", default=None, metavar="PATH",
+                    help="serve: write per-request wait/service times of the last replay, and each "
+                         "request's time alone, as JSON lines to PATH")
     ap.add_argument("--serve-slot-ctas", type=int, default=0,
                     help="serve: at most this many CTAs for a general slot's fit (0: an even share)")
     ap.add_argument("--serve-fast-slots", type=int, default=4,
@@ -1093,6 +1096,26 @@ def run_serve(args, world, rank, local, collect=False):
         peak = srv.peak_running
     finally:
         srv.close()
+    if args.serve_detail:
+        # per-request timeline of the last replay, and each request fitted alone on a
+        # context limited like the slot that served it (outside the timed region)
+        recs = serve.request_records(stream, done)
+        ctxs = {}
+        try:
+            for r in recs:
+                lim = srv.slot_max_ctas(r["slot"], torch.cuda.get_device_properties(local).multi_processor_count)
+                if lim not in ctxs:
+                    ctxs[lim] = native.Context(local)
+                    ctxs[lim].set_max_ctas(lim)
+                t0 = time.perf_counter()
+                native.fit_model(ctxs[lim], stream[r["rid"]][1], native.ModeFindingArguments())
+                r["alone_s"] = time.perf_counter() - t0
+        finally:
+            for c in ctxs.values():
+                c.close()
+        with open(args.serve_detail, "w") as fh:
+            for r in recs:
+                fh.write(json.dumps(r) + "\n")
     s = summaries[-1]
     h2d = sum(d.rows.nbytes + d.vals.nbytes + d.col_start.nbytes + d.val_start.nbytes + d.y.nbytes
               + (d.time.nbytes if d.time is not None else 0) + (d.stratum.nbytes if d.stratum is not None else 0)

@@ -248,6 +248,25 @@ def replay(server: Server, stream, args=None, time_scale: float = 1.0) -> List[C
     return sorted(done, key=lambda c: c.rid)
 
 
+def request_records(stream, done: List[Completed]) -> List[dict]:
+    """One record per completed request of a replay of `stream` ([(arrival
+    seconds, CyclopsData)]): its model, size, slot, and the wait (arrival to
+    start) and service (start to end) times, with the start and end as offsets
+    from the first arrival -- the timeline in which fits held up by their
+    neighbours show as service times far above their time alone."""
+    if not done:
+        return []
+    first = min(c.arrival for c in done)
+    out = []
+    for c in sorted(done, key=lambda c: c.rid):
+        d = stream[c.rid][1]
+        out.append({"rid": int(c.rid), "model": int(d.model_type), "K": int(d.K), "J": int(d.J),
+                    "entries": int(d.nnz), "slot": int(c.slot), "arrival_s": c.arrival - first,
+                    "start_s": c.start - first, "end_s": c.end - first, "wait_s": c.start - c.arrival,
+                    "service_s": c.end - c.start, "flag": int(c.flag), "error": c.error})
+    return out
+
+
 def latency_summary(done: List[Completed]) -> dict:
     lat = np.array([c.latency for c in done])
     first = min(c.arrival for c in done)

@@ -153,3 +153,25 @@ def test_slot_cta_limits():
         assert limits[kw["slots"]:] == [fast] * kw["fast_slots"]
         if general * kw["slots"] >= kw["slots"] and kw["slots"] <= n_sm:
             assert sum(limits) <= n_sm
+
+
+def test_request_records_timeline():
+    """Per-request records of a replay: model, size, slot, and wait / service
+    times consistent with the completion times, offsets from the first arrival."""
+    fit, _ = _stub(duration=0.01)
+    stream = [(0.0, synthetic.small(MODEL_LOGISTIC, seed=i, K=50, P=3)) for i in range(5)]
+    srv = serve.Server(hbm_budget=1e9, slots=2, fit_fn=fit)
+    try:
+        done = serve.replay(srv, stream)
+    finally:
+        srv.close()
+    recs = serve.request_records(stream, done)
+    assert [r["rid"] for r in recs] == list(range(5))
+    for r, c in zip(recs, sorted(done, key=lambda c: c.rid)):
+        assert r["model"] == MODEL_LOGISTIC and r["K"] == 50 and r["J"] == stream[r["rid"]][1].J
+        assert r["slot"] in (0, 1) and r["error"] is None
+        assert r["wait_s"] >= 0 and r["service_s"] >= 0.01
+        assert abs(r["end_s"] - r["start_s"] - r["service_s"]) < 1e-9
+        assert abs(r["start_s"] - r["arrival_s"] - r["wait_s"]) < 1e-9
+    assert min(r["arrival_s"] for r in recs) == 0.0
+    assert serve.request_records(stream, []) == []
