@@ -181,10 +181,47 @@ void run_case(int case_id, std::mt19937_64& rng) {
 
 }  // namespace
 
+// A chain longer than the builder's 16-bit level table holds: 70,000 columns
+// that all share row 0 (level j), a dense column in the middle (a level of its
+// own that every later column follows), and a fixed column; the builder must
+// move to its 32-bit table and keep every level.
+void run_long_chain(int case_id) {
+    const int32_t J = 70000;
+    const int64_t K = 3;
+    std::vector<uint8_t> fmt(J, F_INDICATOR), fixed(J, 0);
+    std::vector<int64_t> col_start(J + 1, 0), entries(J);
+    std::vector<int32_t> rows;
+    fmt[40000] = F_DENSE;
+    fixed[50000] = 1;
+    for (int32_t j = 0; j < J; ++j) {
+        if (fmt[j] == F_INDICATOR) rows.push_back(0);
+        col_start[j + 1] = (int64_t)rows.size();
+        entries[j] = (fmt[j] == F_DENSE) ? K : col_start[j + 1] - col_start[j];
+    }
+    ScheduleParams sp;
+    sp.n_cta = 4;
+    sp.warps_per_cta = 4;
+    const Schedule s = build_schedule(K, J, col_start.data(), rows.data(), fmt.data(), fixed.data(), nullptr, K,
+                                      entries.data(), sp);
+    int32_t want = 0;
+    bool ok = true;
+    for (int32_t j = 0; j < J; ++j) {
+        if (fixed[j]) {
+            ok = ok && s.level_of[j] == -1;
+            continue;
+        }
+        ok = ok && s.level_of[j] == want;
+        ++want;
+    }
+    check(ok, "levels of a chain beyond the 16-bit table", case_id);
+    check(s.n_levels == want, "level count of the long chain", case_id);
+}
+
 int main(int argc, char** argv) {
     const int cases = argc > 1 ? std::atoi(argv[1]) : 400;
     std::mt19937_64 rng(12345);
     for (int i = 0; i < cases; ++i) run_case(i, rng);
+    run_long_chain(cases);
     if (failures) {
         std::fprintf(stderr, "%d check(s) failed\n", failures);
         return 1;
