@@ -13,6 +13,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -1046,15 +1047,20 @@ static int32_t first_row_error(int64_t K, int32_t n_cols, const int64_t* col_sta
     lo[0] = 0;
     for (int32_t j = 0, t = 1; j < n_cols && t < T; ++j)
         if (col_start[j + 1] >= total * t / T) lo[t++] = j + 1;
+    auto walk = [&](int t) {
+        for (int32_t j = lo[t]; j < lo[t + 1]; ++j)
+            if (bad(j)) {
+                found[t] = j;
+                return;
+            }
+    };
     std::vector<std::thread> pool;
-    for (int t = 0; t < T; ++t)
-        pool.emplace_back([&, t] {
-            for (int32_t j = lo[t]; j < lo[t + 1]; ++j)
-                if (bad(j)) {
-                    found[t] = j;
-                    return;
-                }
-        });
+    int started = 0;
+    try {
+        for (; started < T; ++started) pool.emplace_back(walk, started);
+    } catch (const std::system_error&) {  // no more threads: this one walks the rest
+        for (int t = started; t < T; ++t) walk(t);
+    }
     for (auto& th : pool) th.join();
     return *std::min_element(found.begin(), found.end());
 }
