@@ -8,6 +8,7 @@
 #include "csr_host.h"
 
 #include <algorithm>
+#include <system_error>
 #include <thread>
 
 #include "types.h"
@@ -25,7 +26,12 @@ void run_parallel(int T, F&& f) {
     }
     std::vector<std::thread> pool;
     pool.reserve(T);
-    for (int t = 0; t < T; ++t) pool.emplace_back(f, t);
+    int started = 0;
+    try {
+        for (; started < T; ++started) pool.emplace_back(f, started);
+    } catch (const std::system_error&) {  // no more threads: this one runs the rest
+        for (int t = started; t < T; ++t) f(t);
+    }
     for (auto& th : pool) th.join();
 }
 
